@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Throughput of the GPE finite-difference time stepper on B200.
+
+Workload (one "step" = one full RK4 time step of every site): 512^3 periodic
+grid, h = 0.5, 4th-order centred differences, RK4 with dt = 0.005, equation 4
+(g = mu = 1, no trap), complex64 psi with Kahan-compensated accumulation and
+FP64 norm reduction every step; seeded random-phase initial condition
+(|k| <= 1.0, unit amplitudes, uniform phases, rescaled to mean density 1).
+Metric: site-updates/s (sites x steps / device time), whole job.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (launched by torchrun): every rank advances its own 512^3 replica
+(weak scaling, no data-path collective); device time is the max over ranks.
+--impl reference times the CPU restatement of the reference's path (the
+reference's Fortran build is unavailable in this image) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "site-updates/s & HBM GB/s at 512^3; time-to-t at <=1e-3 density err vs plain"
+N_GRID = 512
+H = 0.5
+DT = 0.005
+KMAX = 1.0
+# algorithmic bytes per site per RK4 step with complex64 + Kahan: stage 1
+# reads psi, writes u2 and acc (3 x 8 B); stages 2-3 read u, psi, acc and
+# write u', acc (5 x 8 B each); stage 4 reads u4, psi, acc, c and writes psi, c
+# (6 x 8 B) -> 152 B/site
+BYTES_PER_FAMILY = {"stage_first": 24, "stage_mid": 40, "stage_last": 48}
+BYTES_PER_STEP = 152
+LAUNCHES_PER_STEP = 5
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                if self.uuid and self.uuid not in parts[1]:
+                    continue
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[6:10]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+
+def random_phase_ic(torch, n, h, kmax, seed, device):
+    """Fourier modes with |k| <= kmax get unit amplitude and a uniform random
+    phase (torch Philox generator, fixed seed); inverse FFT; rescaled to mean
+    density 1."""
+    L = n * h
+    m = torch.fft.fftfreq(n, d=1.0 / n, device=device, dtype=torch.float64)
+    k = 2 * math.pi * m / L
+    kz, ky, kx = torch.meshgrid(k, k, k, indexing="ij")
+    mask = (kx * kx + ky * ky + kz * kz) <= kmax * kmax
+    del kx, ky, kz
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    phase = torch.rand((n, n, n), generator=gen, device=device, dtype=torch.float64)
+    a = torch.where(mask, torch.exp(2j * math.pi * phase.to(torch.complex128)),
+                    torch.zeros((), dtype=torch.complex128, device=device))
+    del phase, mask
+    psi = torch.fft.ifftn(a)
+    del a
+    psi = psi / torch.sqrt(torch.mean(psi.abs() ** 2))
+    return psi.to(torch.complex64).contiguous()
+
+
+def cpu_sample(threads: int, min_seconds: float = 10.0, max_steps: int = 50):
+    """Times the oracle (CPU restatement of the reference path, FP64, the
+    reference's own pass structure) on a 512 x 512 x 8 periodic slab of the
+    same workload; returns (site-updates/s, steps, sites, seconds)."""
+    import numpy as np
+
+    import oracle
+
+    oracle.set_threads(threads)
+    nx = ny = N_GRID
+    nz = 8
+    xr = H * (nx - 1) / 2
+    zr = H * (nz - 1) / 2
+    o = oracle.Oracle(oracle.OracleParams(nx=nx, ny=ny, nz=nz, xr=xr, yr=xr, zr=zr,
+                                          scheme="rk4", eqn_to_solve=4, bcs=1, order=4,
+                                          g=1.0, mu=1.0))
+    rng = np.random.default_rng(0)
+    psi = np.exp(2j * np.pi * rng.random((nz, ny, nx)))
+    tm = oracle.OraTime(0.0, 0.0, DT, 0.0, 0)
+    psi, _, _ = o.solver(psi, tm)  # warm-up (page-in)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        psi, _, _ = o.solver(psi, tm)
+        o.get_norm(psi)
+        steps += 1
+        el = time.perf_counter() - t0
+        if (el >= min_seconds and steps >= 2) or steps >= max_steps:
+            break
+    sites = nx * ny * nz
+    return sites * steps / el, steps, sites, el
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    import numpy as np
+
+    import oracle
+
+    oracle.set_threads(threads)
+    nx = ny = N_GRID
+    nz = 8
+    xr = H * (nx - 1) / 2
+    zr = H * (nz - 1) / 2
+    o = oracle.Oracle(oracle.OracleParams(nx=nx, ny=ny, nz=nz, xr=xr, yr=xr, zr=zr,
+                                          scheme="rk4", eqn_to_solve=4, bcs=1, order=4,
+                                          g=1.0, mu=1.0))
+    rng = np.random.default_rng(0)
+    psi = np.exp(2j * np.pi * rng.random((nz, ny, nx)))
+    tm = oracle.OraTime(0.0, 0.0, DT, 0.0, 0)
+    for _ in range(args.warmup):
+        psi, _, _ = o.solver(psi, tm)
+        o.get_norm(psi)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        psi, _, _ = o.solver(psi, tm)
+        o.get_norm(psi)
+    el = time.perf_counter() - t0
+    sites = nx * ny * nz
+    v = sites * args.steps / el
+    sample = (f"each step = one RK4 step (+ get_norm) of a {nx}x{ny}x{nz} periodic slab of the "
+              f"512^3 workload, FP64, {threads} OpenMP threads over z-planes")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "site-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps * (N_GRID / nz),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded random phases)",
+        "config": workload_config(args.gpus),
+        "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": ("the reference Fortran/MPI/FFTW2 build cannot be compiled in this image; "
+                 "this arm runs the project's C restatement of its path (oracle/), which keeps "
+                 "the reference's pass structure"),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(ngpus):
+    return {"workload": "512^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
+                        "(g=mu=1, V=0), complex64 psi + Kahan compensation, FP64 norm per step",
+            "grid": [N_GRID, N_GRID, N_GRID], "h": H, "dt": DT, "scheme": "rk4", "order": 4,
+            "bcs": "periodic", "storage": "complex64+kahan",
+            "ic": "random phase, |k|<=1.0, seed 0",
+            "l2": "inputs larger than L2 (each field 1.07 GB, 5 fields) - no flush needed",
+            "parallelism": f"replicas x{ngpus}" if ngpus > 1 else "single GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpe_b200", choices=["gpe_b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from gpe_b200 import GpeParams, GpeSolver, lib
+
+    n = N_GRID
+    xr = H * (n - 1) / 2
+    prm = GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
+                    order=4, precision=8, kahan=True, g=1.0, mu=1.0, device=local)
+    s = GpeSolver(prm, tau=DT)
+    psi0 = random_phase_ic(torch, n, H, KMAX, 0, torch.device("cuda", local))
+    s.set_state(psi0)
+    del psi0
+    torch.cuda.empty_cache()
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
+
+    # warm-up
+    s.advance(args.warmup)
+
+    props = torch.cuda.get_device_properties(local)
+    uuid = str(getattr(props, "uuid", "") or "")
+    sampler = ClockSampler(uuid[-12:] if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+    s.set_timing(True)
+    s.timing()  # reset accumulators
+    lc0 = s.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    norms = s.advance(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize(local)
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.launch_count() - lc0
+    fam = s.timing()
+    s.set_timing(False)
+    clocks = sampler.stop()
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    sites = n ** 3
+    value = world * sites * args.steps / (ms_max / 1e3)
+
+    # roofline of the dominant kernel family and of the whole step
+    peak, peak_kind = load_peaks()
+    dominant = max(("stage_first", "stage_mid", "stage_last"), key=lambda f: fam[f]["ms"])
+    d = fam[dominant]
+    per_launch_ms = d["ms"] / max(d["launches"], 1)
+    alg_bytes = BYTES_PER_FAMILY[dominant] * sites
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    traffic = load_traffic().get(dominant)
+    kernel_ms_step = sum(fam[f]["ms"] for f in ("stage_first", "stage_mid", "stage_last",
+                                                "reduce")) / args.steps
+    step_gbs = BYTES_PER_STEP * sites / (kernel_ms_step / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": f"stage_kernel ({dominant})",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "per_launch_ms": per_launch_ms,
+                "step": {"alg_bytes_per_site": BYTES_PER_STEP, "kernel_ms_per_step": kernel_ms_step,
+                         "achieved": step_gbs, "frac": step_gbs / peak,
+                         "frac_vs_nominal_8000": step_gbs / 8000.0},
+                "families": fam}
+
+    # end to end through the C-ABI with host buffers (pinned), host<->device
+    # copies inside the timed region: the literal solver(var_in, var_out) form
+    nb = sites * 8
+    L = lib()
+    hin = L.gpe_gpu_host_alloc(nb)
+    hout = L.gpe_gpu_host_alloc(nb)
+    a_in = np.ctypeslib.as_array(ctypes.cast(hin, ctypes.POINTER(ctypes.c_float)), (2 * sites,))
+    a_out = np.ctypeslib.as_array(ctypes.cast(hout, ctypes.POINTER(ctypes.c_float)), (2 * sites,))
+    tmp = s.get_state(np.complex64)
+    a_in[:] = tmp.view(np.float32).ravel()
+    del tmp
+    from gpe_b200._lib import GpeStepInfoC, GpeTimeC, check
+    ke = max(1, args.e2e_steps)
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ke):
+        tm = GpeTimeC(s.t, s.im_t, s.dt.real, s.dt.imag, s.p, 0)
+        info = GpeStepInfoC()
+        check(L.gpe_gpu_solver_host(s.handle, ctypes.c_void_p(hin), ctypes.c_void_p(hout), 8,
+                                    ctypes.byref(tm), ctypes.byref(info)), s.handle)
+        s.t, s.im_t = tm.t, tm.im_t
+        hin, hout = hout, hin
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    e2e_ms = e0.elapsed_time(e1) / ke
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    L.gpe_gpu_host_free(ctypes.c_void_p(hin))
+    L.gpe_gpu_host_free(ctypes.c_void_p(hout))
+    e2e = {"value": world * sites / (e2e_ms / 1e3), "unit": "site-updates/s",
+           "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": e2e_ms,
+           "form": "gpe_gpu_solver_host: pinned host psi in -> step -> host psi out, per step"}
+
+    # resident form: the reference loop's per-step calls (solver + get_norm)
+    e0.record(stream)
+    for _ in range(ke):
+        s.solver()
+        s.get_norm()
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    res_ms = e0.elapsed_time(e1) / ke
+    e2e_resident = {"value": world * sites / (res_ms / 1e3), "unit": "site-updates/s",
+                    "h2d_bytes_per_step": ctypes.sizeof(GpeTimeC), "d2h_bytes_per_step": 8,
+                    "ms_per_step": res_ms,
+                    "form": "psi resident; per step gpe_gpu_solver + gpe_gpu_norm (8 B read back)"}
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, st, ss, el = cpu_sample(threads)
+        cpu = {"value": v, "unit": "site-updates/s", "cores": threads, "kind": "port",
+               "sample": f"{st} RK4 steps (+ get_norm) of a 512x512x8 periodic slab of the "
+                         f"workload ({ss} sites), FP64 oracle with the reference's pass "
+                         f"structure, {threads} OpenMP threads, {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random-phase IC, |k|<=1.0, torch Philox seed 0)",
+            "config": workload_config(world),
+            "hbm_gbs_step": step_gbs,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_resident": e2e_resident,
+            "clocks": clocks, "gpu_launches": int(launches),
+            "gpu_launches_per_step": launches / args.steps,
+            "final_norm": float(norms[-1]) if len(norms) else None,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

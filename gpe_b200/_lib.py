@@ -1,0 +1,119 @@
+"""ctypes binding of ``libgpe_gpu.so`` (the C-ABI declared in include/gpe_gpu.h).
+
+The library is loaded from this package directory only.  There is no CPU or
+eager fallback: if the shared library is missing, or a call is made without a
+B200, the error is raised to the caller.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgpe_gpu.so")
+
+GPE_OK = 0
+STATUS_NAMES = {
+    1: "GPE_ERR_INVALID", 2: "GPE_ERR_SCHEME", 3: "GPE_ERR_CUDA", 4: "GPE_ERR_OOM",
+    5: "GPE_ERR_NAN", 6: "GPE_ERR_TIMEOUT", 7: "GPE_ERR_NODEVICE", 8: "GPE_ERR_UNDERFLOW",
+}
+SCHEMES = {"euler": 0, "rk2": 1, "rk4": 2, "rk45": 3}
+TIMING_FAMILIES = ["stage_first", "stage_mid", "stage_last", "reduce", "energy", "copy", "other",
+                   "unused"]
+
+
+class GpeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        self.code = code
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+
+
+class GpeParamsC(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32),
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("xr", ctypes.c_double), ("yr", ctypes.c_double), ("zr", ctypes.c_double),
+        ("scheme", ctypes.c_int32), ("eqn_to_solve", ctypes.c_int32),
+        ("bcs", ctypes.c_int32), ("order", ctypes.c_int32), ("real_time", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("Urhs", ctypes.c_double), ("diss_amp", ctypes.c_double), ("scal", ctypes.c_double),
+        ("g", ctypes.c_double), ("mu", ctypes.c_double), ("nn", ctypes.c_double),
+        ("omx", ctypes.c_double), ("omy", ctypes.c_double), ("omz", ctypes.c_double),
+        ("kahan", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("tile_y", ctypes.c_int32), ("zchunk", ctypes.c_int32),
+    ]
+
+
+class GpeTimeC(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double), ("im_t", ctypes.c_double),
+                ("dt_re", ctypes.c_double), ("dt_im", ctypes.c_double),
+                ("p", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class GpeStepInfoC(ctypes.Structure):
+    _fields_ = [("errmax", ctypes.c_double), ("dt_did_re", ctypes.c_double),
+                ("dt_did_im", ctypes.c_double), ("attempts", ctypes.c_int32),
+                ("underflow", ctypes.c_int32)]
+
+
+class GpeTimingC(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double * 8), ("launches", ctypes.c_int64 * 8),
+                ("sites", ctypes.c_int64 * 8)]
+
+
+# Every symbol include/gpe_gpu.h declares, with (restype, argtypes).
+_vp, _i32, _i64, _dp = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "gpe_gpu_abi_version": (_i32, []),
+    "gpe_gpu_default_params": (None, [ctypes.POINTER(GpeParamsC), _i32, _i32, _i32]),
+    "gpe_gpu_create": (ctypes.c_int, [ctypes.POINTER(GpeParamsC), ctypes.POINTER(_vp)]),
+    "gpe_gpu_destroy": (None, [_vp]),
+    "gpe_gpu_last_error": (ctypes.c_char_p, [_vp]),
+    "gpe_gpu_grid": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "gpe_gpu_set_state": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_gpu_get_state": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_gpu_set_state_device": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_gpu_get_state_device": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_gpu_solver": (ctypes.c_int, [_vp, ctypes.POINTER(GpeTimeC), ctypes.POINTER(GpeStepInfoC)]),
+    "gpe_gpu_solver_host": (ctypes.c_int, [_vp, _vp, _vp, _i32, ctypes.POINTER(GpeTimeC),
+                                           ctypes.POINTER(GpeStepInfoC)]),
+    "gpe_gpu_advance": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(GpeTimeC), _dp]),
+    "gpe_gpu_norm": (ctypes.c_int, [_vp, _dp]),
+    "gpe_gpu_energy": (ctypes.c_int, [_vp, _dp, _dp]),
+    "gpe_gpu_renormalise": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "gpe_gpu_rhs": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_gpu_laplacian": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_gpu_set_real_time": (ctypes.c_int, [_vp, _i32]),
+    "gpe_gpu_set_timing": (ctypes.c_int, [_vp, _i32]),
+    "gpe_gpu_get_timing": (ctypes.c_int, [_vp, ctypes.POINTER(GpeTimingC)]),
+    "gpe_gpu_launch_count": (_i64, [_vp]),
+    "gpe_gpu_device_bytes": (_i64, [_vp]),
+    "gpe_gpu_stream": (_vp, [_vp]),
+    "gpe_gpu_host_alloc": (_vp, [ctypes.c_size_t]),
+    "gpe_gpu_host_free": (None, [_vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m gpe_b200.build` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, ctx=None) -> None:
+    if rc != GPE_OK:
+        msg = lib().gpe_gpu_last_error(ctx)
+        raise GpeError(rc, msg.decode() if msg else "")

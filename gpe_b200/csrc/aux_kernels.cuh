@@ -1,0 +1,138 @@
+// aux_kernels.cuh -- state transfer, scaling and reduction kernels.
+#pragma once
+
+#include "device_utils.cuh"
+
+namespace gpe {
+
+struct Geom {
+  int nx, ny, nz;  // interior
+  int Nx, Ny;      // padded pitches
+  int bcs;
+};
+
+__device__ __forceinline__ size_t padded_index(const Geom& g, int i, int j,
+                                               int k) {
+  return ((size_t)(k + 2) * g.Ny + (size_t)(j + 2)) * g.Nx + (size_t)(i + 2);
+}
+
+// Dense interior array (any complex type TI) -> padded field of TS, with the
+// boundary ghosts filled (the caller's halo exchange, src/gpe.f90:165-174).
+template <typename TS, typename TI>
+__global__ void unpack_kernel(const TI* __restrict__ src, TS* __restrict__ dst,
+                              Geom g) {
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const size_t r = q / g.nx;
+    const int j = (int)(r % g.ny);
+    const int k = (int)(r / g.ny);
+    const TS vr = (TS)src[2 * q], vi = (TS)src[2 * q + 1];
+    st_one<TS>(dst + 2 * padded_index(g, i, j, k), vr, vi);
+    int a, b;
+    ghost_targets(i, g.nx, g.bcs, a, b);
+    if (a != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, a, j, k), vr, vi);
+    if (b != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, b, j, k), vr, vi);
+    ghost_targets(j, g.ny, g.bcs, a, b);
+    if (a != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, a, k), vr, vi);
+    if (b != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, b, k), vr, vi);
+    ghost_targets(k, g.nz, g.bcs, a, b);
+    if (a != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, j, a), vr, vi);
+    if (b != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, j, b), vr, vi);
+  }
+}
+
+// Padded field -> dense interior array of TO.
+template <typename TS, typename TO>
+__global__ void pack_kernel(const TS* __restrict__ src, TO* __restrict__ dst,
+                            Geom g) {
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const size_t r = q / g.nx;
+    const int j = (int)(r % g.ny);
+    const int k = (int)(r / g.ny);
+    const size_t s = padded_index(g, i, j, k);
+    dst[2 * q] = (TO)src[2 * s];
+    dst[2 * q + 1] = (TO)src[2 * s + 1];
+  }
+}
+
+// renormalise (src/variables.f90:698-709): f = (sqrt(nn) f) / sqrt(norm)
+// over the whole padded buffer, ghosts included (they stay exact copies).
+template <typename TS>
+__global__ void scale_kernel(TS* __restrict__ f, size_t nscalars, double snn,
+                             double sn) {
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nscalars;
+       q += (size_t)gridDim.x * blockDim.x) {
+    f[q] = (TS)(((double)f[q] * snn) / sn);
+  }
+}
+
+// Weighted |psi|^2 per CTA into partials[2*blk] (get_norm without a stencil).
+template <typename TS>
+__global__ void norm_kernel(const TS* __restrict__ f, Geom g,
+                            const double* __restrict__ wx,
+                            const double* __restrict__ wy,
+                            const double* __restrict__ wz,
+                            double* __restrict__ partials) {
+  __shared__ double s[32];
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  double acc = 0.0;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const size_t r = q / g.nx;
+    const int j = (int)(r % g.ny);
+    const int k = (int)(r / g.ny);
+    const size_t pi = padded_index(g, i, j, k);
+    const double a = (double)f[2 * pi], b = (double)f[2 * pi + 1];
+    acc += (wx[i] * wy[j]) * wz[k] * (a * a + b * b);
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s[w];
+    partials[2 * blockIdx.x] = t;
+    partials[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
+// Fixed-order reduction of partials[2*b + slot], b < nblk, by one CTA of
+// 1024 threads.  op 0 = sum, 1 = max.  out[0] = result * scale; when
+// `series` is non-null also series[*counter] = out[0] and ++*counter.
+__global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
+                                int slot, int op, double scale,
+                                double* __restrict__ out,
+                                double* __restrict__ series,
+                                int* __restrict__ counter) {
+  __shared__ double s[1024];
+  double a = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    const double v = partials[2 * (size_t)b + slot];
+    a = op ? fmax(a, v) : a + v;
+  }
+  s[threadIdx.x] = a;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      const double v = s[threadIdx.x + w];
+      s[threadIdx.x] = op ? fmax(s[threadIdx.x], v) : s[threadIdx.x] + v;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double r = s[0] * scale;
+    out[0] = r;
+    if (series) {
+      series[*counter] = r;
+      *counter = *counter + 1;
+    }
+  }
+}
+
+}  // namespace gpe

@@ -1,0 +1,1341 @@
+// gpe_gpu.cu -- context, stage scheduling and the C-ABI of include/gpe_gpu.h.
+//
+// One context = one run on one device.  Fields live in a ghost-padded layout
+// (2 ghost layers on every axis, x pitch rounded to 4 elements) so that each
+// stage kernel reads its stencil plane as one TMA box; ghosts are refreshed by
+// the kernel that writes the field (see stage_kernel.cuh), which replaces the
+// reference's halo exchange (src/variables.f90:186-358).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+#include "aux_kernels.cuh"
+#include "gpe_gpu.h"
+#include "stage_kernel.cuh"
+
+using cd = std::complex<double>;
+using namespace gpe;
+
+namespace {
+
+// Cash-Karp coefficients (src/solve.f90:255-281).
+constexpr double B21 = 0.2;
+constexpr double B31 = 0.075, B32 = 0.225;
+constexpr double B41 = 0.3, B42 = -0.9, B43 = 1.2;
+constexpr double B51 = -11.0 / 54.0, B52 = 2.5, B53 = -70.0 / 27.0,
+                 B54 = 35.0 / 27.0;
+constexpr double B61 = 1631.0 / 55296.0, B62 = 175.0 / 512.0,
+                 B63 = 575.0 / 13824.0, B64 = 44275.0 / 110592.0,
+                 B65 = 253.0 / 4096.0;
+constexpr double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0,
+                 C6 = 512.0 / 1771.0;
+constexpr double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0,
+                 DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0,
+                 DC6 = C6 - 0.25;
+// Adaptive step constants (src/parameters.f90:89-92).
+constexpr double RK_EPS = 1e-6, SAFETY = 0.9, DT_DECREASE = -0.25,
+                 DT_INCREASE = -0.20;
+// Extended-Simpson end weights (src/variables.f90:49-51).
+constexpr double W1 = 3.0 / 8.0, W2 = 7.0 / 6.0, W3 = 23.0 / 24.0;
+
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // 2 s
+
+enum FieldId {
+  F_PSI = 0, F_ALT, F_ACC, F_UA, F_UB, F_C, F_CALT,
+  F_K1, F_K2, F_K3, F_K4, F_K5, F_COUNT
+};
+
+thread_local std::string g_last_create_error;
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+struct Launch {
+  int family;
+  cudaEvent_t a, b;
+  int64_t sites;
+};
+
+}  // namespace
+
+struct gpe_ctx {
+  gpe_params prm;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  int nx, ny, nz, Nx, Ny, Nz;
+  size_t npad, nint;
+  int es;  // bytes per stored complex element (8 or 16)
+  double dx, dy, dz;
+  std::vector<double> x, y, z;
+  void* fld[F_COUNT] = {};
+  int psi_id = F_PSI, alt_id = F_ALT, c_id = F_C, calt_id = F_CALT;
+  // tables: per axis padded to tab_n entries
+  int tab_n[3];
+  float* tabVf[3] = {};
+  float* tabDf[3] = {};
+  double* tabVd[3] = {};
+  double* tabDd[3] = {};
+  double* tabW[3] = {};
+  double* tabX[3] = {};
+  void* d_tables = nullptr;
+  double* d_partials = nullptr;
+  size_t partials_cap = 0;  // CTAs
+  double* d_scal = nullptr;  // [0] norm [1] E [2] H4 [3] errmax
+  double* d_series = nullptr;
+  size_t series_cap = 0;
+  int* d_counter = nullptr;
+  int* d_status = nullptr;
+  void* d_stage = nullptr;  // dense staging, nint * 16 bytes
+  void* h_pinned = nullptr;
+  size_t h_pinned_bytes = 0;
+  bool norm_valid = false;
+  int64_t launches = 0;
+  int last_nblk = 0;
+  int64_t device_bytes = 0;
+  std::map<std::tuple<int, int, int, int>, CUtensorMap> maps;
+  bool timing = false;
+  std::vector<Launch> timed;
+  gpe_timing acc_timing;
+  std::vector<cudaEvent_t> ev_pool;
+  std::string err;
+};
+
+namespace {
+
+int fail(gpe_ctx* c, int code, const std::string& msg) {
+  if (c)
+    c->err = msg;
+  else
+    g_last_create_error = msg;
+  return code;
+}
+
+#define CU_CHECK(c, call)                                                    \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return fail((c), GPE_ERR_CUDA,                                         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+int ensure_encode(gpe_ctx* c) {
+  if (g_encode) return GPE_OK;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn,
+                                          cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+    return fail(c, GPE_ERR_CUDA, "cuTensorMapEncodeTiled entry point not found");
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return GPE_OK;
+}
+
+// kind 0: halo box (64+4) x (TY+2R); kind 1: pointwise box 64 x TY.
+int get_map(gpe_ctx* c, int field, int kind, int TY, int R,
+            CUtensorMap* out) {
+  auto key = std::make_tuple(field, kind, TY, kind == 0 ? R : 0);
+  auto it = c->maps.find(key);
+  if (it != c->maps.end()) {
+    *out = it->second;
+    return GPE_OK;
+  }
+  int rc = ensure_encode(c);
+  if (rc) return rc;
+  const cuuint64_t W = (cuuint64_t)(c->es / 8);
+  cuuint64_t dims[3] = {W * (cuuint64_t)c->Nx, (cuuint64_t)c->Ny,
+                        (cuuint64_t)c->Nz};
+  cuuint64_t strides[2] = {(cuuint64_t)c->Nx * c->es,
+                           (cuuint64_t)c->Nx * c->Ny * c->es};
+  cuuint32_t box[3];
+  if (kind == 0) {
+    box[0] = (cuuint32_t)(W * (TX + 4));
+    box[1] = (cuuint32_t)(TY + 2 * R);
+  } else {
+    box[0] = (cuuint32_t)(W * TX);
+    box[1] = (cuuint32_t)TY;
+  }
+  box[2] = 1;
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap m;
+  CUresult r = g_encode(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, c->fld[field],
+                        dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return fail(c, GPE_ERR_CUDA,
+                "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  c->maps[key] = m;
+  *out = m;
+  return GPE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stage description, independent of precision.
+
+struct StageSpec {
+  int stencil = F_PSI;
+  int np = 0;
+  int pt[MAXP] = {0, 0, 0, 0, 0, 0};
+  int nout = 0;
+  int out[2] = {0, 0};
+  int ghost_mask = 0;
+  cd ca[2] = {cd(0), cd(0)};
+  cd cb[2][MAXP] = {};
+  cd ck[2] = {cd(0), cd(0)};
+  int epi = 0;
+  cd ce[MAXP] = {};
+  cd cek = cd(0);
+  cd dt0 = cd(0);
+  double inv_absdt = 0.0;
+  int family = GPE_FAM_OTHER;
+};
+
+struct LaunchShape {
+  int TY, S, zchunk, ntx, nty, nchunks;
+  size_t smem;
+  unsigned halo_box, pt_box, halo_smem, pt_smem;
+};
+
+LaunchShape choose_shape(const gpe_ctx* c, int R, int np) {
+  LaunchShape s{};
+  const int es = c->es;
+  int TY = c->prm.tile_y > 0 ? c->prm.tile_y : 8;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    s.TY = TY;
+    s.halo_box = (unsigned)((TX + 4) * (TY + 2 * R) * es);
+    s.pt_box = (unsigned)(TX * TY * es);
+    s.halo_smem = (unsigned)round_up(s.halo_box, 128);
+    s.pt_smem = (unsigned)round_up(s.pt_box, 128);
+    const size_t stage = s.halo_smem + (size_t)np * s.pt_smem;
+    int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
+    int ctas = 2;
+    if (S < R + 3) {
+      S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
+      ctas = 1;
+    }
+    if (S >= R + 2 || attempt == 1 || c->prm.tile_y > 0) {
+      s.S = std::max(S, R + 2);
+      s.smem = 128 + (size_t)s.S * stage;
+      s.ntx = (c->nx + TX - 1) / TX;
+      s.nty = (c->ny + TY - 1) / TY;
+      const int ntiles = s.ntx * s.nty;
+      int zc = c->prm.zchunk;
+      if (zc <= 0) {
+        const long target = 148L * ctas * 8;
+        long chunks = (target + ntiles - 1) / ntiles;
+        chunks = std::max<long>(1, std::min<long>(chunks, c->nz));
+        zc = (int)((c->nz + chunks - 1) / chunks);
+        zc = std::max(zc, std::min(4, c->nz));
+      }
+      s.zchunk = zc;
+      s.nchunks = (c->nz + zc - 1) / zc;
+      return s;
+    }
+    TY = 4;
+  }
+  return s;
+}
+
+using KernelFn = const void*;
+
+template <typename TS, typename TC, int R>
+KernelFn pick_kernel(int np, int nout, int epi) {
+#define GPE_CASE(NP_, NOUT_, EPI_)                                       \
+  if (np == NP_ && nout == NOUT_ && epi == (EPI_))                      \
+    return reinterpret_cast<KernelFn>(                                   \
+        &stage_kernel<TS, TC, R, NP_, NOUT_, (EPI_)>);
+  if constexpr (std::is_same<TC, double>::value &&
+                std::is_same<TS, float>::value) {
+    GPE_CASE(0, 0, EPI_ENERGY)
+  } else {
+    GPE_CASE(0, 0, EPI_ENERGY)
+    GPE_CASE(0, 1, 0)
+    GPE_CASE(0, 1, EPI_LAP)
+    GPE_CASE(0, 1, EPI_NORM)
+    GPE_CASE(1, 1, EPI_NORM)
+    GPE_CASE(0, 2, 0)
+    GPE_CASE(2, 2, 0)
+    GPE_CASE(3, 2, 0)
+    GPE_CASE(4, 2, 0)
+    GPE_CASE(5, 2, 0)
+    GPE_CASE(5, 1, EPI_NORM | EPI_ERR)
+    if constexpr (std::is_same<TS, float>::value) {
+      GPE_CASE(1, 2, EPI_KAHAN | EPI_NORM)
+      GPE_CASE(2, 2, EPI_KAHAN | EPI_NORM)
+      GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM)
+      GPE_CASE(6, 2, EPI_KAHAN | EPI_NORM | EPI_ERR)
+    }
+  }
+#undef GPE_CASE
+  return nullptr;
+}
+
+cudaEvent_t pool_event(gpe_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void fill_rhs_coeffs(const gpe_ctx* c, double& ar0, double& ard, double& ai,
+                     double& cL, double& c0, double& cV, double& cn,
+                     double& U, int& use_diss, int& use_V, int& use_sphere,
+                     int& use_grad) {
+  const gpe_params& p = c->prm;
+  // f = m * ( A*(cL*L + (c0 + cV*V + cn*|u|^2) u) + U*u_x ), A = ar + i ai
+  // (src/solve.f90:414-437)
+  ar0 = 0; ard = 0; ai = 1; cL = 1; c0 = 0; cV = 0; cn = -1; U = 0;
+  use_diss = 0; use_V = 0; use_sphere = 0; use_grad = 0;
+  switch (p.eqn_to_solve) {
+    case 1:
+    case 3:
+      ai = 0.5; ard = 0.5; cL = 1; c0 = 1; cn = -1; U = p.Urhs;
+      use_diss = p.diss_amp != 0.0;
+      use_grad = p.Urhs != 0.0;
+      use_sphere = p.eqn_to_solve == 3;
+      break;
+    case 2:
+      ai = 1; cL = 1; c0 = 0; cn = -1; U = p.Urhs;
+      use_grad = p.Urhs != 0.0;
+      break;
+    default:  // 4
+      ai = 1; cL = 0.5; c0 = p.mu; cV = -1; cn = -p.g;
+      use_V = (p.omx != 0.0 || p.omy != 0.0 || p.omz != 0.0);
+      break;
+  }
+}
+
+template <typename TS, typename TC>
+int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
+  const int R = c->prm.order / 2;
+  const LaunchShape sh = choose_shape(c, R, sp.np);
+  StageParams<TS, TC> p;
+  memset(&p, 0, sizeof(p));
+  int rc = get_map(c, sp.stencil, 0, sh.TY, R, &p.maps.halo);
+  if (rc) return rc;
+  for (int q = 0; q < sp.np; q++) {
+    rc = get_map(c, sp.pt[q], 1, sh.TY, R, &p.maps.pt[q]);
+    if (rc) return rc;
+  }
+  p.nx = c->nx; p.ny = c->ny; p.nz = c->nz; p.Nx = c->Nx; p.Ny = c->Ny;
+  p.ntx = sh.ntx; p.zchunk = sh.zchunk; p.bcs = c->prm.bcs; p.TY = sh.TY;
+  p.stages = sh.S;
+  p.halo_box_bytes = sh.halo_box; p.pt_box_bytes = sh.pt_box;
+  p.halo_smem_bytes = sh.halo_smem; p.pt_smem_bytes = sh.pt_smem;
+  p.stencil = static_cast<const TS*>(c->fld[sp.stencil]);
+  for (int o = 0; o < sp.nout; o++) p.out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
+  p.ghost_mask = sp.ghost_mask;
+  const double h2[3] = {c->dx * c->dx, c->dy * c->dy, c->dz * c->dz};
+  double c1[3], c2[3];
+  for (int a = 0; a < 3; a++) {
+    if (R == 1) { c1[a] = 1.0 / h2[a]; c2[a] = 0.0; }
+    else { c1[a] = 16.0 / (12.0 * h2[a]); c2[a] = -1.0 / (12.0 * h2[a]); }
+  }
+  p.cx1 = (TC)c1[0]; p.cx2 = (TC)c2[0];
+  p.cy1 = (TC)c1[1]; p.cy2 = (TC)c2[1];
+  p.cz1 = (TC)c1[2]; p.cz2 = (TC)c2[2];
+  if (R == 1) { p.gx1 = (TC)(1.0 / (2.0 * c->dx)); p.gx2 = (TC)0; }
+  else { p.gx1 = (TC)(8.0 / (12.0 * c->dx)); p.gx2 = (TC)(-1.0 / (12.0 * c->dx)); }
+  double ar0, ard, ai, cL, c0, cV, cn, U;
+  int ud, uv, us, ug;
+  fill_rhs_coeffs(c, ar0, ard, ai, cL, c0, cV, cn, U, ud, uv, us, ug);
+  p.ar0 = (TC)ar0; p.ard = (TC)ard; p.ai = (TC)ai; p.cL = (TC)cL;
+  p.c0 = (TC)c0; p.cV = (TC)cV; p.cn = (TC)cn; p.U = (TC)U;
+  p.use_diss = ud; p.use_V = uv; p.use_sphere = us; p.use_grad = ug;
+  for (int a = 0; a < 3; a++) {
+    if (std::is_same<TC, float>::value) {
+      p.tabV[a] = reinterpret_cast<const TC*>(c->tabVf[a]);
+      p.tabD[a] = reinterpret_cast<const TC*>(c->tabDf[a]);
+    } else {
+      p.tabV[a] = reinterpret_cast<const TC*>(c->tabVd[a]);
+      p.tabD[a] = reinterpret_cast<const TC*>(c->tabDd[a]);
+    }
+    p.tabW[a] = c->tabW[a];
+    p.tabX[a] = c->tabX[a];
+  }
+  for (int o = 0; o < 2; o++) {
+    p.ca_r[o] = (TC)sp.ca[o].real(); p.ca_i[o] = (TC)sp.ca[o].imag();
+    p.ck_r[o] = (TC)sp.ck[o].real(); p.ck_i[o] = (TC)sp.ck[o].imag();
+    for (int q = 0; q < MAXP; q++) {
+      p.cb_r[o][q] = (TC)sp.cb[o][q].real();
+      p.cb_i[o][q] = (TC)sp.cb[o][q].imag();
+    }
+  }
+  for (int q = 0; q < MAXP; q++) { p.ce_r[q] = sp.ce[q].real(); p.ce_i[q] = sp.ce[q].imag(); }
+  p.cek_r = sp.cek.real(); p.cek_i = sp.cek.imag();
+  p.dt0_r = sp.dt0.real(); p.dt0_i = sp.dt0.imag();
+  p.inv_absdt = sp.inv_absdt;
+  p.eg = c->prm.g; p.emu = c->prm.mu;
+  p.partials = c->d_partials;
+  p.status = c->d_status;
+  p.wait_limit_ns = WAIT_LIMIT_NS;
+
+  KernelFn fn = (R == 1) ? pick_kernel<TS, TC, 1>(sp.np, sp.nout, sp.epi)
+                         : pick_kernel<TS, TC, 2>(sp.np, sp.nout, sp.epi);
+  if (!fn) return fail(c, GPE_ERR_INVALID, "no kernel for this stage shape");
+  const size_t nblk = (size_t)sh.ntx * sh.nty * sh.nchunks;
+  if (nblk > c->partials_cap)
+    return fail(c, GPE_ERR_INVALID, "partials buffer too small");
+  CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sh.smem));
+  dim3 grid((unsigned)(sh.ntx * sh.nty), (unsigned)sh.nchunks, 1);
+  dim3 block(32, (unsigned)sh.TY, 1);
+  void* args[] = {&p};
+  Launch L{};
+  if (c->timing) {
+    L.family = sp.family;
+    L.a = pool_event(c);
+    L.b = pool_event(c);
+    L.sites = (int64_t)c->nint;
+    cudaEventRecord(L.a, c->stream);
+  }
+  CU_CHECK(c, cudaLaunchKernel(fn, grid, block, args, sh.smem, c->stream));
+  if (c->timing) {
+    cudaEventRecord(L.b, c->stream);
+    c->timed.push_back(L);
+  }
+  c->launches++;
+  c->last_nblk = (int)nblk;
+  return GPE_OK;
+}
+
+}  // namespace
+
+namespace {
+
+int launch_stage(gpe_ctx* c, const StageSpec& sp) {
+  if (sp.epi & EPI_ENERGY) {
+    if (c->es == 8) return launch_stage_t<float, double>(c, sp);
+    return launch_stage_t<double, double>(c, sp);
+  }
+  if (c->es == 8) return launch_stage_t<float, float>(c, sp);
+  return launch_stage_t<double, double>(c, sp);
+}
+
+Geom geom(const gpe_ctx* c) {
+  Geom g;
+  g.nx = c->nx; g.ny = c->ny; g.nz = c->nz; g.Nx = c->Nx; g.Ny = c->Ny;
+  g.bcs = c->prm.bcs;
+  return g;
+}
+
+int elementwise_blocks(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)std::min<size_t>(b, 148 * 16);
+}
+
+void begin_timed(gpe_ctx* c, Launch& L, int family, int64_t sites) {
+  if (!c->timing) return;
+  L.family = family;
+  L.a = pool_event(c);
+  L.b = pool_event(c);
+  L.sites = sites;
+  cudaEventRecord(L.a, c->stream);
+}
+void end_timed(gpe_ctx* c, Launch& L) {
+  if (!c->timing) return;
+  cudaEventRecord(L.b, c->stream);
+  c->timed.push_back(L);
+}
+
+// partials -> d_scal[slot_out] (and optionally the per-step series).
+int finalize(gpe_ctx* c, int nblk, int slot, int op, double scale,
+             int out_index, bool series) {
+  Launch L{};
+  begin_timed(c, L, GPE_FAM_REDUCE, 0);
+  finalize_kernel<<<1, 1024, 0, c->stream>>>(
+      c->d_partials, nblk, slot, op, scale, c->d_scal + out_index,
+      series ? c->d_series : nullptr, c->d_counter);
+  CU_CHECK(c, cudaGetLastError());
+  end_timed(c, L);
+  c->launches++;
+  return GPE_OK;
+}
+
+double cell_volume(const gpe_ctx* c) { return c->dx * c->dy * c->dz; }
+
+int read_scalars(gpe_ctx* c, double* dst, int first, int count) {
+  CU_CHECK(c, cudaMemcpyAsync(dst, c->d_scal + first, sizeof(double) * count,
+                              cudaMemcpyDeviceToHost, c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return GPE_OK;
+}
+
+int check_status(gpe_ctx* c) {
+  int st = 0;
+  CU_CHECK(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  if (st != 0) {
+    cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
+    return fail(c, GPE_ERR_TIMEOUT,
+                "device-side wait limit expired in a stage kernel");
+  }
+  return GPE_OK;
+}
+
+// --------------------------------------------------------------------------
+// Schemes.  Each function enqueues one full step; the fused final-stage norm
+// lands in the partials and is finalised into d_scal[0].
+
+int step_euler(gpe_ctx* c, cd dt) {
+  StageSpec s;
+  s.stencil = c->psi_id;
+  s.nout = c->prm.kahan ? 2 : 1;
+  s.out[0] = c->alt_id;
+  s.ghost_mask = 1;
+  s.ck[0] = dt;
+  s.family = GPE_FAM_STAGE_LAST;
+  if (c->prm.kahan) {
+    // delta = dt f(psi); compensated psi' = psi + delta, c updated in place
+    s.np = 1; s.pt[0] = c->c_id;
+    s.out[1] = c->c_id;
+    s.epi = EPI_KAHAN | EPI_NORM;
+  } else {
+    s.ca[0] = 1.0;
+    s.epi = EPI_NORM;
+  }
+  int rc = launch_stage(c, s);
+  if (rc) return rc;
+  std::swap(c->psi_id, c->alt_id);
+  return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
+}
+
+int step_rk2(gpe_ctx* c, cd dt) {
+  StageSpec s1;
+  s1.stencil = c->psi_id; s1.nout = 1; s1.out[0] = F_UA; s1.ghost_mask = 1;
+  s1.ca[0] = 1.0; s1.ck[0] = 0.5 * dt; s1.family = GPE_FAM_STAGE_FIRST;
+  int rc = launch_stage(c, s1);
+  if (rc) return rc;
+  StageSpec s2;
+  s2.stencil = F_UA; s2.out[0] = c->psi_id; s2.ghost_mask = 1;
+  s2.family = GPE_FAM_STAGE_LAST;
+  if (c->prm.kahan) {
+    s2.np = 2; s2.pt[0] = c->psi_id; s2.pt[1] = c->c_id;
+    s2.nout = 2; s2.out[1] = c->c_id;
+    s2.ck[0] = dt;
+    s2.epi = EPI_KAHAN | EPI_NORM;
+  } else {
+    s2.np = 1; s2.pt[0] = c->psi_id; s2.nout = 1;
+    s2.cb[0][0] = 1.0; s2.ck[0] = dt;
+    s2.epi = EPI_NORM;
+  }
+  rc = launch_stage(c, s2);
+  if (rc) return rc;
+  return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
+}
+
+int step_rk4(gpe_ctx* c, cd dt) {
+  const bool K = c->prm.kahan != 0;
+  // S1: u2 = psi + dt/2 f(psi); acc = [psi] + dt/6 f(psi)
+  StageSpec s1;
+  s1.stencil = c->psi_id; s1.nout = 2; s1.out[0] = F_UA; s1.out[1] = F_ACC;
+  s1.ghost_mask = 1; s1.ca[0] = 1.0; s1.ck[0] = 0.5 * dt;
+  s1.ca[1] = K ? 0.0 : 1.0; s1.ck[1] = dt / 6.0;
+  s1.family = GPE_FAM_STAGE_FIRST;
+  int rc = launch_stage(c, s1);
+  if (rc) return rc;
+  // S2: u3 = psi + dt/2 f(u2); acc += dt/3 f(u2)
+  StageSpec s2;
+  s2.stencil = F_UA; s2.np = 2; s2.pt[0] = c->psi_id; s2.pt[1] = F_ACC;
+  s2.nout = 2; s2.out[0] = F_UB; s2.out[1] = F_ACC; s2.ghost_mask = 1;
+  s2.cb[0][0] = 1.0; s2.ck[0] = 0.5 * dt;
+  s2.cb[1][1] = 1.0; s2.ck[1] = dt / 3.0;
+  s2.family = GPE_FAM_STAGE_MID;
+  rc = launch_stage(c, s2);
+  if (rc) return rc;
+  // S3: u4 = psi + dt f(u3); acc += dt/3 f(u3)
+  StageSpec s3 = s2;
+  s3.stencil = F_UB; s3.out[0] = F_UA; s3.ck[0] = dt;
+  rc = launch_stage(c, s3);
+  if (rc) return rc;
+  // S4: psi' = acc + dt/6 f(u4)   (Kahan: psi' = psi (+) (acc + dt/6 f))
+  StageSpec s4;
+  s4.stencil = F_UA; s4.out[0] = c->psi_id; s4.ghost_mask = 1;
+  s4.family = GPE_FAM_STAGE_LAST;
+  if (K) {
+    s4.np = 3; s4.pt[0] = c->psi_id; s4.pt[1] = F_ACC; s4.pt[2] = c->c_id;
+    s4.nout = 2; s4.out[1] = c->c_id;
+    s4.cb[0][1] = 1.0; s4.ck[0] = dt / 6.0;
+    s4.epi = EPI_KAHAN | EPI_NORM;
+  } else {
+    s4.np = 1; s4.pt[0] = F_ACC; s4.nout = 1;
+    s4.cb[0][0] = 1.0; s4.ck[0] = dt / 6.0;
+    s4.epi = EPI_NORM;
+  }
+  rc = launch_stage(c, s4);
+  if (rc) return rc;
+  return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
+}
+
+// rkck (src/solve.f90:248-378) with the psi_scal / errmax reduction of rkqs
+// (:176-190) fused into the last stage.  Writes the trial state to alt.
+int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
+  const bool K = c->prm.kahan != 0;
+  const int psi = c->psi_id;
+  const int stencils[6] = {psi, F_UA, F_UB, F_UA, F_UB, F_UA};
+  const int ks[5] = {F_K1, F_K2, F_K3, F_K4, F_K5};
+  const double B[5][5] = {{B21, 0, 0, 0, 0},
+                          {B31, B32, 0, 0, 0},
+                          {B41, B42, B43, 0, 0},
+                          {B51, B52, B53, B54, 0},
+                          {B61, B62, B63, B64, B65}};
+  int rc;
+  for (int st = 0; st < 5; st++) {
+    // stage st+1: k = dt f(u_st); u_{st+1} = psi + sum_j B[st][j] k_j
+    StageSpec s;
+    s.stencil = stencils[st];
+    s.nout = 2;
+    s.out[0] = ks[st];
+    s.out[1] = (st % 2 == 0) ? F_UA : F_UB;
+    s.ghost_mask = 2;
+    s.ck[0] = dt;
+    if (st == 0) {
+      s.np = 0;
+      s.ca[1] = 1.0;
+    } else {
+      s.np = st + 1;
+      s.pt[0] = psi;
+      s.cb[1][0] = 1.0;
+      for (int jj = 0; jj < st; jj++) {
+        s.pt[jj + 1] = ks[jj];
+        s.cb[1][jj + 1] = B[st][jj];
+      }
+    }
+    s.ck[1] = B[st][st] * dt;
+    s.family = st == 0 ? GPE_FAM_STAGE_FIRST : GPE_FAM_STAGE_MID;
+    rc = launch_stage(c, s);
+    if (rc) return rc;
+  }
+  // stage 6: psi_new = psi + c1 k1 + c3 k3 + c4 k4 + c6 dt f(u6)  (c2=c5=0)
+  //          err     = dc1 k1 + dc3 k3 + dc4 k4 + dc5 k5 + dc6 dt f(u6)
+  StageSpec s;
+  s.stencil = F_UA;
+  s.out[0] = c->alt_id;
+  s.ghost_mask = 1;
+  s.family = GPE_FAM_STAGE_LAST;
+  s.dt0 = dt0;
+  s.inv_absdt = 1.0 / std::abs(dt);
+  s.ck[0] = C6 * dt;
+  s.cek = DC6 * dt;
+  // pointwise slots: psi, k1, k3, k4, k5 [, c]  (the kernel takes psi from
+  // slot 0, k1 from slot 1 and the compensation from the last slot)
+  s.pt[0] = psi;
+  s.pt[1] = F_K1; s.pt[2] = F_K3; s.pt[3] = F_K4; s.pt[4] = F_K5;
+  s.cb[0][1] = C1; s.cb[0][2] = C3; s.cb[0][3] = C4;
+  s.ce[1] = DC1; s.ce[2] = DC3; s.ce[3] = DC4; s.ce[4] = DC5;
+  if (K) {
+    s.np = 6;
+    s.pt[5] = c->c_id;
+    s.nout = 2; s.out[1] = c->calt_id;
+    s.epi = EPI_KAHAN | EPI_NORM | EPI_ERR;
+  } else {
+    s.np = 5;
+    s.cb[0][0] = 1.0;
+    s.nout = 1;
+    s.epi = EPI_NORM | EPI_ERR;
+  }
+  rc = launch_stage(c, s);
+  if (rc) return rc;
+  rc = finalize(c, c->last_nblk, 1, 1, 1.0 / RK_EPS, 3, false);
+  if (rc) return rc;
+  return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
+}
+
+// rkqs (src/solve.f90:158-244) with device stages and host step control.
+int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
+  const double errcon = std::pow(5.0 / SAFETY, 1.0 / DT_INCREASE);
+  cd dt(tm->dt_re, tm->dt_im);
+  const cd dt0 = dt;
+  const bool real_time = c->prm.real_time != 0;
+  double errmax = 0.0;
+  int attempts = 0, underflow = 0;
+  for (;;) {
+    attempts++;
+    int rc = attempt_rkck(c, dt, dt0);
+    if (rc) return rc;
+    rc = read_scalars(c, &errmax, 3, 1);
+    if (rc) return rc;
+    if (!std::isfinite(errmax))
+      return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate");
+    if (errmax <= 1.0) break;
+    const cd dt_temp = SAFETY * dt * std::pow(errmax, DT_DECREASE);
+    const double mag = std::max(std::abs(dt_temp), 0.1 * std::abs(dt));
+    dt = real_time ? cd(mag, 0.0) : cd(0.0, -mag);
+    if (real_time && tm->t + dt.real() == tm->t) underflow = 1;
+    if (attempts > 10000)
+      return fail(c, GPE_ERR_UNDERFLOW, "rk45: step size control did not converge");
+  }
+  cd dt_next;
+  if (errmax > errcon)
+    dt_next = SAFETY * dt * std::pow(errmax, DT_INCREASE);
+  else
+    dt_next = 5.0 * dt;
+  tm->t = tm->t + dt.real();
+  if (info) {
+    info->errmax = errmax;
+    info->attempts = attempts;
+    info->underflow = underflow;
+    info->dt_did_re = dt.real();
+    info->dt_did_im = dt.imag();
+  }
+  dt = dt_next;
+  tm->im_t = tm->im_t + std::fabs(dt.imag());
+  tm->dt_re = dt.real();
+  tm->dt_im = dt.imag();
+  std::swap(c->psi_id, c->alt_id);
+  if (c->prm.kahan) std::swap(c->c_id, c->calt_id);
+  return GPE_OK;
+}
+
+int do_step(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
+  const cd dt(tm->dt_re, tm->dt_im);
+  int rc;
+  c->norm_valid = false;
+  switch (c->prm.scheme) {
+    case GPE_SCHEME_EULER: rc = step_euler(c, dt); break;
+    case GPE_SCHEME_RK2: rc = step_rk2(c, dt); break;
+    case GPE_SCHEME_RK4: rc = step_rk4(c, dt); break;
+    case GPE_SCHEME_RK45: rc = step_rk45(c, tm, info); break;
+    default:
+      return fail(c, GPE_ERR_SCHEME, "ERROR: Unrecognised time stepping scheme.");
+  }
+  if (rc) return rc;
+  if (c->prm.scheme != GPE_SCHEME_RK45) {
+    tm->t = tm->t + dt.real();
+    tm->im_t = tm->im_t + std::fabs(dt.imag());
+    if (info) {
+      info->errmax = 0.0;
+      info->attempts = 1;
+      info->underflow = 0;
+      info->dt_did_re = dt.real();
+      info->dt_did_im = dt.imag();
+    }
+  }
+  c->norm_valid = true;
+  return GPE_OK;
+}
+
+// --------------------------------------------------------------------------
+// Tables and allocation.
+
+int build_tables(gpe_ctx* c) {
+  const gpe_params& p = c->prm;
+  const int n[3] = {c->nx, c->ny, c->nz};
+  const std::vector<double>* crd[3] = {&c->x, &c->y, &c->z};
+  const double om[3] = {p.omx, p.omy, p.omz};
+  size_t total = 0;
+  for (int a = 0; a < 3; a++) {
+    c->tab_n[a] = (int)round_up((size_t)n[a], 64) + 64;
+    total += (size_t)c->tab_n[a];
+  }
+  // per axis: Vf, Df (float) + Vd, Dd, W, X (double)
+  const size_t bytes = total * (2 * sizeof(float) + 4 * sizeof(double));
+  CU_CHECK(c, cudaMalloc(&c->d_tables, bytes));
+  c->device_bytes += (int64_t)bytes;
+  std::vector<unsigned char> h(bytes, 0);
+  size_t off = 0;
+  auto take = [&](size_t nbytes) {
+    size_t o = off;
+    off += round_up(nbytes, 256);
+    return o;
+  };
+  // recompute offsets with alignment
+  off = 0;
+  size_t offs[3][6];
+  for (int a = 0; a < 3; a++) {
+    offs[a][0] = take(sizeof(float) * c->tab_n[a]);
+    offs[a][1] = take(sizeof(float) * c->tab_n[a]);
+    for (int k = 2; k < 6; k++) offs[a][k] = take(sizeof(double) * c->tab_n[a]);
+  }
+  if (off > bytes) {
+    cudaFree(c->d_tables);
+    c->device_bytes -= (int64_t)bytes;
+    CU_CHECK(c, cudaMalloc(&c->d_tables, off));
+    c->device_bytes += (int64_t)off;
+    h.assign(off, 0);
+  }
+  for (int a = 0; a < 3; a++) {
+    float* vf = reinterpret_cast<float*>(&h[offs[a][0]]);
+    float* df = reinterpret_cast<float*>(&h[offs[a][1]]);
+    double* vd = reinterpret_cast<double*>(&h[offs[a][2]]);
+    double* dd = reinterpret_cast<double*>(&h[offs[a][3]]);
+    double* w = reinterpret_cast<double*>(&h[offs[a][4]]);
+    double* xx = reinterpret_cast<double*>(&h[offs[a][5]]);
+    const std::vector<double>& X = *crd[a];
+    const int N = n[a];
+    // sponge edge a = x(nx-3) (src/solve.f90:397-409)
+    const double edge = X[N - 3];
+    for (int i = 0; i < N; i++) {
+      const double v = 0.5 * ((om[a] * om[a]) * (X[i] * X[i]));
+      const double d = p.diss_amp * (1.0 + std::tanh(X[i] - edge) * std::tanh(X[i] + edge));
+      vd[i] = v; vf[i] = (float)v;
+      dd[i] = d; df[i] = (float)d;
+      xx[i] = X[i];
+    }
+    // norm weights (src/variables.f90:713-823): x sums every term that
+    // names an index, y and z take the last matching assignment.
+    if (a == 0) {
+      for (int i = 0; i < N; i++) w[i] = 0.0;
+      w[0] += W1; w[1] += W2; w[2] += W3;
+      for (int i = 3; i <= N - 4; i++) w[i] += 1.0;
+      w[N - 3] += W3; w[N - 2] += W2; w[N - 1] += W1;
+    } else {
+      for (int i = 0; i < N; i++) {
+        double t = 1.0;
+        if (i == 0) t = W1;
+        if (i == 1) t = W2;
+        if (i == 2) t = W3;
+        if (i == N - 3) t = W3;
+        if (i == N - 2) t = W2;
+        if (i == N - 1) t = W1;
+        w[i] = t;
+      }
+    }
+  }
+  CU_CHECK(c, cudaMemcpy(c->d_tables, h.data(), h.size(), cudaMemcpyHostToDevice));
+  unsigned char* base = static_cast<unsigned char*>(c->d_tables);
+  for (int a = 0; a < 3; a++) {
+    c->tabVf[a] = reinterpret_cast<float*>(base + offs[a][0]);
+    c->tabDf[a] = reinterpret_cast<float*>(base + offs[a][1]);
+    c->tabVd[a] = reinterpret_cast<double*>(base + offs[a][2]);
+    c->tabDd[a] = reinterpret_cast<double*>(base + offs[a][3]);
+    c->tabW[a] = reinterpret_cast<double*>(base + offs[a][4]);
+    c->tabX[a] = reinterpret_cast<double*>(base + offs[a][5]);
+  }
+  return GPE_OK;
+}
+
+int alloc_field(gpe_ctx* c, int id) {
+  const size_t bytes = c->npad * (size_t)c->es;
+  cudaError_t e = cudaMalloc(&c->fld[id], bytes);
+  if (e != cudaSuccess) {
+    c->fld[id] = nullptr;
+    cudaGetLastError();
+    return fail(c, GPE_ERR_OOM, "cudaMalloc of a field failed: " +
+                                    std::string(cudaGetErrorString(e)));
+  }
+  c->device_bytes += (int64_t)bytes;
+  CU_CHECK(c, cudaMemset(c->fld[id], 0, bytes));
+  return GPE_OK;
+}
+
+int stage_in(gpe_ctx* c, const void* src, int elem_bytes, bool device) {
+  const size_t bytes = c->nint * (size_t)elem_bytes;
+  CU_CHECK(c, cudaMemcpyAsync(c->d_stage, src, bytes,
+                              device ? cudaMemcpyDeviceToDevice
+                                     : cudaMemcpyHostToDevice,
+                              c->stream));
+  Launch L{};
+  begin_timed(c, L, GPE_FAM_COPY, (int64_t)c->nint);
+  const Geom g = geom(c);
+  const int nb = elementwise_blocks(c->nint);
+  void* dst = c->fld[c->psi_id];
+  if (c->es == 8) {
+    if (elem_bytes == 8)
+      unpack_kernel<float, float><<<nb, 256, 0, c->stream>>>(
+          (const float*)c->d_stage, (float*)dst, g);
+    else
+      unpack_kernel<float, double><<<nb, 256, 0, c->stream>>>(
+          (const double*)c->d_stage, (float*)dst, g);
+  } else {
+    if (elem_bytes == 8)
+      unpack_kernel<double, float><<<nb, 256, 0, c->stream>>>(
+          (const float*)c->d_stage, (double*)dst, g);
+    else
+      unpack_kernel<double, double><<<nb, 256, 0, c->stream>>>(
+          (const double*)c->d_stage, (double*)dst, g);
+  }
+  CU_CHECK(c, cudaGetLastError());
+  end_timed(c, L);
+  c->launches++;
+  if (c->prm.kahan && c->fld[c->c_id])
+    CU_CHECK(c, cudaMemsetAsync(c->fld[c->c_id], 0, c->npad * (size_t)c->es,
+                                c->stream));
+  c->norm_valid = false;
+  return GPE_OK;
+}
+
+int stage_out(gpe_ctx* c, int field, void* dst, int elem_bytes, bool device) {
+  Launch L{};
+  begin_timed(c, L, GPE_FAM_COPY, (int64_t)c->nint);
+  const Geom g = geom(c);
+  const int nb = elementwise_blocks(c->nint);
+  const void* src = c->fld[field];
+  if (c->es == 8) {
+    if (elem_bytes == 8)
+      pack_kernel<float, float><<<nb, 256, 0, c->stream>>>(
+          (const float*)src, (float*)c->d_stage, g);
+    else
+      pack_kernel<float, double><<<nb, 256, 0, c->stream>>>(
+          (const float*)src, (double*)c->d_stage, g);
+  } else {
+    if (elem_bytes == 8)
+      pack_kernel<double, float><<<nb, 256, 0, c->stream>>>(
+          (const double*)src, (float*)c->d_stage, g);
+    else
+      pack_kernel<double, double><<<nb, 256, 0, c->stream>>>(
+          (const double*)src, (double*)c->d_stage, g);
+  }
+  CU_CHECK(c, cudaGetLastError());
+  end_timed(c, L);
+  c->launches++;
+  CU_CHECK(c, cudaMemcpyAsync(dst, c->d_stage, c->nint * (size_t)elem_bytes,
+                              device ? cudaMemcpyDeviceToDevice
+                                     : cudaMemcpyDeviceToHost,
+                              c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return GPE_OK;
+}
+
+int check_ctx(gpe_ctx* c) {
+  if (!c) return GPE_ERR_INVALID;
+  CU_CHECK(c, cudaSetDevice(c->dev));
+  return GPE_OK;
+}
+
+int check_elem(gpe_ctx* c, int elem_bytes, const void* ptr) {
+  if (elem_bytes != 8 && elem_bytes != 16)
+    return fail(c, GPE_ERR_INVALID, "elem_bytes must be 8 or 16");
+  if (!ptr) return fail(c, GPE_ERR_INVALID, "null array");
+  return GPE_OK;
+}
+
+}  // namespace
+
+// ==========================================================================
+// C-ABI
+
+extern "C" {
+
+int32_t gpe_gpu_abi_version(void) { return GPE_GPU_ABI_VERSION; }
+
+void gpe_gpu_default_params(gpe_params* p, int32_t nx, int32_t ny,
+                            int32_t nz) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->struct_size = (int32_t)sizeof(gpe_params);
+  p->nx = nx; p->ny = ny; p->nz = nz;
+  p->xr = p->yr = p->zr = 1.0;
+  p->scheme = GPE_SCHEME_RK4;
+  p->eqn_to_solve = 4;
+  p->bcs = 1;
+  p->order = 2;
+  p->real_time = 1;
+  p->precision = 16;
+  p->scal = 1.0; p->g = 1.0; p->mu = 1.0; p->nn = 1.0;
+}
+
+int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
+  if (!out) return fail(nullptr, GPE_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (!prm) return fail(nullptr, GPE_ERR_INVALID, "params is null");
+  if (prm->struct_size != (int32_t)sizeof(gpe_params))
+    return fail(nullptr, GPE_ERR_INVALID, "gpe_params struct_size mismatch");
+  const gpe_params& p = *prm;
+  if (p.nx < 6 || p.ny < 6 || p.nz < 6)
+    return fail(nullptr, GPE_ERR_INVALID, "nx, ny, nz must be >= 6");
+  if (p.order != 2 && p.order != 4)
+    return fail(nullptr, GPE_ERR_INVALID, "order must be 2 or 4");
+  if (p.bcs != 1 && p.bcs != 2)
+    return fail(nullptr, GPE_ERR_INVALID, "bcs must be 1 or 2");
+  if (p.eqn_to_solve < 1 || p.eqn_to_solve > 4)
+    return fail(nullptr, GPE_ERR_INVALID, "eqn_to_solve must be 1..4");
+  if (p.precision != 8 && p.precision != 16)
+    return fail(nullptr, GPE_ERR_INVALID, "precision must be 8 or 16");
+  if (p.kahan && p.precision != 8)
+    return fail(nullptr, GPE_ERR_INVALID, "kahan applies to precision 8 only");
+  if (p.tile_y != 0 && p.tile_y != 4 && p.tile_y != 8)
+    return fail(nullptr, GPE_ERR_INVALID, "tile_y must be 0, 4 or 8");
+  if (p.xr <= 0 || p.yr <= 0 || p.zr <= 0)
+    return fail(nullptr, GPE_ERR_INVALID, "xr, yr, zr must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) {
+    cudaGetLastError();
+    return fail(nullptr, GPE_ERR_NODEVICE, "no CUDA device available");
+  }
+  cudaDeviceProp dp;
+  if (cudaGetDeviceProperties(&dp, p.device) != cudaSuccess || dp.major != 10)
+    return fail(nullptr, GPE_ERR_NODEVICE, "device is not sm_100 (B200)");
+
+  gpe_ctx* c = new gpe_ctx();
+  c->prm = p;
+  c->dev = p.device;
+  memset(&c->acc_timing, 0, sizeof(c->acc_timing));
+  auto bail = [&](int rc) {
+    g_last_create_error = c->err;
+    gpe_gpu_destroy(c);
+    return rc;
+  };
+  if (cudaSetDevice(c->dev) != cudaSuccess) {
+    c->err = "cudaSetDevice failed";
+    return bail(GPE_ERR_CUDA);
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    c->err = "cudaStreamCreate failed";
+    return bail(GPE_ERR_CUDA);
+  }
+  c->nx = p.nx; c->ny = p.ny; c->nz = p.nz;
+  c->Nx = (int)round_up((size_t)p.nx + 4, 4);
+  c->Ny = p.ny + 4;
+  c->Nz = p.nz + 4;
+  c->npad = (size_t)c->Nx * c->Ny * c->Nz;
+  c->nint = (size_t)p.nx * p.ny * p.nz;
+  c->es = p.precision;
+  // get_grid, src/ic.f90:32-69
+  c->dx = (p.xr - (-p.xr)) / (double)(p.nx - 1);
+  c->dy = (p.yr - (-p.yr)) / (double)(p.ny - 1);
+  c->dz = (p.zr - (-p.zr)) / (double)(p.nz - 1);
+  c->x.resize(p.nx); c->y.resize(p.ny); c->z.resize(p.nz);
+  for (int i = 0; i < p.nx; i++) c->x[i] = -p.xr + (double)i * c->dx;
+  for (int j = 0; j < p.ny; j++) c->y[j] = -p.yr + (double)j * c->dy;
+  for (int k = 0; k < p.nz; k++) c->z[k] = -p.zr + (double)k * c->dz;
+
+  int rc = build_tables(c);
+  if (rc) return bail(rc);
+  std::vector<int> need = {F_PSI, F_ALT};
+  switch (p.scheme) {
+    case GPE_SCHEME_RK2: need.push_back(F_UA); break;
+    case GPE_SCHEME_RK4:
+      need.insert(need.end(), {F_UA, F_UB, F_ACC});
+      break;
+    case GPE_SCHEME_RK45:
+      need.insert(need.end(), {F_UA, F_UB, F_K1, F_K2, F_K3, F_K4, F_K5});
+      break;
+    default: break;
+  }
+  if (p.kahan) {
+    need.push_back(F_C);
+    if (p.scheme == GPE_SCHEME_RK45) need.push_back(F_CALT);
+  }
+  for (int id : need) {
+    rc = alloc_field(c, id);
+    if (rc) return bail(rc);
+  }
+  // partials: upper bound over every launch shape (TY >= 4, zchunk >= 1)
+  const size_t ntiles_max = (size_t)((p.nx + TX - 1) / TX) * ((p.ny + 3) / 4);
+  c->partials_cap = std::max<size_t>(ntiles_max * (size_t)p.nz, 148 * 16);
+  if (cudaMalloc(&c->d_partials, 2 * sizeof(double) * c->partials_cap) != cudaSuccess ||
+      cudaMalloc(&c->d_scal, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_counter, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->d_stage, c->nint * 16) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "cudaMalloc of scratch buffers failed";
+    return bail(GPE_ERR_OOM);
+  }
+  c->device_bytes += (int64_t)(2 * sizeof(double) * c->partials_cap +
+                               16 * sizeof(double) + 2 * sizeof(int) + c->nint * 16);
+  cudaMemset(c->d_scal, 0, 16 * sizeof(double));
+  cudaMemset(c->d_status, 0, sizeof(int));
+  cudaMemset(c->d_counter, 0, sizeof(int));
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    c->err = "device synchronisation failed during create";
+    return bail(GPE_ERR_CUDA);
+  }
+  *out = c;
+  return GPE_OK;
+}
+
+void gpe_gpu_destroy(gpe_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < F_COUNT; i++)
+    if (c->fld[i]) cudaFree(c->fld[i]);
+  if (c->d_tables) cudaFree(c->d_tables);
+  if (c->d_partials) cudaFree(c->d_partials);
+  if (c->d_scal) cudaFree(c->d_scal);
+  if (c->d_series) cudaFree(c->d_series);
+  if (c->d_counter) cudaFree(c->d_counter);
+  if (c->d_status) cudaFree(c->d_status);
+  if (c->d_stage) cudaFree(c->d_stage);
+  for (auto& L : c->timed) {
+    cudaEventDestroy(L.a);
+    cudaEventDestroy(L.b);
+  }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* gpe_gpu_last_error(const gpe_ctx* c) {
+  if (!c) return g_last_create_error.c_str();
+  return c->err.c_str();
+}
+
+int gpe_gpu_grid(const gpe_ctx* c, double* x, double* y, double* z) {
+  if (!c) return GPE_ERR_INVALID;
+  if (x) memcpy(x, c->x.data(), sizeof(double) * c->nx);
+  if (y) memcpy(y, c->y.data(), sizeof(double) * c->ny);
+  if (z) memcpy(z, c->z.data(), sizeof(double) * c->nz);
+  return GPE_OK;
+}
+
+int gpe_gpu_set_state(gpe_ctx* c, const void* psi, int32_t elem_bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, psi);
+  if (rc) return rc;
+  rc = stage_in(c, psi, elem_bytes, false);
+  if (rc) return rc;
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return GPE_OK;
+}
+
+int gpe_gpu_get_state(gpe_ctx* c, void* psi, int32_t elem_bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, psi);
+  if (rc) return rc;
+  return stage_out(c, c->psi_id, psi, elem_bytes, false);
+}
+
+int gpe_gpu_set_state_device(gpe_ctx* c, const void* psi, int32_t elem_bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, psi);
+  if (rc) return rc;
+  rc = stage_in(c, psi, elem_bytes, true);
+  if (rc) return rc;
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return GPE_OK;
+}
+
+int gpe_gpu_get_state_device(gpe_ctx* c, void* psi, int32_t elem_bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, psi);
+  if (rc) return rc;
+  return stage_out(c, c->psi_id, psi, elem_bytes, true);
+}
+
+int gpe_gpu_solver(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!tm) return fail(c, GPE_ERR_INVALID, "tm is null");
+  rc = do_step(c, tm, info);
+  if (rc) return rc;
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int gpe_gpu_solver_host(gpe_ctx* c, const void* var_in, void* var_out,
+                        int32_t elem_bytes, gpe_time* tm, gpe_step_info* info) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, var_in);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, var_out);
+  if (rc) return rc;
+  if (!tm) return fail(c, GPE_ERR_INVALID, "tm is null");
+  rc = stage_in(c, var_in, elem_bytes, false);
+  if (rc) return rc;
+  rc = do_step(c, tm, info);
+  if (rc) return rc;
+  rc = stage_out(c, c->psi_id, var_out, elem_bytes, false);
+  if (rc) return rc;
+  return check_status(c);
+}
+
+int gpe_gpu_advance(gpe_ctx* c, int64_t nsteps, gpe_time* tm, double* norms) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!tm || nsteps < 0) return fail(c, GPE_ERR_INVALID, "bad advance arguments");
+  if ((size_t)nsteps > c->series_cap) {
+    if (c->d_series) cudaFree(c->d_series);
+    c->d_series = nullptr;
+    const size_t cap = std::max<size_t>((size_t)nsteps, 1024);
+    CU_CHECK(c, cudaMalloc(&c->d_series, cap * sizeof(double)));
+    c->series_cap = cap;
+  }
+  CU_CHECK(c, cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
+  for (int64_t s = 0; s < nsteps; s++) {
+    rc = do_step(c, tm, nullptr);
+    if (rc) return rc;
+    // copy the fused norm into the per-step series
+    CU_CHECK(c, cudaMemcpyAsync(c->d_series + s, c->d_scal, sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+    tm->p += 1;
+  }
+  if (norms && nsteps > 0)
+    CU_CHECK(c, cudaMemcpyAsync(norms, c->d_series, sizeof(double) * nsteps,
+                                cudaMemcpyDeviceToHost, c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int gpe_gpu_norm(gpe_ctx* c, double* norm) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!norm) return fail(c, GPE_ERR_INVALID, "norm is null");
+  if (!c->norm_valid) {
+    const Geom g = geom(c);
+    const int nb = elementwise_blocks(c->nint);
+    Launch L{};
+    begin_timed(c, L, GPE_FAM_REDUCE, (int64_t)c->nint);
+    if (c->es == 8)
+      norm_kernel<float><<<nb, 256, 0, c->stream>>>(
+          (const float*)c->fld[c->psi_id], g, c->tabW[0], c->tabW[1], c->tabW[2],
+          c->d_partials);
+    else
+      norm_kernel<double><<<nb, 256, 0, c->stream>>>(
+          (const double*)c->fld[c->psi_id], g, c->tabW[0], c->tabW[1], c->tabW[2],
+          c->d_partials);
+    CU_CHECK(c, cudaGetLastError());
+    end_timed(c, L);
+    c->launches++;
+    rc = finalize(c, nb, 0, 0, cell_volume(c), 0, false);
+    if (rc) return rc;
+    c->norm_valid = true;
+  }
+  rc = read_scalars(c, norm, 0, 1);
+  if (rc) return rc;
+  if (!std::isfinite(*norm)) return fail(c, GPE_ERR_NAN, "non-finite norm");
+  return GPE_OK;
+}
+
+int gpe_gpu_energy(gpe_ctx* c, double* E, double* H4) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!E) return fail(c, GPE_ERR_INVALID, "E is null");
+  StageSpec s;
+  s.stencil = c->psi_id;
+  s.epi = EPI_ENERGY;
+  s.family = GPE_FAM_ENERGY;
+  rc = launch_stage(c, s);
+  if (rc) return rc;
+  const int nb = c->last_nblk;
+  rc = finalize(c, nb, 0, 0, cell_volume(c), 1, false);
+  if (rc) return rc;
+  rc = finalize(c, nb, 1, 0, cell_volume(c), 2, false);
+  if (rc) return rc;
+  double v[2];
+  rc = read_scalars(c, v, 1, 2);
+  if (rc) return rc;
+  *E = v[0];
+  if (H4) *H4 = v[1];
+  return check_status(c);
+}
+
+int gpe_gpu_renormalise(gpe_ctx* c, double norm) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!(norm > 0.0)) return fail(c, GPE_ERR_INVALID, "norm must be positive");
+  const size_t n = c->npad * 2;
+  const int nb = elementwise_blocks(n);
+  Launch L{};
+  begin_timed(c, L, GPE_FAM_COPY, (int64_t)c->nint);
+  if (c->es == 8)
+    scale_kernel<float><<<nb, 256, 0, c->stream>>>((float*)c->fld[c->psi_id], n,
+                                                     std::sqrt(c->prm.nn), std::sqrt(norm));
+  else
+    scale_kernel<double><<<nb, 256, 0, c->stream>>>((double*)c->fld[c->psi_id], n,
+                                                      std::sqrt(c->prm.nn), std::sqrt(norm));
+  CU_CHECK(c, cudaGetLastError());
+  end_timed(c, L);
+  c->launches++;
+  c->norm_valid = false;
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return GPE_OK;
+}
+
+static int rhs_like(gpe_ctx* c, void* out, int32_t elem_bytes, bool lap) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, out);
+  if (rc) return rc;
+  StageSpec s;
+  s.stencil = c->psi_id;
+  s.nout = 1;
+  s.out[0] = c->alt_id;
+  s.ck[0] = 1.0;
+  s.epi = lap ? EPI_LAP : 0;
+  rc = launch_stage(c, s);
+  if (rc) return rc;
+  rc = stage_out(c, c->alt_id, out, elem_bytes, false);
+  if (rc) return rc;
+  return check_status(c);
+}
+
+int gpe_gpu_rhs(gpe_ctx* c, void* out, int32_t elem_bytes) {
+  return rhs_like(c, out, elem_bytes, false);
+}
+
+int gpe_gpu_laplacian(gpe_ctx* c, void* out, int32_t elem_bytes) {
+  return rhs_like(c, out, elem_bytes, true);
+}
+
+int gpe_gpu_set_real_time(gpe_ctx* c, int32_t real_time) {
+  if (!c) return GPE_ERR_INVALID;
+  c->prm.real_time = real_time ? 1 : 0;
+  return GPE_OK;
+}
+
+int gpe_gpu_set_timing(gpe_ctx* c, int32_t on) {
+  if (!c) return GPE_ERR_INVALID;
+  c->timing = on != 0;
+  return GPE_OK;
+}
+
+int gpe_gpu_get_timing(gpe_ctx* c, gpe_timing* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  for (auto& L : c->timed) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, L.a, L.b);
+    if (L.family >= 0 && L.family < GPE_TIMING_FAMILIES) {
+      c->acc_timing.ms[L.family] += ms;
+      c->acc_timing.launches[L.family] += 1;
+      c->acc_timing.sites[L.family] += L.sites;
+    }
+    c->ev_pool.push_back(L.a);
+    c->ev_pool.push_back(L.b);
+  }
+  c->timed.clear();
+  if (out) *out = c->acc_timing;
+  memset(&c->acc_timing, 0, sizeof(c->acc_timing));
+  return GPE_OK;
+}
+
+int64_t gpe_gpu_launch_count(const gpe_ctx* c) { return c ? c->launches : -1; }
+
+int64_t gpe_gpu_device_bytes(const gpe_ctx* c) { return c ? c->device_bytes : -1; }
+
+void* gpe_gpu_stream(const gpe_ctx* c) {
+  return c ? static_cast<void*>(c->stream) : nullptr;
+}
+
+void* gpe_gpu_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void gpe_gpu_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

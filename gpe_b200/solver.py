@@ -1,0 +1,284 @@
+"""Host-side mirror of the reference solver module over the C-ABI.
+
+The reference exposes its hot path as Fortran module procedures operating on
+module globals (src/solve.f90:21 ``solver``; src/variables.f90 ``get_norm``,
+``energy``, ``renormalise``; globals in src/parameters.f90).  ``GpeSolver``
+keeps the same names and argument meaning, with the globals held on the
+object (``t``, ``im_t``, ``dt``, ``p``) and psi resident on the GPU.
+
+Arrays are the reference's interior layout: complex, x fastest, i.e. numpy
+shape (nz, ny, nx) in C order.  Errors raise ``GpeError`` where the
+reference would call emergency_stop (src/error.f90:24-46).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from ._lib import (GpeError, GpeParamsC, GpeStepInfoC, GpeTimeC, GpeTimingC, SCHEMES,
+                   TIMING_FAMILIES, check, lib)
+
+
+@dataclass
+class GpeParams:
+    """run_params / eqn_params (src/parameters.f90:24-55) plus the grid and
+    storage form.  ``precision`` 16 = complex128, 8 = complex64."""
+    nx: int
+    ny: int
+    nz: int
+    xr: float = 1.0
+    yr: float = 1.0
+    zr: float = 1.0
+    scheme: str = "rk4"
+    eqn_to_solve: int = 4
+    bcs: int = 1
+    order: int = 2
+    real_time: bool = True
+    precision: int = 16
+    Urhs: float = 0.0
+    diss_amp: float = 0.0
+    scal: float = 1.0
+    g: float = 1.0
+    mu: float = 1.0
+    nn: float = 1.0
+    omx: float = 0.0
+    omy: float = 0.0
+    omz: float = 0.0
+    kahan: bool = False
+    device: int = 0
+    tile_y: int = 0
+    zchunk: int = 0
+
+    def to_c(self) -> GpeParamsC:
+        c = GpeParamsC()
+        lib().gpe_gpu_default_params(ctypes.byref(c), self.nx, self.ny, self.nz)
+        for f in fields(self):
+            v = getattr(self, f.name)
+            if f.name == "scheme":
+                if v not in SCHEMES:
+                    # the reference fails only when solver() is called
+                    # (src/solve.f90:47-49); keep an invalid code for that
+                    v = 99
+                else:
+                    v = SCHEMES[v]
+            elif isinstance(v, bool):
+                v = int(v)
+            setattr(c, f.name, v)
+        return c
+
+
+def _as_host(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class GpeSolver:
+    """One resident run on one B200 (a ``gpe_ctx``)."""
+
+    def __init__(self, prm: GpeParams, t: float = 0.0, im_t: float = 0.0, p: int = 0,
+                 dt: complex | None = None, tau: float | None = None):
+        self.prm = prm
+        self._ctx = ctypes.c_void_p()
+        cp = prm.to_c()
+        check(lib().gpe_gpu_create(ctypes.byref(cp), ctypes.byref(self._ctx)), None)
+        self.shape = (prm.nz, prm.ny, prm.nx)
+        self.t, self.im_t, self.p = float(t), float(im_t), int(p)
+        if dt is None:
+            # src/gpe.f90:76-80
+            tau = 0.0 if tau is None else float(tau)
+            dt = complex(tau, 0.0) if prm.real_time else complex(0.0, -tau)
+        self.dt = complex(dt)
+        self.last_info = None
+
+    # ---- lifetime -------------------------------------------------------
+    def close(self) -> None:
+        if self._ctx:
+            lib().gpe_gpu_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    # ---- state ------------------------------------------------------------
+    def _elem(self, dtype) -> int:
+        return 16 if np.dtype(dtype) == np.complex128 else 8
+
+    def set_state(self, psi) -> None:
+        """Load psi (numpy host array or CUDA torch tensor, interior layout)."""
+        if hasattr(psi, "is_cuda") and psi.is_cuda:
+            t = psi.contiguous()
+            eb = 16 if str(t.dtype) == "torch.complex128" else 8
+            check(lib().gpe_gpu_set_state_device(self._ctx, ctypes.c_void_p(t.data_ptr()), eb),
+                  self._ctx)
+            return
+        a = np.asarray(psi)
+        if a.dtype not in (np.complex64, np.complex128):
+            a = a.astype(np.complex128)
+        a = np.ascontiguousarray(a)
+        if a.shape != self.shape:
+            raise GpeError(1, f"state shape {a.shape} != {self.shape}")
+        check(lib().gpe_gpu_set_state(self._ctx, a.ctypes.data_as(ctypes.c_void_p),
+                                      self._elem(a.dtype)), self._ctx)
+
+    def get_state(self, dtype=np.complex128) -> np.ndarray:
+        out = np.empty(self.shape, dtype=dtype)
+        check(lib().gpe_gpu_get_state(self._ctx, out.ctypes.data_as(ctypes.c_void_p),
+                                      self._elem(dtype)), self._ctx)
+        return out
+
+    def get_state_device(self, out) -> None:
+        """Copy the state into a contiguous CUDA torch tensor (complex64/128)."""
+        eb = 16 if str(out.dtype) == "torch.complex128" else 8
+        check(lib().gpe_gpu_get_state_device(self._ctx, ctypes.c_void_p(out.data_ptr()), eb),
+              self._ctx)
+
+    # ---- the reference's hot-path procedures --------------------------------
+    def _tm(self) -> GpeTimeC:
+        return GpeTimeC(self.t, self.im_t, self.dt.real, self.dt.imag, self.p, 0)
+
+    def _untm(self, tm: GpeTimeC) -> None:
+        self.t, self.im_t, self.p = tm.t, tm.im_t, tm.p
+        self.dt = complex(tm.dt_re, tm.dt_im)
+
+    def solver(self) -> GpeStepInfoC:
+        """solver(var_in, var_out) (src/solve.f90:25-53) on the resident psi;
+        updates t, im_t (and dt for rk45) like the reference."""
+        tm = self._tm()
+        info = GpeStepInfoC()
+        check(lib().gpe_gpu_solver(self._ctx, ctypes.byref(tm), ctypes.byref(info)), self._ctx)
+        self._untm(tm)
+        self.last_info = info
+        return info
+
+    def solver_host(self, var_in: np.ndarray) -> np.ndarray:
+        """Literal host-array form: returns var_out for var_in."""
+        a = np.ascontiguousarray(var_in)
+        out = np.empty_like(a)
+        tm = self._tm()
+        info = GpeStepInfoC()
+        check(lib().gpe_gpu_solver_host(self._ctx, a.ctypes.data_as(ctypes.c_void_p),
+                                        out.ctypes.data_as(ctypes.c_void_p),
+                                        self._elem(a.dtype), ctypes.byref(tm),
+                                        ctypes.byref(info)), self._ctx)
+        self._untm(tm)
+        self.last_info = info
+        return out
+
+    def advance(self, nsteps: int) -> np.ndarray:
+        """nsteps fixed-step solver() calls with the per-step norm."""
+        norms = np.zeros(max(nsteps, 1), dtype=np.float64)
+        tm = self._tm()
+        check(lib().gpe_gpu_advance(self._ctx, int(nsteps), ctypes.byref(tm),
+                                    norms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              self._ctx)
+        self._untm(tm)
+        return norms[:nsteps]
+
+    def get_norm(self) -> float:
+        """get_norm (src/variables.f90:537-559)."""
+        v = ctypes.c_double()
+        check(lib().gpe_gpu_norm(self._ctx, ctypes.byref(v)), self._ctx)
+        return v.value
+
+    def energy(self) -> tuple[float, float]:
+        """energy (src/variables.f90:563-587) -> (E, H4)."""
+        e, h = ctypes.c_double(), ctypes.c_double()
+        check(lib().gpe_gpu_energy(self._ctx, ctypes.byref(e), ctypes.byref(h)), self._ctx)
+        return e.value, h.value
+
+    def renormalise(self, norm: float) -> None:
+        """renormalise (src/variables.f90:698-709)."""
+        check(lib().gpe_gpu_renormalise(self._ctx, float(norm)), self._ctx)
+
+    def rhs(self, dtype=np.complex128) -> np.ndarray:
+        """get_rhs (src/solve.f90:382-440) of the resident psi."""
+        out = np.empty(self.shape, dtype=dtype)
+        check(lib().gpe_gpu_rhs(self._ctx, out.ctypes.data_as(ctypes.c_void_p),
+                                self._elem(dtype)), self._ctx)
+        return out
+
+    def laplacian(self, dtype=np.complex128) -> np.ndarray:
+        out = np.empty(self.shape, dtype=dtype)
+        check(lib().gpe_gpu_laplacian(self._ctx, out.ctypes.data_as(ctypes.c_void_p),
+                                      self._elem(dtype)), self._ctx)
+        return out
+
+    def set_real_time(self, on: bool) -> None:
+        check(lib().gpe_gpu_set_real_time(self._ctx, 1 if on else 0), self._ctx)
+        self.prm.real_time = bool(on)
+
+    def grid(self):
+        x = np.zeros(self.prm.nx); y = np.zeros(self.prm.ny); z = np.zeros(self.prm.nz)
+        P = ctypes.POINTER(ctypes.c_double)
+        check(lib().gpe_gpu_grid(self._ctx, x.ctypes.data_as(P), y.ctypes.data_as(P),
+                                 z.ctypes.data_as(P)), self._ctx)
+        return x, y, z
+
+    # ---- instrumentation ------------------------------------------------------
+    def set_timing(self, on: bool) -> None:
+        check(lib().gpe_gpu_set_timing(self._ctx, 1 if on else 0), self._ctx)
+
+    def timing(self) -> dict:
+        t = GpeTimingC()
+        check(lib().gpe_gpu_get_timing(self._ctx, ctypes.byref(t)), self._ctx)
+        return {name: {"ms": t.ms[i], "launches": int(t.launches[i]), "sites": int(t.sites[i])}
+                for i, name in enumerate(TIMING_FAMILIES)}
+
+    def launch_count(self) -> int:
+        return int(lib().gpe_gpu_launch_count(self._ctx))
+
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer."""
+        return int(lib().gpe_gpu_stream(self._ctx) or 0)
+
+    def device_bytes(self) -> int:
+        return int(lib().gpe_gpu_device_bytes(self._ctx))
+
+
+def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool = False,
+             record=None):
+    """The per-step bookkeeping of the reference time loop (src/gpe.f90:134-278)
+    with an explicit step count: solver, get_norm + relnorm (equation 4),
+    imaginary-to-real switch at relnorm < 1e-12 (:251-268), renormalise.
+    Returns the list of (t, im_t, norm, relnorm) after each step."""
+    prm = s.prm
+    out = [] if record is None else record
+    prev_norm = 1.0
+    if prm.eqn_to_solve == 4 and not prm.real_time:
+        prev_norm = s.get_norm()
+        if renorm:
+            s.renormalise(prev_norm)
+    norm = 0.0
+    for _ in range(nsteps):
+        s.solver()
+        relnorm = 0.0
+        if prm.eqn_to_solve == 4:
+            norm = s.get_norm()
+            relnorm = abs((norm - prev_norm) / prev_norm)
+            out.append((s.t, s.im_t, norm, relnorm))
+        if prm.eqn_to_solve == 4 and not prm.real_time:
+            if relnorm < 1e-12:
+                if stop_imag:
+                    break
+                s.set_real_time(True)
+                s.im_t = 0.0
+                s.dt = complex(abs(s.dt.imag), abs(s.dt.real))
+            if renorm:
+                s.renormalise(norm)
+        prev_norm = norm
+        s.p += 1
+    return out

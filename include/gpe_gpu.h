@@ -1,0 +1,216 @@
+/*
+ * gpe_gpu.h -- C-ABI of the B200 (sm_100a) Gross-Pitaevskii time stepper.
+ *
+ * This is the drop-in boundary for the reference solver's hot path
+ * (liangjj/gpe, Fortran 90 + MPI).  The reference reaches that path through
+ * the module procedure solver(var_in, var_out) (src/solve.f90:25-53, called
+ * from src/gpe.f90:228) plus get_norm / energy / renormalise
+ * (src/variables.f90:537-587, 698-709).  Those procedures read and write
+ * module globals (dt, t, im_t, p, scheme, eqn_to_solve, bcs, order, dx..,
+ * g, mu, omx.., Urhs, diss_amp: src/parameters.f90:24-127); here the
+ * globals are the explicit gpe_params / gpe_time structs.
+ *
+ * Plain C types only: no C++ types, exceptions or torch objects cross this
+ * boundary.  A context owns all device memory; psi stays resident on the GPU
+ * between calls and crosses PCIe only in set_state / get_state (or the
+ * host-array form gpe_gpu_solver_host).  Every call is stream-ordered on the
+ * context's own CUDA stream and has completed when it returns.  One context
+ * per host thread.
+ *
+ * Host arrays are the reference's interior layout: complex, Fortran order,
+ * x fastest, psi[(k*ny + j)*nx + i]; elem_bytes 8 = complex64 (single
+ * precision `pr`), 16 = complex128 (double precision `pr`,
+ * src/parameters.in:21-23).
+ *
+ * Status codes: 0 = success, otherwise one of GPE_ERR_*; the message is
+ * available from gpe_gpu_last_error().  The reference has no status codes --
+ * it calls emergency_stop (src/error.f90:24-46); a driver maps a non-zero
+ * status to that behaviour.
+ */
+#ifndef GPE_GPU_H
+#define GPE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPE_GPU_ABI_VERSION 1
+
+/* status codes */
+#define GPE_OK 0
+#define GPE_ERR_INVALID 1    /* bad argument or configuration */
+#define GPE_ERR_SCHEME 2     /* 'ERROR: Unrecognised time stepping scheme.'
+                                (src/solve.f90:47-49) */
+#define GPE_ERR_CUDA 3       /* CUDA runtime/driver error */
+#define GPE_ERR_OOM 4        /* device allocation failed */
+#define GPE_ERR_NAN 5        /* non-finite value in a reduction */
+#define GPE_ERR_TIMEOUT 6    /* a bounded device-side wait expired */
+#define GPE_ERR_NODEVICE 7   /* no usable sm_100 device */
+#define GPE_ERR_UNDERFLOW 8  /* rk45 step underflow (a warning in
+                                src/solve.f90:203-211; reported, not fatal) */
+
+/* scheme values (the reference's character(5) scheme) */
+#define GPE_SCHEME_EULER 0   /* 'euler', src/solve.f90:57-74 */
+#define GPE_SCHEME_RK2 1     /* 'rk2',   src/solve.f90:78-105 */
+#define GPE_SCHEME_RK4 2     /* 'rk4',   src/solve.f90:109-154 */
+#define GPE_SCHEME_RK45 3    /* 'rk45',  src/solve.f90:158-378 */
+
+/* Run configuration.  Mirrors run_params / eqn_params
+ * (src/parameters.f90:24-55) and the compile-time grid of parameters.in
+ * (nx, ny, nz, pr); the remaining fields select the B200 storage form. */
+typedef struct gpe_params {
+  int32_t struct_size;  /* sizeof(gpe_params), for ABI checks */
+  int32_t nx, ny, nz;   /* grid points (parameters.in nx, ny, nz) */
+  double xr, yr, zr;    /* box half-widths; dx = 2 xr/(nx-1) (ic.f90:43-48) */
+  int32_t scheme;       /* GPE_SCHEME_* */
+  int32_t eqn_to_solve; /* 1..4 (src/solve.f90:414-437) */
+  int32_t bcs;          /* 1 periodic, 2 reflective */
+  int32_t order;        /* 2 or 4 (centred differences) */
+  int32_t real_time;    /* 1 real time, 0 imaginary time */
+  int32_t precision;    /* storage: 8 = complex64, 16 = complex128 */
+  double Urhs, diss_amp, scal, g, mu, nn, omx, omy, omz;
+  int32_t kahan;        /* complex64 only: compensated (Kahan) accumulation
+                           of the step increment, FP32 compensation field */
+  int32_t device;       /* CUDA device ordinal */
+  int32_t tile_y;       /* 0 = auto; else rows per tile (4 or 8) */
+  int32_t zchunk;       /* 0 = auto; else z-planes per block */
+} gpe_params;
+
+/* The solver's time globals: t, im_t, dt (complex), p
+ * (src/parameters.f90:115-127). */
+typedef struct gpe_time {
+  double t, im_t;
+  double dt_re, dt_im;
+  int32_t p;
+  int32_t reserved;
+} gpe_time;
+
+/* Per-call diagnostics of solver(); for rk45: the accepted errmax
+ * (errmaxr(1), src/solve.f90:184-193), number of rkck attempts, the step
+ * actually taken (dt_did, :223) and an underflow flag (tnew == t, :203-211). */
+typedef struct gpe_step_info {
+  double errmax;
+  double dt_did_re, dt_did_im;
+  int32_t attempts;
+  int32_t underflow;
+} gpe_step_info;
+
+/* Per-kernel-family device times collected while timing is on. */
+#define GPE_TIMING_FAMILIES 8
+typedef struct gpe_timing {
+  double ms[GPE_TIMING_FAMILIES];      /* summed CUDA-event time */
+  int64_t launches[GPE_TIMING_FAMILIES];
+  int64_t sites[GPE_TIMING_FAMILIES];  /* grid sites processed */
+} gpe_timing;
+/* families */
+#define GPE_FAM_STAGE_FIRST 0  /* first stage of a step (reads psi only) */
+#define GPE_FAM_STAGE_MID 1    /* middle stages */
+#define GPE_FAM_STAGE_LAST 2   /* final stage (writes psi, fused norm) */
+#define GPE_FAM_REDUCE 3       /* reduction finalisers */
+#define GPE_FAM_ENERGY 4
+#define GPE_FAM_COPY 5         /* state pack/unpack, ghost fill, scale */
+#define GPE_FAM_OTHER 6
+
+typedef struct gpe_ctx gpe_ctx;
+
+/* Fill *prm with the reference defaults for an nx x ny x nz grid. */
+void gpe_gpu_default_params(gpe_params* prm, int32_t nx, int32_t ny,
+                            int32_t nz);
+
+/* Allocate a context on prm->device: all fields, tensor maps and scratch.
+ * Replaces the reference's allocation of psi%old/psi%new and work arrays
+ * (src/gpe.f90:56-68) and its grid set-up get_grid (src/ic.f90:32-69). */
+int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out);
+void gpe_gpu_destroy(gpe_ctx* ctx);
+
+/* Last error message of ctx (or of the last failed create when ctx is
+ * NULL).  Valid until the next call on ctx. */
+const char* gpe_gpu_last_error(const gpe_ctx* ctx);
+
+/* Grid coordinates x(0:nx-1), y, z (src/ic.f90:24-26, 53-66). */
+int gpe_gpu_grid(const gpe_ctx* ctx, double* x, double* y, double* z);
+
+/* Load / read the resident state from / to a HOST array (interior layout).
+ * set_state also fills the boundary ghosts, which is what the caller's
+ * halo exchange did before solver() (src/gpe.f90:165-174). */
+int gpe_gpu_set_state(gpe_ctx* ctx, const void* psi, int32_t elem_bytes);
+int gpe_gpu_get_state(gpe_ctx* ctx, void* psi, int32_t elem_bytes);
+/* Same with DEVICE arrays on the context's device. */
+int gpe_gpu_set_state_device(gpe_ctx* ctx, const void* psi,
+                             int32_t elem_bytes);
+int gpe_gpu_get_state_device(gpe_ctx* ctx, void* psi, int32_t elem_bytes);
+
+/* One call of solver(var_in, var_out) (src/solve.f90:25-53) on the
+ * resident state: advances psi by one step of the configured scheme and
+ * updates tm->t, tm->im_t and (rk45) tm->dt exactly as the reference updates
+ * its globals (src/solve.f90:70-71, 101-102, 150-151, 222-229).  tm->p is
+ * not changed (the caller's loop increments it, src/gpe.f90:277).  info may
+ * be NULL.  The fused final-stage norm of the new state is cached for
+ * gpe_gpu_norm. */
+int gpe_gpu_solver(gpe_ctx* ctx, gpe_time* tm, gpe_step_info* info);
+
+/* The literal host-array form of solver(var_in, var_out): copies var_in
+ * (interior, HOST) to the device, steps, copies the result to var_out.
+ * The halo of the reference's var_in is not needed: boundary ghosts are
+ * rebuilt on the device. */
+int gpe_gpu_solver_host(gpe_ctx* ctx, const void* var_in, void* var_out,
+                        int32_t elem_bytes, gpe_time* tm,
+                        gpe_step_info* info);
+
+/* nsteps fixed-step solver() calls (euler/rk2/rk4) replayed from one CUDA
+ * graph, with get_norm after every step as the reference loop does
+ * (src/gpe.f90:241-243); norms (HOST, may be NULL) receives nsteps values.
+ * tm->p is advanced by nsteps.  rk45 is stepped one call at a time. */
+int gpe_gpu_advance(gpe_ctx* ctx, int64_t nsteps, gpe_time* tm,
+                    double* norms);
+
+/* get_norm (src/variables.f90:537-559 with integrate_x/y/z :713-823) of the
+ * resident state, FP64. */
+int gpe_gpu_norm(gpe_ctx* ctx, double* norm);
+
+/* energy (src/variables.f90:563-587): *E = sum Re(-lap psi conj(psi)
+ * + 0.5|psi|^4) dx dy dz (energy.dat holds E/(nx ny nz), src/io.f90:213).
+ * *H4 (may be NULL) = the discrete Hamiltonian of equation 4,
+ * sum [0.5 Re(-lap psi conj psi) + V|psi|^2 + 0.5 g|psi|^4 - mu|psi|^2]
+ * dx dy dz, which that equation conserves (no reference counterpart). */
+int gpe_gpu_energy(gpe_ctx* ctx, double* E, double* H4);
+
+/* renormalise (src/variables.f90:698-709): psi = sqrt(nn) psi / sqrt(norm). */
+int gpe_gpu_renormalise(gpe_ctx* ctx, double norm);
+
+/* get_rhs (src/solve.f90:382-440) and laplacian (src/variables.f90:55-71)
+ * of the resident state into a HOST array (interior layout). */
+int gpe_gpu_rhs(gpe_ctx* ctx, void* out, int32_t elem_bytes);
+int gpe_gpu_laplacian(gpe_ctx* ctx, void* out, int32_t elem_bytes);
+
+/* Switch the time direction in place, as the imaginary-to-real switch of
+ * src/gpe.f90:251-268 does (real_time flag used by rk45 step control). */
+int gpe_gpu_set_real_time(gpe_ctx* ctx, int32_t real_time);
+
+/* Per-kernel-family CUDA-event timing (off by default). */
+int gpe_gpu_set_timing(gpe_ctx* ctx, int32_t on);
+int gpe_gpu_get_timing(gpe_ctx* ctx, gpe_timing* out);
+/* Number of kernels this context has launched (graph replays count their
+ * kernels). */
+int64_t gpe_gpu_launch_count(const gpe_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or CUDA events against the solver's. */
+void* gpe_gpu_stream(const gpe_ctx* ctx);
+
+/* Device bytes held by the context. */
+int64_t gpe_gpu_device_bytes(const gpe_ctx* ctx);
+
+/* Pinned host memory for the host-array calls (cudaHostAlloc/FreeHost). */
+void* gpe_gpu_host_alloc(size_t bytes);
+void gpe_gpu_host_free(void* p);
+
+int32_t gpe_gpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPE_GPU_H */

@@ -1,0 +1,86 @@
+"""CPU checks of the C-ABI library: it loads without a GPU, exports exactly
+what include/gpe_gpu.h declares, its structs match the ctypes mirror, and
+calls without a device fail with a clean status (no compute here)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from gpe_b200 import _lib
+from gpe_b200.build import build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gpe_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = set(re.findall(r"\b(gpe_gpu_\w+)\s*\(", src))
+    return names
+
+
+@pytest.fixture(scope="module")
+def L():
+    build()
+    return _lib.lib()
+
+
+def test_every_declared_symbol_is_exported(L):
+    names = declared_functions()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (gpe_gpu_\w+)", out))
+    assert names == exported, (names ^ exported)
+    for n in names:
+        assert hasattr(L, n)
+    assert set(_lib.SIGNATURES) == names
+
+
+def test_struct_layout_matches_header(L):
+    p = _lib.GpeParamsC()
+    L.gpe_gpu_default_params(ctypes.byref(p), 16, 16, 16)
+    assert p.struct_size == ctypes.sizeof(_lib.GpeParamsC)
+    assert (p.nx, p.ny, p.nz, p.scheme, p.eqn_to_solve, p.bcs, p.order) == (16, 16, 16, 2, 4, 1, 2)
+    assert p.precision == 16 and p.g == 1.0 and p.nn == 1.0
+    assert ctypes.sizeof(_lib.GpeTimeC) == 40
+    assert L.gpe_gpu_abi_version() == 1
+
+
+def test_create_validates_before_touching_a_device(L):
+    p = _lib.GpeParamsC()
+    L.gpe_gpu_default_params(ctypes.byref(p), 4, 16, 16)
+    h = ctypes.c_void_p()
+    rc = L.gpe_gpu_create(ctypes.byref(p), ctypes.byref(h))
+    assert rc == 1 and not h
+    assert b">= 6" in L.gpe_gpu_last_error(None)
+    L.gpe_gpu_default_params(ctypes.byref(p), 16, 16, 16)
+    p.struct_size = 12
+    assert L.gpe_gpu_create(ctypes.byref(p), ctypes.byref(h)) == 1
+    L.gpe_gpu_default_params(ctypes.byref(p), 16, 16, 16)
+    p.kahan = 1  # kahan needs complex64 storage
+    assert L.gpe_gpu_create(ctypes.byref(p), ctypes.byref(h)) == 1
+
+
+def test_no_device_is_a_clean_error_without_gpu(L):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = _lib.GpeParamsC()
+    L.gpe_gpu_default_params(ctypes.byref(p), 16, 16, 16)
+    h = ctypes.c_void_p()
+    rc = L.gpe_gpu_create(ctypes.byref(p), ctypes.byref(h))
+    assert rc == 7 and not h
+    assert L.gpe_gpu_last_error(None)
+    with pytest.raises(_lib.GpeError):
+        _lib.check(rc)
+
+
+def test_null_context_calls_are_rejected(L):
+    assert L.gpe_gpu_solver(None, None, None) == 1
+    assert L.gpe_gpu_norm(None, None) == 1
+    assert L.gpe_gpu_launch_count(None) == -1
+    L.gpe_gpu_destroy(None)

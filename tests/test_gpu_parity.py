@@ -1,0 +1,240 @@
+"""GPU parity: the CUDA path through the C-ABI against the CPU oracle on the
+same seeded inputs.
+
+Tolerances (FP64 storage vs the FP64 oracle): relative L2 of psi <= 1e-12,
+relative norm / energy <= 1e-12 -- both compute the same arithmetic in a
+different order.  rk45 step sizes: <= 1e-8 relative (the embedded error
+estimate cancels ~8 digits, see tests/test_oracle.py).  Complex64 storage:
+<= 2e-6 per step against FP64, Kahan runs as stated in each test."""
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from gpe_b200 import GpeError, GpeParams, GpeSolver, run_loop
+from tests.conftest import rel_l2, random_field
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(Urhs=0.3, diss_amp=0.2, g=1.3, mu=0.9, omx=0.3, omy=0.2, omz=0.4)
+
+
+def pair(n, xr, scheme="rk4", eqn=4, bcs=1, order=2, rt=True, precision=16, kahan=False,
+         **kw):
+    prm = GpeParams(nx=n[0], ny=n[1], nz=n[2], xr=xr[0], yr=xr[1], zr=xr[2], scheme=scheme,
+                    eqn_to_solve=eqn, bcs=bcs, order=order, real_time=rt, precision=precision,
+                    kahan=kahan, **kw)
+    o = oracle.Oracle(oracle.OracleParams(nx=n[0], ny=n[1], nz=n[2], xr=xr[0], yr=xr[1],
+                                          zr=xr[2], scheme=scheme, eqn_to_solve=eqn, bcs=bcs,
+                                          order=order, real_time=rt, **kw))
+    return GpeSolver(prm), o
+
+
+COMBOS = list(itertools.product([1, 2, 3, 4], [1, 2], [2, 4], ["euler", "rk2", "rk4", "rk45"],
+                                [True, False]))
+
+
+@pytest.mark.parametrize("eqn,bcs,order,scheme,rt", COMBOS)
+def test_one_step_matches_oracle(eqn, bcs, order, scheme, rt):
+    n = (70, 13, 11)  # two x tiles (second ragged), ragged y tile
+    g, o = pair(n, (8.0, 4.0, 3.5), scheme, eqn, bcs, order, rt, **KW)
+    psi = random_field((n[2], n[1], n[0]), seed=eqn * 1000 + bcs * 100 + order)
+    dt = 0.01 if rt else -0.01j
+    g.dt = dt
+    g.set_state(psi)
+    g.solver()
+    tm = oracle.OraTime(0.0, 0.0, dt.real, dt.imag, 0)
+    exp, em, att = o.solver(psi, tm)
+    out = g.get_state()
+    assert rel_l2(out, exp) < 1e-12
+    assert g.t == pytest.approx(tm.t, rel=1e-12, abs=1e-15)
+    assert g.im_t == pytest.approx(tm.im_t, rel=1e-8, abs=1e-15)
+    if scheme == "rk45":
+        assert g.dt == pytest.approx(complex(tm.dt_re, tm.dt_im), rel=1e-8)
+        assert g.last_info.attempts == att
+    assert g.get_norm() == pytest.approx(o.get_norm(exp), rel=1e-12)
+    g.close()
+
+
+@pytest.mark.parametrize("eqn,bcs,order", list(itertools.product([1, 2, 3, 4], [1, 2], [2, 4])))
+def test_rhs_laplacian_norm_energy(eqn, bcs, order):
+    n = (67, 17, 9)
+    g, o = pair(n, (9.0, 5.0, 3.0), "rk4", eqn, bcs, order, True, **KW)
+    psi = random_field((n[2], n[1], n[0]), seed=11 + eqn)
+    g.set_state(psi)
+    assert rel_l2(g.rhs(), o.rhs(psi)) < 1e-12
+    assert rel_l2(g.laplacian(), o.laplacian(psi)) < 1e-12
+    assert g.get_norm() == pytest.approx(o.get_norm(psi), rel=1e-12)
+    E, H = g.energy()
+    assert E == pytest.approx(o.energy(psi), rel=1e-12)
+    if eqn == 4:
+        assert H == pytest.approx(o.hamiltonian4(psi), rel=1e-12)
+    g.close()
+
+
+def vortex_line_pade(x, y, z):
+    """psi = R(r) e^{i atan2(y,x)}, R = r * get_rr(r) (src/ic.f90:888-901)."""
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    r = np.sqrt(X ** 2 + Y ** 2)
+    rr = np.sqrt((0.3437 + 0.0286 * r ** 2) / (1 + 0.3333 * r ** 2 + 0.0286 * r ** 4))
+    return r * rr * np.exp(1j * np.arctan2(Y, X))
+
+
+def test_config_64cube_rk4_100_steps():
+    """64^3, h=0.5, periodic, 2nd order, RK4 dt=0.01, 100 steps, equation 4
+    with g=mu=1, straight Pade vortex line: complex128 GPU vs FP64 oracle."""
+    n = 64
+    xr = 0.5 * (n - 1) / 2
+    g, o = pair((n, n, n), (xr, xr, xr), "rk4", 4, 1, 2, True, g=1.0, mu=1.0)
+    x, y, z = o.grid()
+    psi0 = vortex_line_pade(x, y, z)
+    g.dt = 0.01
+    g.set_state(psi0)
+    oracle.set_threads(8)
+    tm = oracle.OraTime(0.0, 0.0, 0.01, 0.0, 0)
+    psi = psi0
+    for _ in range(100):
+        psi, _, _ = o.solver(psi, tm)
+    norms = g.advance(100)
+    out = g.get_state()
+    assert rel_l2(out, psi) < 1e-12
+    assert norms[-1] == pytest.approx(o.get_norm(psi), rel=1e-12)
+    assert g.energy()[0] == pytest.approx(o.energy(psi), rel=1e-12)
+    assert g.t == pytest.approx(1.0, rel=1e-13)
+    g.close()
+
+
+def test_rk45_reflective_order4_multi_step():
+    n = 24
+    g, o = pair((n, n, n), (4.6, 4.6, 4.6), "rk45", 4, 2, 4, True, g=1.0, mu=1.0)
+    x, y, z = o.grid()
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    psi = np.tanh(np.sqrt((X - 1) ** 2 + Y ** 2) + 0.1) * np.exp(1j * np.arctan2(Y, X - 1))
+    g.dt = 0.005
+    g.set_state(psi)
+    tm = oracle.OraTime(0.0, 0.0, 0.005, 0.0, 0)
+    for _ in range(8):
+        psi, _, _ = o.solver(psi, tm)
+        g.solver()
+    assert rel_l2(g.get_state(), psi) < 1e-10
+    assert g.t == pytest.approx(tm.t, rel=1e-9)
+    assert g.dt.real == pytest.approx(tm.dt_re, rel=1e-7)
+    g.close()
+
+
+@pytest.mark.parametrize("scheme", ["euler", "rk2", "rk4", "rk45"])
+def test_complex64_kahan_close_to_fp64(scheme):
+    n = (64, 24, 20)
+    g, o = pair(n, (8.0, 3.0, 2.5), scheme, 4, 1, 4, True, precision=8, kahan=True,
+                g=1.0, mu=1.0)
+    psi = random_field((n[2], n[1], n[0]), seed=5, amp=0.2)
+    g.dt = 0.002
+    g.set_state(psi)
+    tm = oracle.OraTime(0.0, 0.0, 0.002, 0.0, 0)
+    for _ in range(20):
+        psi, _, _ = o.solver(psi, tm)
+        g.solver()
+    assert rel_l2(g.get_state(), psi) < 5e-6
+    g.close()
+
+
+def test_complex64_plain_one_step():
+    n = (40, 20, 12)
+    g, o = pair(n, (5.0, 3.0, 2.0), "rk4", 4, 2, 2, True, precision=8, g=1.0, mu=1.0)
+    psi = random_field((n[2], n[1], n[0]), seed=9)
+    g.dt = 0.01
+    g.set_state(psi)
+    g.solver()
+    exp, _, _ = o.solver(psi, oracle.OraTime(0, 0, 0.01, 0, 0))
+    assert rel_l2(g.get_state(), exp) < 2e-6
+    g.close()
+
+
+def test_state_roundtrip_and_dtypes():
+    n = (33, 7, 6)
+    g, _ = pair(n, (3.0, 2.0, 2.0))
+    psi = random_field((n[2], n[1], n[0]), seed=2)
+    g.set_state(psi)
+    assert np.array_equal(g.get_state(), psi)
+    g.set_state(psi.astype(np.complex64))
+    assert np.array_equal(g.get_state(np.complex64), psi.astype(np.complex64))
+    g.close()
+
+
+def test_solver_host_is_the_resident_step():
+    n = (30, 12, 10)
+    g, o = pair(n, (4.0, 2.0, 2.0), "rk4", 4, 2, 4, True, g=1.0, mu=1.0)
+    psi = random_field((n[2], n[1], n[0]), seed=21)
+    g.dt = 0.01
+    out = g.solver_host(psi)
+    exp, _, _ = o.solver(psi, oracle.OraTime(0, 0, 0.01, 0, 0))
+    assert rel_l2(out, exp) < 1e-12
+    g.close()
+
+
+def test_imaginary_time_loop_matches_oracle_drive():
+    n = (20, 20, 20)
+    kw = dict(g=1.0, mu=1.0, nn=1.0, omx=1.0, omy=1.0, omz=1.0)
+    g, o = pair(n, (4.0, 4.0, 4.0), "rk4", 4, 2, 2, False, **kw)
+    psi = o.ic_fermi() + 0.05
+    g.dt = -0.005j
+    g.set_state(psi)
+    rec_g = run_loop(g, 6, renorm=True)
+    tm = oracle.OraTime(0.0, 0.0, 0.0, -0.005, 0)
+    psi_o, rec_o = oracle.drive(o, psi, tm, 6, renorm=True)
+    assert rel_l2(g.get_state(), psi_o) < 1e-12
+    for a, b in zip(rec_g, rec_o):
+        assert a[2] == pytest.approx(b[2], rel=1e-12)
+        assert a[1] == pytest.approx(b[1], rel=1e-12)
+    assert g.p == tm.p == 6
+    g.close()
+
+
+def test_renormalise():
+    n = (16, 16, 16)
+    g, o = pair(n, (3.0, 3.0, 3.0), nn=2.0)
+    psi = random_field((16, 16, 16), seed=4)
+    g.set_state(psi)
+    nrm = g.get_norm()
+    g.renormalise(nrm)
+    assert g.get_norm() == pytest.approx(2.0, rel=1e-12)
+    assert rel_l2(g.get_state(), o.renormalise(psi, nrm)) < 1e-15
+    g.close()
+
+
+def test_unknown_scheme_fails_at_solver_like_the_reference():
+    prm = GpeParams(nx=8, ny=8, nz=8, scheme="bogus")
+    g = GpeSolver(prm, tau=0.01)
+    g.set_state(np.ones((8, 8, 8), complex))
+    with pytest.raises(GpeError) as e:
+        g.solver()
+    assert e.value.code == 2 and "Unrecognised time stepping scheme" in str(e.value)
+    g.close()
+
+
+@pytest.mark.parametrize("n", [(6, 6, 6), (129, 9, 7), (64, 64, 8)])
+def test_edge_sizes(n):
+    g, o = pair(n, (3.0, 2.0, 1.5), "rk4", 2, 1, 4, True, Urhs=0.2)
+    psi = random_field((n[2], n[1], n[0]), seed=sum(n))
+    g.dt = 0.003
+    g.set_state(psi)
+    g.solver()
+    exp, _, _ = o.solver(psi, oracle.OraTime(0, 0, 0.003, 0, 0))
+    assert rel_l2(g.get_state(), exp) < 1e-12
+    g.close()
+
+
+def test_timing_and_launch_count():
+    n = (64, 32, 32)
+    g, _ = pair(n, (4.0, 2.0, 2.0), "rk4", 4, 1, 4)
+    g.set_state(random_field((32, 32, 64), seed=1))
+    g.dt = 0.001
+    g.set_timing(True)
+    c0 = g.launch_count()
+    g.advance(3)
+    assert g.launch_count() - c0 == 3 * 5
+    t = g.timing()
+    assert t["stage_mid"]["launches"] == 6 and t["stage_mid"]["ms"] > 0
+    g.close()

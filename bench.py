@@ -228,24 +228,27 @@ def run_reference(args):
     return 0
 
 
-def workload_config(ngpus):
-    return {"workload": "512^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
+def workload_config(ngpus, n=N_GRID):
+    return {"workload": f"{n}^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
                         "(g=mu=1, V=0), complex64 psi + Kahan compensation, FP64 norm per step",
-            "grid": [N_GRID, N_GRID, N_GRID], "h": H, "dt": DT, "scheme": "rk4", "order": 4,
+            "grid": [n, n, n], "h": H, "dt": DT, "scheme": "rk4", "order": 4,
             "bcs": "periodic", "storage": "complex64+kahan",
             "ic": "random phase, |k|<=1.0, seed 0",
-            "l2": "inputs larger than L2 (each field 1.07 GB, 5 fields) - no flush needed",
+            "l2": f"inputs larger than L2 (each field {8 * (n + 4) ** 3 / 1e9:.2f} GB, "
+                  "6 fields) - no flush needed",
             "parallelism": f"replicas x{ngpus}" if ngpus > 1 else "single GPU"}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpe_b200", choices=["gpe_b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=N_GRID,
+                    help="cube edge (default 512; smaller sizes are for profiling captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -267,7 +270,7 @@ def main():
 
     from gpe_b200 import GpeParams, GpeSolver, lib
 
-    n = N_GRID
+    n = args.grid
     xr = H * (n - 1) / 2
     prm = GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
                     order=4, precision=8, kahan=True, g=1.0, mu=1.0, device=local)
@@ -401,7 +404,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random-phase IC, |k|<=1.0, torch Philox seed 0)",
-            "config": workload_config(world),
+            "config": workload_config(world, n),
             "hbm_gbs_step": step_gbs,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_resident": e2e_resident,
             "clocks": clocks, "gpu_launches": int(launches),

@@ -60,6 +60,12 @@ thread_local std::string g_last_create_error;
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
+struct LaunchShape {
+  int TY, S, zchunk, ntx, nty, nchunks;
+  size_t smem;
+  unsigned halo_box, pt_box, halo_smem, pt_smem;
+};
+
 struct Launch {
   int family;
   cudaEvent_t a, b;
@@ -73,6 +79,7 @@ struct gpe_ctx {
   int dev = 0;
   cudaStream_t stream = nullptr;
   int nx, ny, nz, Nx, Ny, Nz;
+  int num_sms = 148;
   size_t npad, nint;
   int es;  // bytes per stored complex element (8 or 16)
   double dx, dy, dz;
@@ -103,6 +110,7 @@ struct gpe_ctx {
   int last_nblk = 0;
   int64_t device_bytes = 0;
   std::map<std::tuple<int, int, int, int>, CUtensorMap> maps;
+  std::map<const void*, LaunchShape> shapes;
   bool timing = false;
   std::vector<Launch> timed;
   gpe_timing acc_timing;
@@ -193,24 +201,32 @@ struct StageSpec {
   int nout = 0;
   int out[2] = {0, 0};
   int ghost_mask = 0;
-  cd ca[2] = {cd(0), cd(0)};
-  cd cb[2][MAXP] = {};
-  cd ck[2] = {cd(0), cd(0)};
+  // out[o] = alpha[o]*u + sum_q beta[o][q]*P_q + a[o]*f(u)
+  double alpha[2] = {0.0, 0.0};
+  double beta[2][MAXP] = {};
+  cd a[2] = {cd(0), cd(0)};
   int epi = 0;
-  cd ce[MAXP] = {};
+  // rkqs error: err = sum_q ce[q]*P_q + cek*f(u)
+  double ce[MAXP] = {};
   cd cek = cd(0);
   cd dt0 = cd(0);
   double inv_absdt = 0.0;
   int family = GPE_FAM_OTHER;
 };
 
-struct LaunchShape {
-  int TY, S, zchunk, ntx, nty, nchunks;
-  size_t smem;
-  unsigned halo_box, pt_box, halo_smem, pt_smem;
-};
+using KernelFn = const void*;
 
-LaunchShape choose_shape(const gpe_ctx* c, int R, int np) {
+// Ring depth S and tile height TY from the shared-memory budget, then the
+// z-chunking from the kernel's real occupancy: among chunk counts, pick the
+// one that minimises (waves of CTAs) x (planes per CTA + pipeline fill),
+// which trades the last wave's idle SMs against the R extra halo planes and
+// the fill latency every chunk pays.
+int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, LaunchShape* out) {
+  auto hit = c->shapes.find(fn);
+  if (hit != c->shapes.end()) {
+    *out = hit->second;
+    return GPE_OK;
+  }
   LaunchShape s{};
   const int es = c->es;
   int TY = c->prm.tile_y > 0 ? c->prm.tile_y : 8;
@@ -222,62 +238,79 @@ LaunchShape choose_shape(const gpe_ctx* c, int R, int np) {
     s.pt_smem = (unsigned)round_up(s.pt_box, 128);
     const size_t stage = s.halo_smem + (size_t)np * s.pt_smem;
     int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
-    int ctas = 2;
-    if (S < R + 3) {
-      S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
-      ctas = 1;
-    }
+    if (S < R + 3) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
     if (S >= R + 2 || attempt == 1 || c->prm.tile_y > 0) {
       s.S = std::max(S, R + 2);
-      s.smem = 128 + (size_t)s.S * stage;
-      s.ntx = (c->nx + TX - 1) / TX;
-      s.nty = (c->ny + TY - 1) / TY;
-      const int ntiles = s.ntx * s.nty;
-      int zc = c->prm.zchunk;
-      if (zc <= 0) {
-        const long target = 148L * ctas * 8;
-        long chunks = (target + ntiles - 1) / ntiles;
-        chunks = std::max<long>(1, std::min<long>(chunks, c->nz));
-        zc = (int)((c->nz + chunks - 1) / chunks);
-        zc = std::max(zc, std::min(4, c->nz));
-      }
-      s.zchunk = zc;
-      s.nchunks = (c->nz + zc - 1) / zc;
-      return s;
+      break;
     }
     TY = 4;
   }
-  return s;
+  s.smem = 128 + (size_t)s.S * (s.halo_smem + (size_t)np * s.pt_smem);
+  s.ntx = (c->nx + TX - 1) / TX;
+  s.nty = (c->ny + s.TY - 1) / s.TY;
+  CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)s.smem));
+  int occ = 0;
+  CU_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (s.TY + 1),
+                                                            s.smem));
+  if (occ < 1) return fail(c, GPE_ERR_INVALID, "stage kernel cannot be resident");
+  const long slots = (long)occ * c->num_sms;
+  const long ntiles = (long)s.ntx * s.nty;
+  int zc = c->prm.zchunk;
+  if (zc <= 0) {
+    double best = 1e300;
+    const int nmax = std::min(c->nz, 256);
+    for (int n = 1; n <= nmax; n++) {
+      const int z = (c->nz + n - 1) / n;
+      const long nch = (c->nz + z - 1) / z;
+      const long waves = (ntiles * nch + slots - 1) / slots;
+      const double cost = (double)waves * (double)(z + R + 3);
+      if (cost < best - 1e-9) {
+        best = cost;
+        zc = z;
+      }
+    }
+  }
+  s.zchunk = zc;
+  s.nchunks = (c->nz + zc - 1) / zc;
+  c->shapes[fn] = s;
+  *out = s;
+  return GPE_OK;
 }
 
-using KernelFn = const void*;
-
-template <typename TS, typename TC, int R>
-KernelFn pick_kernel(int np, int nout, int epi) {
-#define GPE_CASE(NP_, NOUT_, EPI_)                                       \
-  if (np == NP_ && nout == NOUT_ && epi == (EPI_))                      \
-    return reinterpret_cast<KernelFn>(                                   \
-        &stage_kernel<TS, TC, R, NP_, NOUT_, (EPI_)>);
-  if constexpr (std::is_same<TC, double>::value &&
-                std::is_same<TS, float>::value) {
-    GPE_CASE(0, 0, EPI_ENERGY)
-  } else {
-    GPE_CASE(0, 0, EPI_ENERGY)
-    GPE_CASE(0, 1, 0)
-    GPE_CASE(0, 1, EPI_LAP)
-    GPE_CASE(0, 1, EPI_NORM)
-    GPE_CASE(1, 1, EPI_NORM)
-    GPE_CASE(0, 2, 0)
-    GPE_CASE(2, 2, 0)
-    GPE_CASE(3, 2, 0)
-    GPE_CASE(4, 2, 0)
-    GPE_CASE(5, 2, 0)
-    GPE_CASE(5, 1, EPI_NORM | EPI_ERR)
+// The stage recipes that the schemes use; see stage_kernel.cuh for the
+// meaning of (NP, NOUT, EPI, AMASK, BMASK).  BMASK bit o*8+q: beta[o][q] != 0.
+template <typename TS, typename TC, int R, bool FULL>
+KernelFn pick_kernel(int np, int nout, int epi, int am, int bm) {
+#define GPE_CASE(NP_, NOUT_, EPI_, AM_, BM_)                                   \
+  if (np == NP_ && nout == NOUT_ && epi == (EPI_) && am == AM_ && bm == BM_)   \
+    return reinterpret_cast<KernelFn>(                                         \
+        &stage_kernel<TS, TC, R, NP_, NOUT_, (EPI_), AM_, BM_, FULL>);
+  if constexpr (std::is_same<TC, double>::value && !FULL) {
+    GPE_CASE(0, 0, EPI_ENERGY, 0, 0)
+  }
+  if constexpr (std::is_same<TS, TC>::value) {
+    GPE_CASE(0, 1, EPI_NORM, 1, 0)            // euler
+    GPE_CASE(0, 1, 0, 1, 0)                   // rk2 stage 1
+    GPE_CASE(1, 1, EPI_NORM, 0, 0x1)          // rk2 stage 2, rk4 stage 4
+    GPE_CASE(0, 2, 0, 3, 0)                   // rk4 stage 1
+    GPE_CASE(0, 2, 0, 1, 0)                   // rk4 stage 1 (compensated)
+    GPE_CASE(2, 2, 0, 0, 0x201)               // rk4 stages 2, 3
+    GPE_CASE(0, 2, 0, 2, 0)                   // rkck stage 1
+    GPE_CASE(2, 2, 0, 0, 0x300)               // rkck stage 2
+    GPE_CASE(3, 2, 0, 0, 0x700)               // rkck stage 3
+    GPE_CASE(4, 2, 0, 0, 0xF00)               // rkck stage 4
+    GPE_CASE(5, 2, 0, 0, 0x1F00)              // rkck stage 5
+    GPE_CASE(5, 1, EPI_NORM | EPI_ERR, 0, 0xF)  // rkck stage 6
+    GPE_CASE(0, 1, 0, 0, 0)                   // get_rhs
+    if constexpr (!FULL) {
+      GPE_CASE(0, 1, EPI_LAP, 0, 0)           // laplacian
+    }
     if constexpr (std::is_same<TS, float>::value) {
-      GPE_CASE(1, 2, EPI_KAHAN | EPI_NORM)
-      GPE_CASE(2, 2, EPI_KAHAN | EPI_NORM)
-      GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM)
-      GPE_CASE(6, 2, EPI_KAHAN | EPI_NORM | EPI_ERR)
+      GPE_CASE(1, 2, EPI_KAHAN | EPI_NORM, 0, 0)       // euler (compensated)
+      GPE_CASE(2, 2, EPI_KAHAN | EPI_NORM, 0, 0)       // rk2 stage 2
+      GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM, 0, 0x2)     // rk4 stage 4
+      GPE_CASE(6, 2, EPI_KAHAN | EPI_NORM | EPI_ERR, 0, 0xE)  // rkck stage 6
     }
   }
 #undef GPE_CASE
@@ -326,20 +359,10 @@ void fill_rhs_coeffs(const gpe_ctx* c, double& ar0, double& ard, double& ai,
 template <typename TS, typename TC>
 int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   const int R = c->prm.order / 2;
-  const LaunchShape sh = choose_shape(c, R, sp.np);
   StageParams<TS, TC> p;
   memset(&p, 0, sizeof(p));
-  int rc = get_map(c, sp.stencil, 0, sh.TY, R, &p.maps.halo);
-  if (rc) return rc;
-  for (int q = 0; q < sp.np; q++) {
-    rc = get_map(c, sp.pt[q], 1, sh.TY, R, &p.maps.pt[q]);
-    if (rc) return rc;
-  }
   p.nx = c->nx; p.ny = c->ny; p.nz = c->nz; p.Nx = c->Nx; p.Ny = c->Ny;
-  p.ntx = sh.ntx; p.zchunk = sh.zchunk; p.bcs = c->prm.bcs; p.TY = sh.TY;
-  p.stages = sh.S;
-  p.halo_box_bytes = sh.halo_box; p.pt_box_bytes = sh.pt_box;
-  p.halo_smem_bytes = sh.halo_smem; p.pt_smem_bytes = sh.pt_smem;
+  p.bcs = c->prm.bcs;
   p.stencil = static_cast<const TS*>(c->fld[sp.stencil]);
   for (int o = 0; o < sp.nout; o++) p.out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
   p.ghost_mask = sp.ghost_mask;
@@ -352,13 +375,19 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   p.cx1 = (TC)c1[0]; p.cx2 = (TC)c2[0];
   p.cy1 = (TC)c1[1]; p.cy2 = (TC)c2[1];
   p.cz1 = (TC)c1[2]; p.cz2 = (TC)c2[2];
+  p.c0lap = (TC)(-2.0 * (c1[0] + c2[0] + c1[1] + c2[1] + c1[2] + c2[2]));
   if (R == 1) { p.gx1 = (TC)(1.0 / (2.0 * c->dx)); p.gx2 = (TC)0; }
   else { p.gx1 = (TC)(8.0 / (12.0 * c->dx)); p.gx2 = (TC)(-1.0 / (12.0 * c->dx)); }
   double ar0, ard, ai, cL, c0, cV, cn, U;
   int ud, uv, us, ug;
   fill_rhs_coeffs(c, ar0, ard, ai, cL, c0, cV, cn, U, ud, uv, us, ug);
-  p.ar0 = (TC)ar0; p.ard = (TC)ard; p.ai = (TC)ai; p.cL = (TC)cL;
-  p.c0 = (TC)c0; p.cV = (TC)cV; p.cn = (TC)cn; p.U = (TC)U;
+  const bool full = ud || uv || us || ug;
+  const bool fold = !full && !(sp.epi & (EPI_LAP | EPI_ENERGY));
+  // plain right-hand side: f = i*ai*(cL*L + (c0 + cn|u|^2)u); the kernel
+  // forms K = ai*(...) and the factor i moves into the output coefficients
+  const double sc = full ? 1.0 : ai;
+  p.ar0 = (TC)ar0; p.ard = (TC)ard; p.ai = (TC)ai; p.cL = (TC)(sc * cL);
+  p.c0 = (TC)(sc * c0); p.cV = (TC)cV; p.cn = (TC)(sc * cn); p.U = (TC)U;
   p.use_diss = ud; p.use_V = uv; p.use_sphere = us; p.use_grad = ug;
   for (int a = 0; a < 3; a++) {
     if (std::is_same<TC, float>::value) {
@@ -371,16 +400,21 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
     p.tabW[a] = c->tabW[a];
     p.tabX[a] = c->tabX[a];
   }
+  const cd I(0.0, 1.0);
+  int am = 0, bm = 0;
   for (int o = 0; o < 2; o++) {
-    p.ca_r[o] = (TC)sp.ca[o].real(); p.ca_i[o] = (TC)sp.ca[o].imag();
-    p.ck_r[o] = (TC)sp.ck[o].real(); p.ck_i[o] = (TC)sp.ck[o].imag();
+    p.alpha[o] = (TC)sp.alpha[o];
+    if (o < sp.nout && sp.alpha[o] != 0.0) am |= 1 << o;
+    const cd a = fold ? I * sp.a[o] : sp.a[o];
+    p.a_r[o] = (TC)a.real(); p.a_i[o] = (TC)a.imag();
     for (int q = 0; q < MAXP; q++) {
-      p.cb_r[o][q] = (TC)sp.cb[o][q].real();
-      p.cb_i[o][q] = (TC)sp.cb[o][q].imag();
+      p.beta[o][q] = (TC)sp.beta[o][q];
+      if (o < sp.nout && q < sp.np && sp.beta[o][q] != 0.0) bm |= 1 << (o * 8 + q);
     }
   }
-  for (int q = 0; q < MAXP; q++) { p.ce_r[q] = sp.ce[q].real(); p.ce_i[q] = sp.ce[q].imag(); }
-  p.cek_r = sp.cek.real(); p.cek_i = sp.cek.imag();
+  for (int q = 0; q < MAXP; q++) p.ce[q] = sp.ce[q];
+  const cd cek = fold ? I * sp.cek : sp.cek;
+  p.cek_r = cek.real(); p.cek_i = cek.imag();
   p.dt0_r = sp.dt0.real(); p.dt0_i = sp.dt0.imag();
   p.inv_absdt = sp.inv_absdt;
   p.eg = c->prm.g; p.emu = c->prm.mu;
@@ -388,16 +422,32 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   p.status = c->d_status;
   p.wait_limit_ns = WAIT_LIMIT_NS;
 
-  KernelFn fn = (R == 1) ? pick_kernel<TS, TC, 1>(sp.np, sp.nout, sp.epi)
-                         : pick_kernel<TS, TC, 2>(sp.np, sp.nout, sp.epi);
+  const bool kfull = full && !(sp.epi & (EPI_LAP | EPI_ENERGY));
+  KernelFn fn;
+  if (R == 1)
+    fn = kfull ? pick_kernel<TS, TC, 1, true>(sp.np, sp.nout, sp.epi, am, bm)
+               : pick_kernel<TS, TC, 1, false>(sp.np, sp.nout, sp.epi, am, bm);
+  else
+    fn = kfull ? pick_kernel<TS, TC, 2, true>(sp.np, sp.nout, sp.epi, am, bm)
+               : pick_kernel<TS, TC, 2, false>(sp.np, sp.nout, sp.epi, am, bm);
   if (!fn) return fail(c, GPE_ERR_INVALID, "no kernel for this stage shape");
+  LaunchShape sh;
+  int rc = choose_shape(c, fn, R, sp.np, &sh);
+  if (rc) return rc;
+  rc = get_map(c, sp.stencil, 0, sh.TY, R, &p.maps.halo);
+  if (rc) return rc;
+  for (int q = 0; q < sp.np; q++) {
+    rc = get_map(c, sp.pt[q], 1, sh.TY, R, &p.maps.pt[q]);
+    if (rc) return rc;
+  }
+  p.ntx = sh.ntx; p.zchunk = sh.zchunk; p.TY = sh.TY; p.stages = sh.S;
+  p.halo_box_bytes = sh.halo_box; p.pt_box_bytes = sh.pt_box;
+  p.halo_smem_bytes = sh.halo_smem; p.pt_smem_bytes = sh.pt_smem;
   const size_t nblk = (size_t)sh.ntx * sh.nty * sh.nchunks;
   if (nblk > c->partials_cap)
     return fail(c, GPE_ERR_INVALID, "partials buffer too small");
-  CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)sh.smem));
   dim3 grid((unsigned)(sh.ntx * sh.nty), (unsigned)sh.nchunks, 1);
-  dim3 block(32, (unsigned)sh.TY, 1);
+  dim3 block(32, (unsigned)sh.TY + 1, 1);
   void* args[] = {&p};
   Launch L{};
   if (c->timing) {
@@ -502,7 +552,7 @@ int step_euler(gpe_ctx* c, cd dt) {
   s.nout = c->prm.kahan ? 2 : 1;
   s.out[0] = c->alt_id;
   s.ghost_mask = 1;
-  s.ck[0] = dt;
+  s.a[0] = dt;
   s.family = GPE_FAM_STAGE_LAST;
   if (c->prm.kahan) {
     // delta = dt f(psi); compensated psi' = psi + delta, c updated in place
@@ -510,7 +560,7 @@ int step_euler(gpe_ctx* c, cd dt) {
     s.out[1] = c->c_id;
     s.epi = EPI_KAHAN | EPI_NORM;
   } else {
-    s.ca[0] = 1.0;
+    s.alpha[0] = 1.0;
     s.epi = EPI_NORM;
   }
   int rc = launch_stage(c, s);
@@ -522,7 +572,7 @@ int step_euler(gpe_ctx* c, cd dt) {
 int step_rk2(gpe_ctx* c, cd dt) {
   StageSpec s1;
   s1.stencil = c->psi_id; s1.nout = 1; s1.out[0] = F_UA; s1.ghost_mask = 1;
-  s1.ca[0] = 1.0; s1.ck[0] = 0.5 * dt; s1.family = GPE_FAM_STAGE_FIRST;
+  s1.alpha[0] = 1.0; s1.a[0] = 0.5 * dt; s1.family = GPE_FAM_STAGE_FIRST;
   int rc = launch_stage(c, s1);
   if (rc) return rc;
   StageSpec s2;
@@ -531,11 +581,11 @@ int step_rk2(gpe_ctx* c, cd dt) {
   if (c->prm.kahan) {
     s2.np = 2; s2.pt[0] = c->psi_id; s2.pt[1] = c->c_id;
     s2.nout = 2; s2.out[1] = c->c_id;
-    s2.ck[0] = dt;
+    s2.a[0] = dt;
     s2.epi = EPI_KAHAN | EPI_NORM;
   } else {
     s2.np = 1; s2.pt[0] = c->psi_id; s2.nout = 1;
-    s2.cb[0][0] = 1.0; s2.ck[0] = dt;
+    s2.beta[0][0] = 1.0; s2.a[0] = dt;
     s2.epi = EPI_NORM;
   }
   rc = launch_stage(c, s2);
@@ -548,8 +598,8 @@ int step_rk4(gpe_ctx* c, cd dt) {
   // S1: u2 = psi + dt/2 f(psi); acc = [psi] + dt/6 f(psi)
   StageSpec s1;
   s1.stencil = c->psi_id; s1.nout = 2; s1.out[0] = F_UA; s1.out[1] = F_ACC;
-  s1.ghost_mask = 1; s1.ca[0] = 1.0; s1.ck[0] = 0.5 * dt;
-  s1.ca[1] = K ? 0.0 : 1.0; s1.ck[1] = dt / 6.0;
+  s1.ghost_mask = 1; s1.alpha[0] = 1.0; s1.a[0] = 0.5 * dt;
+  s1.alpha[1] = K ? 0.0 : 1.0; s1.a[1] = dt / 6.0;
   s1.family = GPE_FAM_STAGE_FIRST;
   int rc = launch_stage(c, s1);
   if (rc) return rc;
@@ -557,14 +607,14 @@ int step_rk4(gpe_ctx* c, cd dt) {
   StageSpec s2;
   s2.stencil = F_UA; s2.np = 2; s2.pt[0] = c->psi_id; s2.pt[1] = F_ACC;
   s2.nout = 2; s2.out[0] = F_UB; s2.out[1] = F_ACC; s2.ghost_mask = 1;
-  s2.cb[0][0] = 1.0; s2.ck[0] = 0.5 * dt;
-  s2.cb[1][1] = 1.0; s2.ck[1] = dt / 3.0;
+  s2.beta[0][0] = 1.0; s2.a[0] = 0.5 * dt;
+  s2.beta[1][1] = 1.0; s2.a[1] = dt / 3.0;
   s2.family = GPE_FAM_STAGE_MID;
   rc = launch_stage(c, s2);
   if (rc) return rc;
   // S3: u4 = psi + dt f(u3); acc += dt/3 f(u3)
   StageSpec s3 = s2;
-  s3.stencil = F_UB; s3.out[0] = F_UA; s3.ck[0] = dt;
+  s3.stencil = F_UB; s3.out[0] = F_UA; s3.a[0] = dt;
   rc = launch_stage(c, s3);
   if (rc) return rc;
   // S4: psi' = acc + dt/6 f(u4)   (Kahan: psi' = psi (+) (acc + dt/6 f))
@@ -574,11 +624,11 @@ int step_rk4(gpe_ctx* c, cd dt) {
   if (K) {
     s4.np = 3; s4.pt[0] = c->psi_id; s4.pt[1] = F_ACC; s4.pt[2] = c->c_id;
     s4.nout = 2; s4.out[1] = c->c_id;
-    s4.cb[0][1] = 1.0; s4.ck[0] = dt / 6.0;
+    s4.beta[0][1] = 1.0; s4.a[0] = dt / 6.0;
     s4.epi = EPI_KAHAN | EPI_NORM;
   } else {
     s4.np = 1; s4.pt[0] = F_ACC; s4.nout = 1;
-    s4.cb[0][0] = 1.0; s4.ck[0] = dt / 6.0;
+    s4.beta[0][0] = 1.0; s4.a[0] = dt / 6.0;
     s4.epi = EPI_NORM;
   }
   rc = launch_stage(c, s4);
@@ -607,20 +657,20 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
     s.out[0] = ks[st];
     s.out[1] = (st % 2 == 0) ? F_UA : F_UB;
     s.ghost_mask = 2;
-    s.ck[0] = dt;
+    s.a[0] = dt;
     if (st == 0) {
       s.np = 0;
-      s.ca[1] = 1.0;
+      s.alpha[1] = 1.0;
     } else {
       s.np = st + 1;
       s.pt[0] = psi;
-      s.cb[1][0] = 1.0;
+      s.beta[1][0] = 1.0;
       for (int jj = 0; jj < st; jj++) {
         s.pt[jj + 1] = ks[jj];
-        s.cb[1][jj + 1] = B[st][jj];
+        s.beta[1][jj + 1] = B[st][jj];
       }
     }
-    s.ck[1] = B[st][st] * dt;
+    s.a[1] = B[st][st] * dt;
     s.family = st == 0 ? GPE_FAM_STAGE_FIRST : GPE_FAM_STAGE_MID;
     rc = launch_stage(c, s);
     if (rc) return rc;
@@ -634,13 +684,13 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
   s.family = GPE_FAM_STAGE_LAST;
   s.dt0 = dt0;
   s.inv_absdt = 1.0 / std::abs(dt);
-  s.ck[0] = C6 * dt;
+  s.a[0] = C6 * dt;
   s.cek = DC6 * dt;
   // pointwise slots: psi, k1, k3, k4, k5 [, c]  (the kernel takes psi from
   // slot 0, k1 from slot 1 and the compensation from the last slot)
   s.pt[0] = psi;
   s.pt[1] = F_K1; s.pt[2] = F_K3; s.pt[3] = F_K4; s.pt[4] = F_K5;
-  s.cb[0][1] = C1; s.cb[0][2] = C3; s.cb[0][3] = C4;
+  s.beta[0][1] = C1; s.beta[0][2] = C3; s.beta[0][3] = C4;
   s.ce[1] = DC1; s.ce[2] = DC3; s.ce[3] = DC4; s.ce[4] = DC5;
   if (K) {
     s.np = 6;
@@ -649,7 +699,7 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
     s.epi = EPI_KAHAN | EPI_NORM | EPI_ERR;
   } else {
     s.np = 5;
-    s.cb[0][0] = 1.0;
+    s.beta[0][0] = 1.0;
     s.nout = 1;
     s.epi = EPI_NORM | EPI_ERR;
   }
@@ -978,6 +1028,7 @@ int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
 
   gpe_ctx* c = new gpe_ctx();
   c->prm = p;
+  c->num_sms = dp.multiProcessorCount;
   c->dev = p.device;
   memset(&c->acc_timing, 0, sizeof(c->acc_timing));
   auto bail = [&](int rc) {
@@ -1267,7 +1318,7 @@ static int rhs_like(gpe_ctx* c, void* out, int32_t elem_bytes, bool lap) {
   s.stencil = c->psi_id;
   s.nout = 1;
   s.out[0] = c->alt_id;
-  s.ck[0] = 1.0;
+  s.a[0] = 1.0;
   s.epi = lap ? EPI_LAP : 0;
   rc = launch_stage(c, s);
   if (rc) return rc;

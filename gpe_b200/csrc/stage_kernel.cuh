@@ -14,17 +14,34 @@
 //     (src/variables.f90:537-559, 713-823), the rkqs error maximum
 //     (src/solve.f90:176-190) or the energy sum (src/variables.f90:563-587).
 //
-// Tiling: a CTA owns a 64 x TY tile in (x, y) -- one warp per row, two
-// consecutive x sites per lane -- and marches a chunk of z-planes.  For each
-// plane a single thread issues TMA tile loads (no multicast) of the stencil
-// plane with its halo and of the pointwise input tiles into a ring of
-// `stages` shared-memory slots completed on mbarriers.  The z-neighbours come
-// from a register queue of 2R+1 planes (R = order/2); x and y neighbours are
-// read from the staged halo plane.  Outputs go straight from registers to
-// global memory as 16-byte stores.
+// Tiling: a CTA owns a 64 x TY tile in (x, y) and marches a chunk of
+// z-planes.  TY compute warps each own one row (two consecutive x sites per
+// lane); one more warp is the producer: its lane 0 issues, plane by plane,
+// TMA tile loads (no multicast) of the stencil plane with its halo and of the
+// pointwise input tiles into a ring of `stages` shared-memory slots.  A slot
+// is handed over on a "full" mbarrier (TMA transaction count) and handed back
+// on an "empty" mbarrier that every compute warp arrives on once it no longer
+// reads the slot, so no block-wide barrier is taken per plane.  The
+// z-neighbours come from a register queue of 2R+1 planes (R = order/2),
+// rotated by unrolling the plane loop 2R+1 times; x and y neighbours are read
+// from the staged halo plane.  Outputs go straight from registers to global
+// memory as 16-byte stores.
+//
+// The combination each stage performs is fixed at compile time ("recipe"):
+//   out[o] = alpha[o]*u + sum_q beta[o][q]*P_q + a[o] (x) K
+// where u is the stencil field at the site, P_q the pointwise inputs, alpha
+// and beta real Runge-Kutta weights present only where AMASK/BMASK say so,
+// a[o] one complex coefficient per output (it carries dt), and K the
+// right-hand side.  Without trap, sponge, gradient or sphere terms (FULL =
+// false) the right-hand side of every equation is i*B with
+// B = cL*lap(u) + (c0 + cn|u|^2) u, so K = B and the host folds the factor i
+// into a[o]; with FULL = true K = f(u) is formed site by site.
 #pragma once
 
+#include <type_traits>
+
 #include "device_utils.cuh"
+#include "vec2.cuh"
 
 namespace gpe {
 
@@ -37,7 +54,7 @@ enum : int {
   EPI_ERR = 2,     // reduce max |err / psi_scal| into partial slot 1
   EPI_KAHAN = 4,   // out0 = psi + delta with compensation, out1 = new c
   EPI_ENERGY = 8,  // no outputs; reduce E (slot 0) and H4 (slot 1)
-  EPI_LAP = 16,    // the stage's f(u) is the Laplacian alone
+  EPI_LAP = 16,    // K is the Laplacian itself
 };
 
 struct TileMaps {
@@ -56,24 +73,24 @@ struct StageParams {
   const TS* stencil;    // stencil field (padded layout), warm-up planes
   TS* out[2];           // output fields (padded layout)
   int ghost_mask;       // bit o set: out[o] gets its boundary ghosts filled
-  // second differences: L = sum_axes c1*((f1+f-1)-2f0) + c2*((f2+f-2)-2f0)
-  TC cx1, cx2, cy1, cy2, cz1, cz2;
+  // Laplacian: T = sum_axes c1*(f1+f-1) + c2*(f2+f-2); L = T + c0*f0
+  TC cx1, cx2, cy1, cy2, cz1, cz2, c0lap;
   // x gradient: gx1*(f1-f-1) + gx2*(f2-f-2)
   TC gx1, gx2;
-  // f = m * ( A*(cL*L + (c0 + cV*V + cn*|u|^2) u) + U*u_x ),
-  // A = (ar0 + ard*diss) + i*ai
+  // FULL: f = m * ( A*(cL*L + (c0 + cV*V + cn*|u|^2) u) + U*u_x ),
+  //       A = (ar0 + ard*diss) + i*ai
+  // plain: K = cL*L + (c0 + cn*|u|^2) u   (the factor i is folded into a[o])
   TC ar0, ard, ai, cL, c0, cV, cn, U;
   int use_diss, use_V, use_sphere, use_grad;
   const TC* tabV[3];      // per-axis trap terms, V = Vx[i]+Vy[j]+Vz[k]
   const TC* tabD[3];      // per-axis sponge terms (times diss_amp)
   const double* tabW[3];  // per-axis norm weights
   const double* tabX[3];  // coordinates (sphere mask)
-  // out[o] = ca[o]*u + sum_q cb[o][q]*P_q + ck[o]*f
-  TC ca_r[2], ca_i[2];
-  TC cb_r[2][MAXP], cb_i[2][MAXP];
-  TC ck_r[2], ck_i[2];
-  // rkqs error: err = sum_q ce[q]*P_q + cek*f (FP64)
-  double ce_r[MAXP], ce_i[MAXP], cek_r, cek_i;
+  TC alpha[2];
+  TC beta[2][MAXP];
+  TC a_r[2], a_i[2];
+  // rkqs error: err = sum_q ce[q]*P_q + cek (x) K (FP64)
+  double ce[MAXP], cek_r, cek_i;
   double dt0_r, dt0_i;    // dt of the first attempt (psi_scal)
   double inv_absdt;       // 1/|dt| of this attempt (|f(psi)| = |k1|/|dt|)
   double eg, emu;         // energy: g, mu
@@ -82,45 +99,26 @@ struct StageParams {
   unsigned long long wait_limit_ns;
 };
 
-template <typename TC>
-struct Cx {
-  TC r, i;
-};
-
-template <typename TC>
-__device__ __forceinline__ Cx<TC> cmul(TC ar, TC ai, Cx<TC> b) {
-  return {ar * b.r - ai * b.i, ar * b.i + ai * b.r};
+__device__ __forceinline__ bool near_edge(int i, int n) {
+  return i < 3 || i >= n - 3;
 }
 
-template <typename TC, int R>
-__device__ __forceinline__ Cx<TC> second_diff(Cx<TC> m2, Cx<TC> m1, Cx<TC> c,
-                                              Cx<TC> p1, Cx<TC> p2, TC c1,
-                                              TC c2) {
-  const TC two = TC(2);
-  Cx<TC> d1 = {(p1.r + m1.r) - two * c.r, (p1.i + m1.i) - two * c.i};
-  if (R == 1) return {c1 * d1.r, c1 * d1.i};
-  Cx<TC> d2 = {(p2.r + m2.r) - two * c.r, (p2.i + m2.i) - two * c.i};
-  return {c1 * d1.r + c2 * d2.r, c1 * d1.i + c2 * d2.i};
-}
+template <int K>
+using IC = std::integral_constant<int, K>;
 
-template <typename TC>
-__device__ __forceinline__ Cx<TC> lo(const Pair<TC>& a) {
-  return {a.r0, a.i0};
-}
-template <typename TC>
-__device__ __forceinline__ Cx<TC> hi(const Pair<TC>& a) {
-  return {a.r1, a.i1};
-}
-
-template <typename TS, typename TC, int R, int NP, int NOUT, int EPI>
-__global__ void __launch_bounds__(256)
+template <typename TS, typename TC, int R, int NP, int NOUT, int EPI, int AMASK,
+          int BMASK, bool FULL>
+__global__ void __launch_bounds__(288)
     stage_kernel(const __grid_constant__ StageParams<TS, TC> p) {
+  using V = typename VT<TC>::T;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int s_abort;
+  __shared__ int s_abort, s_issued;
   __shared__ double s_red[2][32];
 
   constexpr int W = (int)(sizeof(TS) / 4);  // 8-byte TMA units per complex
   constexpr int HW = TX + 4;                // halo tile row width (complex)
+  constexpr int QN = 2 * R + 1;             // z-queue length
+  constexpr unsigned ES = 2 * sizeof(TS);   // bytes per stored complex
   const int TY = p.TY, S = p.stages;
   const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
   const int tile_x = blockIdx.x % p.ntx, tile_y = blockIdx.x / p.ntx;
@@ -132,289 +130,338 @@ __global__ void __launch_bounds__(256)
   const bool ok0 = (i0 < p.nx) && (j < p.ny);
   const bool ok1 = (i0 + 1 < p.nx) && (j < p.ny);
 
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  // shared memory: full[S] and empty[S] barriers (S <= 8), then the slots
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + 8;
   unsigned char* sbase = smem + 128;
-  const size_t stride = (size_t)p.halo_smem_bytes + (size_t)NP * p.pt_smem_bytes;
+  const unsigned stride = p.halo_smem_bytes + (unsigned)NP * p.pt_smem_bytes;
   const size_t Nx = (size_t)p.Nx, NxNy = (size_t)p.Nx * (size_t)p.Ny;
-  auto gidx = [&](int i, int jj, int k) -> size_t {
-    return (size_t)(k + GH) * NxNy + (size_t)(jj + GH) * Nx + (size_t)(i + GH);
-  };
-
-  auto issue = [&](int u) {
-    const int slot = u % S;
-    unsigned char* st = sbase + (size_t)slot * stride;
-    const bool with_pt = (NP > 0) && (u >= R);
-    mbar_arrive_expect_tx(&bars[slot],
-                          p.halo_box_bytes + (with_pt ? NP * p.pt_box_bytes : 0u));
-    tma_load_3d(st, &p.maps.halo, &bars[slot], W * tile_x * TX,
-                tile_y * TY + GH - R, z0 + u + GH);
-    if (with_pt) {
-#pragma unroll
-      for (int q = 0; q < NP; q++)
-        tma_load_3d(st + p.halo_smem_bytes + (size_t)q * p.pt_smem_bytes,
-                    &p.maps.pt[q], &bars[slot], W * (tile_x * TX + GH),
-                    tile_y * TY + GH, z0 + u - R + GH);
-    }
-  };
 
   if (tid == 0) {
-    for (int s = 0; s < S; s++) mbar_init(&bars[s], 1);
+    for (int s = 0; s < S; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], (uint32_t)TY);
+    }
     fence_mbar_init();
     s_abort = 0;
-    prefetch_tmap(&p.maps.halo);
-#pragma unroll
-    for (int q = 0; q < NP; q++) prefetch_tmap(&p.maps.pt[q]);
+    s_issued = 0;
   }
   __syncthreads();
-  if (tid == 0) {
-    const int n0 = min(S, niters);
-    for (int u = 0; u < n0; u++) issue(u);
-  }
-
-  // Per-thread constants along x and y.
-  TC Vx[2] = {TC(0), TC(0)}, Dx[2] = {TC(0), TC(0)}, Vy = TC(0), Dy = TC(0);
-  double Wx[2] = {0.0, 0.0}, Wy = 0.0;
-  if (p.use_V) {
-    Vx[0] = p.tabV[0][i0]; Vx[1] = p.tabV[0][i0 + 1]; Vy = p.tabV[1][j];
-  }
-  if (p.use_diss) {
-    Dx[0] = p.tabD[0][i0]; Dx[1] = p.tabD[0][i0 + 1]; Dy = p.tabD[1][j];
-  }
-  if (EPI & EPI_NORM) {
-    Wx[0] = p.tabW[0][i0]; Wx[1] = p.tabW[0][i0 + 1]; Wy = p.tabW[1][j];
-  }
-  int gxa[2], gxb[2], gya, gyb;
-  ghost_targets(i0, p.nx, p.bcs, gxa[0], gxb[0]);
-  ghost_targets(i0 + 1, p.nx, p.bcs, gxa[1], gxb[1]);
-  ghost_targets(j, p.ny, p.bcs, gya, gyb);
-
-  // Register queue of the stencil field's z-column: q[R] is the plane being
-  // computed, q[R+d] the plane d above it.
-  Pair<TC> q[2 * R + 1];
-#pragma unroll
-  for (int s = 0; s < 2 * R + 1; s++) q[s] = {TC(0), TC(0), TC(0), TC(0)};
-#pragma unroll
-  for (int w = 0; w < R; w++) {
-    const int zz = z0 - R + w;
-    Pair<TC> v = {TC(0), TC(0), TC(0), TC(0)};
-    if (ok0) v = cvt_pair<TC>(ld_pair<TS>(p.stencil + 2 * gidx(i0, j, zz)));
-#pragma unroll
-    for (int s = 0; s < 2 * R; s++) q[s] = q[s + 1];
-    q[2 * R] = v;
-  }
 
   double red0 = 0.0, red1 = 0.0;
-  int t_stop = niters;                          // first iteration not completed
-  int issued = (tid == 0) ? min(S, niters) : 0;  // tracked by the issuing thread
+  if (ty == TY) {
+    // ---------------- producer warp: lane 0 streams the planes -------------
+    if (lane == 0) {
+      prefetch_tmap(&p.maps.halo);
+#pragma unroll
+      for (int qq = 0; qq < NP; qq++) prefetch_tmap(&p.maps.pt[qq]);
+      int slot = 0;
+      uint32_t cyc = 0;  // completed passes over the ring
+      for (int u = 0; u < niters; u++) {
+        if (cyc > 0) {
+          // the slot's previous plane must have been released by every
+          // compute warp
+          if (!mbar_wait_bounded(&empty[slot], (cyc - 1) & 1u, p.wait_limit_ns)) {
+            s_abort = 1;
+            atomicExch(p.status, 6);
+            break;
+          }
+          fence_proxy_async();
+        }
+        unsigned char* st = sbase + (size_t)slot * stride;
+        const bool with_pt = (NP > 0) && (u >= R);
+        mbar_arrive_expect_tx(&full[slot],
+                              p.halo_box_bytes + (with_pt ? NP * p.pt_box_bytes : 0u));
+        tma_load_3d(st, &p.maps.halo, &full[slot], W * tile_x * TX,
+                    tile_y * TY + GH - R, z0 + u + GH);
+        if (with_pt) {
+#pragma unroll
+          for (int qq = 0; qq < NP; qq++)
+            tma_load_3d(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
+                        &p.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
+                        tile_y * TY + GH, z0 + u - R + GH);
+        }
+        s_issued = u + 1;
+        if (++slot == S) {
+          slot = 0;
+          ++cyc;
+        }
+        if (*(volatile int*)&s_abort) break;
+      }
+    }
+  } else {
+  // Per-thread constants.
+  TC Vxy[2] = {TC(0), TC(0)}, Dxy[2] = {TC(0), TC(0)};
+  double Wxy[2] = {0.0, 0.0};
+  if ((FULL || (EPI & EPI_ENERGY)) && p.use_V) {
+    Vxy[0] = p.tabV[0][i0] + p.tabV[1][j];
+    Vxy[1] = p.tabV[0][i0 + 1] + p.tabV[1][j];
+  }
+  if (FULL && p.use_diss) {
+    Dxy[0] = p.tabD[0][i0] + p.tabD[1][j];
+    Dxy[1] = p.tabD[0][i0 + 1] + p.tabD[1][j];
+  }
+  if (EPI & EPI_NORM) {
+    Wxy[0] = p.tabW[0][i0] * p.tabW[1][j];
+    Wxy[1] = p.tabW[0][i0 + 1] * p.tabW[1][j];
+  }
+  const V cx1 = vsplat(p.cx1), cx2 = vsplat(p.cx2), cy1 = vsplat(p.cy1),
+          cy2 = vsplat(p.cy2), cz1 = vsplat(p.cz1), cz2 = vsplat(p.cz2),
+          c0l = vsplat(p.c0lap), cLv = vsplat(p.cL);
+  V ar[2], aix[2], alv[2], bev[2][NP > 0 ? NP : 1];
+#pragma unroll
+  for (int o = 0; o < 2; o++) {
+    ar[o] = vsplat(p.a_r[o]);
+    aix[o] = vpair(-p.a_i[o], p.a_i[o]);
+    alv[o] = vsplat(p.alpha[o]);
+#pragma unroll
+    for (int qq = 0; qq < (NP > 0 ? NP : 1); qq++) bev[o][qq] = vsplat(p.beta[o][qq]);
+  }
+  const V mone = vsplat(TC(-1));
+  // Ghost copies this thread's sites feed, as element offsets from the site
+  // (x and y fixed per thread; z per plane, uniform across the CTA).
+  int gxo[2][2], gyo[2];
+  {
+    int a, b;
+    for (int e = 0; e < 2; e++) {
+      ghost_targets(i0 + e, p.nx, p.bcs, a, b);
+      gxo[e][0] = (a != NO_GHOST) ? a - (i0 + e) : 0;
+      gxo[e][1] = (b != NO_GHOST) ? b - (i0 + e) : 0;
+    }
+    ghost_targets(j, p.ny, p.bcs, a, b);
+    gyo[0] = (a != NO_GHOST) ? (a - j) * p.Nx : 0;
+    gyo[1] = (b != NO_GHOST) ? (b - j) * p.Nx : 0;
+  }
+  const bool edge_xy = (gxo[0][0] | gxo[0][1] | gxo[1][0] | gxo[1][1] | gyo[0] | gyo[1]) != 0;
+  // element offset of this thread's first site in plane z0
+  size_t base = (size_t)(z0 + GH) * NxNy + (size_t)(j + GH) * Nx + (size_t)(i0 + GH);
 
-  for (int t = 0; t < niters; t++) {
-    const int slot = t % S;
-    if (!mbar_wait_bounded(&bars[slot], (uint32_t)((t / S) & 1), p.wait_limit_ns)) {
+  // z-queue: physical slot of push number c is c % QN; after push c the
+  // plane d above the one being computed sits in slot (c + 1 + R + d) % QN.
+  CPair<TC> q[QN];
+#pragma unroll
+  for (int w = 0; w < R; w++) {
+    CPair<TC> v = {vsplat(TC(0)), vsplat(TC(0))};
+    if (ok0) v = ld_cpair<TS, TC>(p.stencil + 2 * (base - (size_t)(R - w) * NxNy));
+    q[w] = v;
+  }
+#pragma unroll
+  for (int w = R; w < QN; w++) q[w] = {vsplat(TC(0)), vsplat(TC(0))};
+
+  int t = 0, slot = 0, cslot = 0;
+  uint32_t phase = 0;
+  const unsigned row_off = ES * (unsigned)((ty + R) * HW + 2 * lane + 2);
+  const unsigned pt_off = ES * (unsigned)(ty * TX + 2 * lane);
+
+  auto step = [&](auto kc) -> bool {
+    constexpr int KK = decltype(kc)::value;
+    if (t >= niters) return false;
+    if (!mbar_wait_bounded(&full[slot], phase, p.wait_limit_ns)) {
       s_abort = 1;
       atomicExch(p.status, 6);
+      return false;
     }
-    {
-      const TS* ht = reinterpret_cast<const TS*>(sbase + (size_t)slot * stride);
-      const Pair<TC> v =
-          cvt_pair<TC>(ld_pair<TS>(ht + 2 * ((ty + R) * HW + 2 * lane + 2)));
-#pragma unroll
-      for (int s = 0; s < 2 * R; s++) q[s] = q[s + 1];
-      q[2 * R] = v;
-    }
+    q[(R + KK) % QN] = ld_cpair<TS, TC>(
+        reinterpret_cast<const TS*>(sbase + (size_t)slot * stride + row_off));
     if (t >= R) {
       const int z = z0 + t - R;
-      const TS* hc =
-          reinterpret_cast<const TS*>(sbase + (size_t)((t - R) % S) * stride);
-      const TS* row = hc + 2 * ((ty + R) * HW);
-      const Pair<TC> xa = cvt_pair<TC>(ld_pair<TS>(row + 2 * (2 * lane)));
-      const Pair<TC> xb = q[R];
-      const Pair<TC> xc = cvt_pair<TC>(ld_pair<TS>(row + 2 * (2 * lane + 4)));
-      const Pair<TC> yp1 =
-          cvt_pair<TC>(ld_pair<TS>(hc + 2 * ((ty + R + 1) * HW + 2 * lane + 2)));
-      const Pair<TC> ym1 =
-          cvt_pair<TC>(ld_pair<TS>(hc + 2 * ((ty + R - 1) * HW + 2 * lane + 2)));
-      Pair<TC> yp2 = yp1, ym2 = ym1;
+      const unsigned char* hc = sbase + (size_t)cslot * stride + row_off;
+      auto lds = [&](int drow, int dcol) {
+        return ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hc + (int)ES * (drow * HW + dcol)));
+      };
+      auto zq = [&](int d) -> const CPair<TC>& { return q[(R + KK + 1 + R + d + 2 * QN) % QN]; };
+      const CPair<TC> xa = lds(0, -2);
+      const CPair<TC> xc = lds(0, 2);
+      const CPair<TC> yp1 = lds(1, 0), ym1 = lds(-1, 0);
+      CPair<TC> yp2 = yp1, ym2 = ym1;
       if (R == 2) {
-        yp2 = cvt_pair<TC>(ld_pair<TS>(hc + 2 * ((ty + R + 2) * HW + 2 * lane + 2)));
-        ym2 = cvt_pair<TC>(ld_pair<TS>(hc + 2 * ((ty + R - 2) * HW + 2 * lane + 2)));
+        yp2 = lds(2, 0);
+        ym2 = lds(-2, 0);
       }
-      const Pair<TC> zp1 = q[R + 1], zm1 = q[R - 1];
-      const Pair<TC> zp2 = q[2 * R], zm2 = q[0];
-
-      // pointwise inputs of this plane
-      Pair<TC> P[NP > 0 ? NP : 1];
+      CPair<TC> P[NP > 0 ? NP : 1];
       if (NP > 0) {
-        const unsigned char* pb = sbase + (size_t)slot * stride + p.halo_smem_bytes;
+        const unsigned char* pb = sbase + (size_t)slot * stride + p.halo_smem_bytes + pt_off;
 #pragma unroll
         for (int qq = 0; qq < NP; qq++)
-          P[qq] = cvt_pair<TC>(ld_pair<TS>(
-              reinterpret_cast<const TS*>(pb + (size_t)qq * p.pt_smem_bytes) +
-              2 * (ty * TX + 2 * lane)));
+          P[qq] = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(pb + (size_t)qq * p.pt_smem_bytes));
       }
-
       TC Vz = TC(0), Dz = TC(0);
       double Wz = 0.0;
-      if (p.use_V) Vz = p.tabV[2][z];
-      if (p.use_diss) Dz = p.tabD[2][z];
+      if ((FULL || (EPI & EPI_ENERGY)) && p.use_V) Vz = p.tabV[2][z];
+      if (FULL && p.use_diss) Dz = p.tabD[2][z];
       if (EPI & EPI_NORM) Wz = p.tabW[2][z];
-      int gza, gzb;
-      ghost_targets(z, p.nz, p.bcs, gza, gzb);
 
-      Cx<TC> res[2][2];  // [output][site]
+      V res[2][2];  // [output][site]
 #pragma unroll
       for (int e = 0; e < 2; e++) {
-        const Cx<TC> f0 = e ? hi(xb) : lo(xb);
-        const Cx<TC> xm2 = e ? hi(xa) : lo(xa), xm1 = e ? lo(xb) : hi(xa);
-        const Cx<TC> xp1 = e ? lo(xc) : hi(xb), xp2 = e ? hi(xc) : lo(xc);
-        Cx<TC> L = second_diff<TC, R>(xm2, xm1, f0, xp1, xp2, p.cx1, p.cx2);
-        const Cx<TC> Ly = second_diff<TC, R>(e ? hi(ym2) : lo(ym2), e ? hi(ym1) : lo(ym1),
-                                             f0, e ? hi(yp1) : lo(yp1),
-                                             e ? hi(yp2) : lo(yp2), p.cy1, p.cy2);
-        const Cx<TC> Lz = second_diff<TC, R>(e ? hi(zm2) : lo(zm2), e ? hi(zm1) : lo(zm1),
-                                             f0, e ? hi(zp1) : lo(zp1),
-                                             e ? hi(zp2) : lo(zp2), p.cz1, p.cz2);
-        L.r = (L.r + Ly.r) + Lz.r;
-        L.i = (L.i + Ly.i) + Lz.i;
-        const TC a2 = f0.r * f0.r + f0.i * f0.i;
-        const TC V = p.use_V ? (Vx[e] + Vy) + Vz : TC(0);
+        const CPair<TC>& ctr = zq(0);
+        const V f0 = e ? ctr.b : ctr.a;
+        const V xm1 = e ? ctr.a : xa.b, xp1 = e ? xc.a : ctr.b;
+        const V xm2 = e ? xa.b : xa.a, xp2 = e ? xc.b : xc.a;
+        V L = vmul(cx1, vadd(xp1, xm1));
+        L = vfma(cy1, vadd(e ? yp1.b : yp1.a, e ? ym1.b : ym1.a), L);
+        L = vfma(cz1, vadd(e ? zq(1).b : zq(1).a, e ? zq(-1).b : zq(-1).a), L);
+        if (R == 2) {
+          L = vfma(cx2, vadd(xp2, xm2), L);
+          L = vfma(cy2, vadd(e ? yp2.b : yp2.a, e ? ym2.b : ym2.a), L);
+          L = vfma(cz2, vadd(e ? zq(2).b : zq(2).a, e ? zq(-2).b : zq(-2).a), L);
+        }
+        L = vfma(c0l, f0, L);
         const bool ok = e ? ok1 : ok0;
 
         if (EPI & EPI_ENERGY) {
           if (ok) {
-            const double lr = (double)L.r, li = (double)L.i;
-            const double fr = (double)f0.r, fi = (double)f0.i;
+            const double lr = (double)L.x, li = (double)L.y;
+            const double fr = (double)f0.x, fi = (double)f0.y;
             const double d2 = fr * fr + fi * fi;
             const double kin = -(lr * fr + li * fi);
             red0 += kin + 0.5 * (d2 * d2);
-            red1 += 0.5 * kin + (double)V * d2 + 0.5 * p.eg * d2 * d2 - p.emu * d2;
+            red1 += 0.5 * kin + (double)(Vxy[e] + Vz) * d2 + 0.5 * p.eg * d2 * d2 -
+                    p.emu * d2;
           }
           continue;
         }
 
-        Cx<TC> f;
+        const TC a2 = fma(f0.y, f0.y, f0.x * f0.x);
+        V Kv;
         if (EPI & EPI_LAP) {
-          f = L;
+          Kv = L;
+        } else if (!FULL) {
+          const TC s = fma(p.cn, a2, p.c0);
+          Kv = vfma(vsplat(s), f0, vmul(cLv, L));
         } else {
-          const TC s = p.c0 + p.cV * V + p.cn * a2;
-          const Cx<TC> B = {p.cL * L.r + s * f0.r, p.cL * L.i + s * f0.i};
-          const TC ar = p.use_diss ? p.ar0 + p.ard * ((Dx[e] + Dy) + Dz) : p.ar0;
-          f = cmul<TC>(ar, p.ai, B);
+          const TC Vs = p.use_V ? Vxy[e] + Vz : TC(0);
+          const TC s = p.c0 + p.cV * Vs + p.cn * a2;
+          const V B = vfma(vsplat(s), f0, vmul(cLv, L));
+          const TC arr = p.use_diss ? p.ar0 + p.ard * (Dxy[e] + Dz) : p.ar0;
+          Kv = vfma(vsplat(arr), B, vmul(vpair(-p.ai, p.ai), vswap(B)));
           if (p.use_grad) {
-            Cx<TC> gx = {p.gx1 * (xp1.r - xm1.r), p.gx1 * (xp1.i - xm1.i)};
-            if (R == 2) {
-              gx.r += p.gx2 * (xp2.r - xm2.r);
-              gx.i += p.gx2 * (xp2.i - xm2.i);
-            }
-            f.r += p.U * gx.r;
-            f.i += p.U * gx.i;
+            V gx = vmul(vsplat(p.gx1), vfma(xm1, mone, xp1));
+            if (R == 2) gx = vfma(vsplat(p.gx2), vfma(xm2, mone, xp2), gx);
+            Kv = vfma(vsplat(p.U), gx, Kv);
           }
           if (p.use_sphere) {
             const double X = p.tabX[0][i0 + e], Y = p.tabX[1][j], Z = p.tabX[2][z];
             const TC m = (TC)(0.5 * (1.0 + tanh(sqrt(X * X + Y * Y + Z * Z) - 10.0 - 2.0)));
-            f.r *= m;
-            f.i *= m;
+            Kv = vmul(vsplat(m), Kv);
           }
         }
 
+        const V Ks = vswap(Kv);
 #pragma unroll
         for (int o = 0; o < NOUT; o++) {
-          Cx<TC> v = cmul<TC>(p.ca_r[o], p.ca_i[o], f0);
+          V v = vfma(ar[o], Kv, vmul(aix[o], Ks));
+          if (AMASK & (1 << o)) v = vfma(alv[o], f0, v);
 #pragma unroll
-          for (int qq = 0; qq < NP; qq++) {
-            const Cx<TC> pv = e ? hi(P[qq]) : lo(P[qq]);
-            const Cx<TC> t2 = cmul<TC>(p.cb_r[o][qq], p.cb_i[o][qq], pv);
-            v.r += t2.r;
-            v.i += t2.i;
-          }
-          const Cx<TC> tk = cmul<TC>(p.ck_r[o], p.ck_i[o], f);
-          v.r += tk.r;
-          v.i += tk.i;
+          for (int qq = 0; qq < NP; qq++)
+            if (BMASK & (1 << (o * 8 + qq))) v = vfma(bev[o][qq], e ? P[qq].b : P[qq].a, v);
           res[o][e] = v;
         }
 
         if (EPI & EPI_KAHAN) {
-          // res[0] is the increment delta; compensated add to psi.
-          // slot convention: psi = P[0] when NP >= 2 (else the stencil
-          // field itself), compensation = P[NP-1]
-          const Cx<TC> psi = (NP >= 2) ? (e ? hi(P[0]) : lo(P[0])) : f0;
-          const Cx<TC> cc = e ? hi(P[NP - 1]) : lo(P[NP - 1]);
-          const Cx<TC> y = {res[0][e].r - cc.r, res[0][e].i - cc.i};
-          const Cx<TC> tt = {psi.r + y.r, psi.i + y.i};
-          res[1][e] = {(tt.r - psi.r) - y.r, (tt.i - psi.i) - y.i};
+          // res[0] is the increment delta; compensated add to psi.  Slots:
+          // psi = P[0] when NP >= 2 (else the stencil field), c = P[NP-1].
+          const V psi = (NP >= 2) ? (e ? P[0].b : P[0].a) : f0;
+          const V cc = e ? P[NP > 0 ? NP - 1 : 0].b : P[NP > 0 ? NP - 1 : 0].a;
+          const V y = vfma(cc, mone, res[0][e]);
+          const V tt = vadd(psi, y);
+          res[1][e] = vfma(y, mone, vfma(psi, mone, tt));
           res[0][e] = tt;
         }
 
         if (ok && (EPI & EPI_NORM)) {
-          const double vr = (double)res[0][e].r, vi = (double)res[0][e].i;
-          red0 += (Wx[e] * Wy) * Wz * (vr * vr + vi * vi);
+          const double vr = (double)res[0][e].x, vi = (double)res[0][e].y;
+          red0 = fma(Wxy[e] * Wz, fma(vr, vr, vi * vi), red0);
         }
         if (ok && (EPI & EPI_ERR)) {
-          double er = p.cek_r * (double)f.r - p.cek_i * (double)f.i;
-          double ei = p.cek_r * (double)f.i + p.cek_i * (double)f.r;
+          // err = sum_q ce[q] P_q + cek (x) K; psi = P[0], k1 = P[1]
+          const double kr = (double)Kv.x, ki = (double)Kv.y;
+          double er = p.cek_r * kr - p.cek_i * ki;
+          double ei = p.cek_r * ki + p.cek_i * kr;
 #pragma unroll
-          for (int qq = 0; qq < NP; qq++) {
-            const Cx<TC> pv = e ? hi(P[qq]) : lo(P[qq]);
-            er += p.ce_r[qq] * (double)pv.r - p.ce_i[qq] * (double)pv.i;
-            ei += p.ce_r[qq] * (double)pv.i + p.ce_i[qq] * (double)pv.r;
+          for (int qq = 1; qq < NP; qq++) {
+            const V pv = e ? P[qq].b : P[qq].a;
+            er = fma(p.ce[qq], (double)pv.x, er);
+            ei = fma(p.ce[qq], (double)pv.y, ei);
           }
-          // slot convention: psi = P[0], k1 = dt f(psi) = P[1]
-          const Cx<TC> psi0 = e ? hi(P[0]) : lo(P[0]);
-          const Cx<TC> k1 = e ? hi(P[1]) : lo(P[1]);
-          const double apsi = hypot((double)psi0.r, (double)psi0.i);
-          const double m = hypot((double)k1.r, (double)k1.i) * p.inv_absdt;
+          const V psi0 = e ? P[0].b : P[0].a;
+          const V k1 = e ? P[NP > 1 ? 1 : 0].b : P[NP > 1 ? 1 : 0].a;
+          const double apsi = hypot((double)psi0.x, (double)psi0.y);
+          const double m = hypot((double)k1.x, (double)k1.y) * p.inv_absdt;
           const double sr = apsi + p.dt0_r * m + 1e-30, si = p.dt0_i * m;
-          const double ratio = hypot(er, ei) / hypot(sr, si);
-          red1 = fmax(red1, ratio);
+          red1 = fmax(red1, hypot(er, ei) / hypot(sr, si));
         }
       }
 
       if (!(EPI & EPI_ENERGY)) {
+        long gzo[2] = {0, 0};
+        if (near_edge(z, p.nz)) {
+          int a, b;
+          ghost_targets(z, p.nz, p.bcs, a, b);
+          gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
+          gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
+        }
+        const bool edge = edge_xy || ((gzo[0] | gzo[1]) != 0);
 #pragma unroll
         for (int o = 0; o < NOUT; o++) {
-          TS* out = p.out[o];
-          const Pair<TS> pv = cvt_pair<TS>(Pair<TC>{res[o][0].r, res[o][0].i,
-                                                    res[o][1].r, res[o][1].i});
+          TS* out = p.out[o] + 2 * base;
           if (ok1) {
-            st_pair<TS>(out + 2 * gidx(i0, j, z), pv);
+            st_cpair<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
+                                              cvt_v<TS>(res[o][1]));
           } else if (ok0) {
-            st_one<TS>(out + 2 * gidx(i0, j, z), pv.r0, pv.i0);
+            st_c1<TS>(out, res[o][0]);
           }
-          if (p.ghost_mask & (1 << o)) {
+          if (edge && (p.ghost_mask & (1 << o))) {
 #pragma unroll
             for (int e = 0; e < 2; e++) {
               if (!(e ? ok1 : ok0)) continue;
-              const int i = i0 + e;
-              const TS vr = e ? pv.r1 : pv.r0, vi = e ? pv.i1 : pv.i0;
-              if (gxa[e] != NO_GHOST) st_one<TS>(out + 2 * gidx(gxa[e], j, z), vr, vi);
-              if (gxb[e] != NO_GHOST) st_one<TS>(out + 2 * gidx(gxb[e], j, z), vr, vi);
-              if (gya != NO_GHOST) st_one<TS>(out + 2 * gidx(i, gya, z), vr, vi);
-              if (gyb != NO_GHOST) st_one<TS>(out + 2 * gidx(i, gyb, z), vr, vi);
-              if (gza != NO_GHOST) st_one<TS>(out + 2 * gidx(i, j, gza), vr, vi);
-              if (gzb != NO_GHOST) st_one<TS>(out + 2 * gidx(i, j, gzb), vr, vi);
+              TS* o1 = out + 2 * e;
+              const V v = res[o][e];
+              if (gxo[e][0]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gxo[e][0], v);
+              if (gxo[e][1]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gxo[e][1], v);
+              if (gyo[0]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gyo[0], v);
+              if (gyo[1]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gyo[1], v);
+              if (gzo[0]) st_c1<TS>(o1 + 2 * gzo[0], v);
+              if (gzo[1]) st_c1<TS>(o1 + 2 * gzo[1], v);
             }
           }
         }
       }
+      base += NxNy;
     }
-    __syncthreads();
-    if (s_abort) {
-      t_stop = t;
-      break;
+    if (t >= R) {
+      // this warp no longer reads plane t-R's slot
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[cslot]);
+      if (++cslot == S) cslot = 0;
     }
-    if (t >= R && tid == 0) {
-      const int u = t - R + S;
-      if (u < niters) {
-        fence_proxy_async();
-        issue(u);
-        issued = u + 1;
-      }
+    if (++slot == S) {
+      slot = 0;
+      phase ^= 1u;
+    }
+    ++t;
+    return true;
+  };
+
+  while (!*(volatile int*)&s_abort) {
+    if (!step(IC<0>())) break;
+    if (!step(IC<1>())) break;
+    if (!step(IC<2>())) break;
+    if constexpr (QN > 3) {
+      if (!step(IC<3>())) break;
+      if (!step(IC<4>())) break;
     }
   }
+  }  // compute warps
+
+  __syncthreads();
   // After a timed-out wait, let the copies already in flight land (bounded)
-  // before the CTA's shared memory is released.
-  if (t_stop < niters && tid == 0) {
-    for (int u = t_stop; u < issued; u++)
-      mbar_wait_bounded(&bars[u % S], (uint32_t)((u / S) & 1), p.wait_limit_ns);
+  // before the CTA's shared memory is released: the last load issued into
+  // each slot completes phase (u / S) of that slot's full barrier.
+  if (s_abort && tid == 0) {
+    const int issued = s_issued;
+    for (int u = max(0, issued - S); u < issued; u++)
+      mbar_wait_bounded(&full[u % S], (uint32_t)((u / S) & 1), p.wait_limit_ns);
   }
 
   if (EPI & (EPI_NORM | EPI_ERR | EPI_ENERGY)) {

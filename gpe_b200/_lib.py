@@ -91,6 +91,8 @@ SIGNATURES = {
     "gpe_gpu_stream": (_vp, [_vp]),
     "gpe_gpu_host_alloc": (_vp, [ctypes.c_size_t]),
     "gpe_gpu_host_free": (None, [_vp]),
+    "gpe_gpu_norm_noalloc": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, _dp, _vp]),
 }
 
 _lib = None

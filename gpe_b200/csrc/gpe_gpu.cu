@@ -74,6 +74,9 @@ struct Launch {
 
 }  // namespace
 
+// Shared with noalloc.cu, which has no context to hold its messages.
+void gpe_internal_set_last_error(const std::string& msg) { g_last_create_error = msg; }
+
 struct gpe_ctx {
   gpe_params prm;
   int dev = 0;

@@ -210,6 +210,32 @@ void gpe_gpu_host_free(void* p);
 
 int32_t gpe_gpu_abi_version(void);
 
+/* No counterpart in the reference: an allocation-free get_norm.
+ *
+ * For callers that cannot call cudaMalloc -- hosts whose device memory is
+ * owned by another allocator (a framework's caching allocator, or a driver
+ * that sizes all device memory up front and treats a later allocation as an
+ * error).  Computes the extended-Simpson norm of get_norm
+ * (src/variables.f90:537-559) of psi, a DEVICE array on the current device
+ * in the interior layout (complex64 when elem_bytes = 8, complex128 when 16),
+ * for the grid nx x ny x nz with half-widths xr, yr, zr, and writes it to
+ * *norm_out, a DEVICE double.  No context is needed and nothing is
+ * allocated: the only scratch is a fixed per-process array of
+ * GPE_NOALLOC_MAX_PLANES doubles (one partial sum per z-plane) that every GPU
+ * loading this library holds until exit; nz above that limit is rejected
+ * with GPE_ERR_INVALID.  The work is queued on `stream` (a cudaStream_t, NULL
+ * for the default stream) and is complete once that stream is synchronised.
+ * The first call on a device looks up the scratch array's device address;
+ * make that first call before any stream capture.  Every call uses the same
+ * scratch array, so calls that overlap on the GPU (two streams, two host
+ * threads) race and must be serialised by the caller.  Each call writes every
+ * scratch entry it reads, so nothing needs clearing between calls.  Errors:
+ * the status code, with the message from gpe_gpu_last_error(NULL). */
+#define GPE_NOALLOC_MAX_PLANES 8192
+int gpe_gpu_norm_noalloc(const void* psi, int32_t elem_bytes, int32_t nx,
+                         int32_t ny, int32_t nz, double xr, double yr,
+                         double zr, double* norm_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

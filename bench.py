@@ -122,28 +122,6 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------
 
-def random_phase_ic(torch, n, h, kmax, seed, device):
-    """Fourier modes with |k| <= kmax get unit amplitude and a uniform random
-    phase (torch Philox generator, fixed seed); inverse FFT; rescaled to mean
-    density 1."""
-    L = n * h
-    m = torch.fft.fftfreq(n, d=1.0 / n, device=device, dtype=torch.float64)
-    k = 2 * math.pi * m / L
-    kz, ky, kx = torch.meshgrid(k, k, k, indexing="ij")
-    mask = (kx * kx + ky * ky + kz * kz) <= kmax * kmax
-    del kx, ky, kz
-    gen = torch.Generator(device=device)
-    gen.manual_seed(seed)
-    phase = torch.rand((n, n, n), generator=gen, device=device, dtype=torch.float64)
-    a = torch.where(mask, torch.exp(2j * math.pi * phase.to(torch.complex128)),
-                    torch.zeros((), dtype=torch.complex128, device=device))
-    del phase, mask
-    psi = torch.fft.ifftn(a)
-    del a
-    psi = psi / torch.sqrt(torch.mean(psi.abs() ** 2))
-    return psi.to(torch.complex64).contiguous()
-
-
 def cpu_sample(threads: int, min_seconds: float = 10.0, max_steps: int = 50):
     """Times the oracle (CPU restatement of the reference path, FP64, the
     reference's own pass structure) on a 512 x 512 x 8 periodic slab of the
@@ -275,7 +253,8 @@ def main():
     prm = GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
                     order=4, precision=8, kahan=True, g=1.0, mu=1.0, device=local)
     s = GpeSolver(prm, tau=DT)
-    psi0 = random_phase_ic(torch, n, H, KMAX, 0, torch.device("cuda", local))
+    from gpe_b200.ic import random_phase
+    psi0 = random_phase(torch, n, H, KMAX, 0, torch.device("cuda", local))
     s.set_state(psi0)
     del psi0
     torch.cuda.empty_cache()

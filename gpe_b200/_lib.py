@@ -89,6 +89,9 @@ SIGNATURES = {
     "gpe_gpu_launch_count": (_i64, [_vp]),
     "gpe_gpu_device_bytes": (_i64, [_vp]),
     "gpe_gpu_stream": (_vp, [_vp]),
+    "gpe_gpu_set_slab": (ctypes.c_int, [_vp, _i32, _i32]),
+    "gpe_gpu_comm_unique_id": (ctypes.c_int, [_vp]),
+    "gpe_gpu_comm_init": (ctypes.c_int, [_vp, _vp, _i32, _i32]),
     "gpe_gpu_host_alloc": (_vp, [ctypes.c_size_t]),
     "gpe_gpu_host_free": (None, [_vp]),
     "gpe_gpu_norm_noalloc": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32, ctypes.c_double,

@@ -9,6 +9,7 @@ struct Geom {
   int nx, ny, nz;  // interior
   int Nx, Ny;      // padded pitches
   int bcs;
+  int zg_lo, zg_hi;  // fill z ghosts below / above locally
 };
 
 __device__ __forceinline__ size_t padded_index(const Geom& g, int i, int j,
@@ -38,8 +39,10 @@ __global__ void unpack_kernel(const TI* __restrict__ src, TS* __restrict__ dst,
     if (a != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, a, k), vr, vi);
     if (b != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, b, k), vr, vi);
     ghost_targets(k, g.nz, g.bcs, a, b);
-    if (a != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, j, a), vr, vi);
-    if (b != NO_GHOST) st_one<TS>(dst + 2 * padded_index(g, i, j, b), vr, vi);
+    if (a != NO_GHOST && ((a < 0) ? g.zg_lo : g.zg_hi))
+      st_one<TS>(dst + 2 * padded_index(g, i, j, a), vr, vi);
+    if (b != NO_GHOST && ((b < 0) ? g.zg_lo : g.zg_hi))
+      st_one<TS>(dst + 2 * padded_index(g, i, j, b), vr, vi);
   }
 }
 

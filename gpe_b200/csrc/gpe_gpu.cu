@@ -8,6 +8,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <cmath>
@@ -60,6 +62,53 @@ thread_local std::string g_last_create_error;
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
+// NCCL, resolved at run time so that the library loads without it and uses
+// the libnccl.so.2 already present in the process when there is one.
+struct NcclApi {
+  bool ok = false;
+  ncclResult_t (*GetUniqueId)(ncclUniqueId*) = nullptr;
+  ncclResult_t (*CommInitRank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*CommDestroy)(ncclComm_t) = nullptr;
+  ncclResult_t (*Send)(const void*, size_t, ncclDataType_t, int, ncclComm_t,
+                       cudaStream_t) = nullptr;
+  ncclResult_t (*Recv)(void*, size_t, ncclDataType_t, int, ncclComm_t,
+                       cudaStream_t) = nullptr;
+  ncclResult_t (*AllReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t,
+                            ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*GroupStart)() = nullptr;
+  ncclResult_t (*GroupEnd)() = nullptr;
+  const char* (*GetErrorString)(ncclResult_t) = nullptr;
+};
+NcclApi g_nccl;
+
+bool load_nccl(std::string* why) {
+  if (g_nccl.ok) return true;
+  void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+  if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+  if (!h) {
+    *why = "libnccl.so.2 not found";
+    return false;
+  }
+#define GPE_SYM(field, name)                                             \
+  g_nccl.field = reinterpret_cast<decltype(g_nccl.field)>(dlsym(h, name)); \
+  if (!g_nccl.field) {                                                   \
+    *why = std::string("NCCL symbol missing: ") + name;                  \
+    return false;                                                        \
+  }
+  GPE_SYM(GetUniqueId, "ncclGetUniqueId")
+  GPE_SYM(CommInitRank, "ncclCommInitRank")
+  GPE_SYM(CommDestroy, "ncclCommDestroy")
+  GPE_SYM(Send, "ncclSend")
+  GPE_SYM(Recv, "ncclRecv")
+  GPE_SYM(AllReduce, "ncclAllReduce")
+  GPE_SYM(GroupStart, "ncclGroupStart")
+  GPE_SYM(GroupEnd, "ncclGroupEnd")
+  GPE_SYM(GetErrorString, "ncclGetErrorString")
+#undef GPE_SYM
+  g_nccl.ok = true;
+  return true;
+}
+
 struct LaunchShape {
   int TY, S, zchunk, ntx, nty, nchunks;
   size_t smem;
@@ -83,6 +132,11 @@ struct gpe_ctx {
   cudaStream_t stream = nullptr;
   int nx, ny, nz, Nx, Ny, Nz;
   int num_sms = 148;
+  // z-slab of a global grid (single domain: nzg == nz, z_off == 0)
+  int nzg = 0, z_off = 0;
+  ncclComm_t comm = nullptr;
+  int rank = 0, nranks = 1, nbr_lo = 0, nbr_hi = 0;
+  bool exch_lo = false, exch_hi = false;  // z ghosts come from a neighbour
   size_t npad, nint;
   int es;  // bytes per stored complex element (8 or 16)
   double dx, dy, dz;
@@ -191,6 +245,50 @@ int get_map(gpe_ctx* c, int field, int kind, int TY, int R,
                 "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   c->maps[key] = m;
   *out = m;
+  return GPE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// z-slab halo exchange.  The two boundary planes of a stencil field go to
+// the z-neighbours' ghost planes: sends "up" (my top planes -> the upper
+// neighbour's lower ghosts) then "down", receives "from below" (into my
+// lower ghosts) then "from above".  NCCL matches sends and receives per peer
+// in issue order, so this order is right for any rank count, including two
+// ranks (both neighbours are the same peer) and one rank with periodic
+// wrap-around (both neighbours are the rank itself).
+
+#define NCCL_CHECK(c, call)                                                  \
+  do {                                                                       \
+    ncclResult_t r_ = (call);                                                \
+    if (r_ != ncclSuccess)                                                   \
+      return fail((c), GPE_ERR_CUDA, std::string(#call) + ": " +             \
+                                         g_nccl.GetErrorString(r_));         \
+  } while (0)
+
+int exchange_ghosts(gpe_ctx* c, int field) {
+  if (!c->comm || !(c->exch_lo || c->exch_hi)) return GPE_OK;
+  const size_t plane = (size_t)c->Nx * c->Ny * (size_t)c->es;  // bytes
+  unsigned char* f = static_cast<unsigned char*>(c->fld[field]);
+  // padded plane index pz = z + 2
+  unsigned char* bottom = f + 2 * plane;                    // z = 0, 1
+  unsigned char* top = f + (size_t)c->nz * plane;           // z = nz-2, nz-1
+  unsigned char* ghost_lo = f;                              // z = -2, -1
+  unsigned char* ghost_hi = f + (size_t)(c->nz + 2) * plane; // z = nz, nz+1
+  const size_t n = 2 * plane;
+  NCCL_CHECK(c, g_nccl.GroupStart());
+  if (c->exch_hi) NCCL_CHECK(c, g_nccl.Send(top, n, ncclUint8, c->nbr_hi, c->comm, c->stream));
+  if (c->exch_lo) NCCL_CHECK(c, g_nccl.Send(bottom, n, ncclUint8, c->nbr_lo, c->comm, c->stream));
+  if (c->exch_lo) NCCL_CHECK(c, g_nccl.Recv(ghost_lo, n, ncclUint8, c->nbr_lo, c->comm, c->stream));
+  if (c->exch_hi) NCCL_CHECK(c, g_nccl.Recv(ghost_hi, n, ncclUint8, c->nbr_hi, c->comm, c->stream));
+  NCCL_CHECK(c, g_nccl.GroupEnd());
+  return GPE_OK;
+}
+
+// Sum (op 0) or max (op 1) of `count` doubles of d_scal across the ranks.
+int allreduce_scalars(gpe_ctx* c, int first, int count, int op) {
+  if (!c->comm || c->nranks < 2) return GPE_OK;
+  NCCL_CHECK(c, g_nccl.AllReduce(c->d_scal + first, c->d_scal + first, (size_t)count,
+                                 ncclFloat64, op ? ncclMax : ncclSum, c->comm, c->stream));
   return GPE_OK;
 }
 
@@ -369,6 +467,8 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   p.stencil = static_cast<const TS*>(c->fld[sp.stencil]);
   for (int o = 0; o < sp.nout; o++) p.out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
   p.ghost_mask = sp.ghost_mask;
+  p.zg_lo = c->exch_lo ? 0 : 1;
+  p.zg_hi = c->exch_hi ? 0 : 1;
   const double h2[3] = {c->dx * c->dx, c->dy * c->dy, c->dz * c->dz};
   double c1[3], c2[3];
   for (int a = 0; a < 3; a++) {
@@ -467,6 +567,11 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   }
   c->launches++;
   c->last_nblk = (int)nblk;
+  for (int o = 0; o < sp.nout; o++)
+    if (sp.ghost_mask & (1 << o)) {
+      rc = exchange_ghosts(c, sp.out[o]);
+      if (rc) return rc;
+    }
   return GPE_OK;
 }
 
@@ -487,6 +592,8 @@ Geom geom(const gpe_ctx* c) {
   Geom g;
   g.nx = c->nx; g.ny = c->ny; g.nz = c->nz; g.Nx = c->Nx; g.Ny = c->Ny;
   g.bcs = c->prm.bcs;
+  g.zg_lo = c->exch_lo ? 0 : 1;
+  g.zg_hi = c->exch_hi ? 0 : 1;
   return g;
 }
 
@@ -520,7 +627,7 @@ int finalize(gpe_ctx* c, int nblk, int slot, int op, double scale,
   CU_CHECK(c, cudaGetLastError());
   end_timed(c, L);
   c->launches++;
-  return GPE_OK;
+  return allreduce_scalars(c, out_index, 1, op);
 }
 
 double cell_volume(const gpe_ctx* c) { return c->dx * c->dy * c->dz; }
@@ -790,9 +897,14 @@ int do_step(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
 // --------------------------------------------------------------------------
 // Tables and allocation.
 
+// Per-axis tables.  Along z a context may hold the slab z_off .. z_off+nz-1
+// of a global axis of nzg planes: coordinates, sponge edge and norm weights
+// follow the global index.
 int build_tables(gpe_ctx* c) {
   const gpe_params& p = c->prm;
   const int n[3] = {c->nx, c->ny, c->nz};
+  const int ng[3] = {c->nx, c->ny, c->nzg};
+  const int zoff[3] = {0, 0, c->z_off};
   const std::vector<double>* crd[3] = {&c->x, &c->y, &c->z};
   const double om[3] = {p.omx, p.omy, p.omz};
   size_t total = 0;
@@ -834,9 +946,11 @@ int build_tables(gpe_ctx* c) {
     double* w = reinterpret_cast<double*>(&h[offs[a][4]]);
     double* xx = reinterpret_cast<double*>(&h[offs[a][5]]);
     const std::vector<double>& X = *crd[a];
-    const int N = n[a];
-    // sponge edge a = x(nx-3) (src/solve.f90:397-409)
-    const double edge = X[N - 3];
+    const int N = n[a], NG = ng[a], O = zoff[a];
+    const double h = (a == 0) ? c->dx : (a == 1) ? c->dy : c->dz;
+    const double r = (a == 0) ? p.xr : (a == 1) ? p.yr : p.zr;
+    // sponge edge a = x(nx-3) of the global axis (src/solve.f90:397-409)
+    const double edge = -r + (double)(NG - 3) * h;
     for (int i = 0; i < N; i++) {
       const double v = 0.5 * ((om[a] * om[a]) * (X[i] * X[i]));
       const double d = p.diss_amp * (1.0 + std::tanh(X[i] - edge) * std::tanh(X[i] + edge));
@@ -853,13 +967,14 @@ int build_tables(gpe_ctx* c) {
       w[N - 3] += W3; w[N - 2] += W2; w[N - 1] += W1;
     } else {
       for (int i = 0; i < N; i++) {
+        const int gi = O + i;
         double t = 1.0;
-        if (i == 0) t = W1;
-        if (i == 1) t = W2;
-        if (i == 2) t = W3;
-        if (i == N - 3) t = W3;
-        if (i == N - 2) t = W2;
-        if (i == N - 1) t = W1;
+        if (gi == 0) t = W1;
+        if (gi == 1) t = W2;
+        if (gi == 2) t = W3;
+        if (gi == NG - 3) t = W3;
+        if (gi == NG - 2) t = W2;
+        if (gi == NG - 1) t = W1;
         w[i] = t;
       }
     }
@@ -924,7 +1039,7 @@ int stage_in(gpe_ctx* c, const void* src, int elem_bytes, bool device) {
     CU_CHECK(c, cudaMemsetAsync(c->fld[c->c_id], 0, c->npad * (size_t)c->es,
                                 c->stream));
   c->norm_valid = false;
-  return GPE_OK;
+  return exchange_ghosts(c, c->psi_id);
 }
 
 int stage_out(gpe_ctx* c, int field, void* dst, int elem_bytes, bool device) {
@@ -1054,6 +1169,8 @@ int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
   c->npad = (size_t)c->Nx * c->Ny * c->Nz;
   c->nint = (size_t)p.nx * p.ny * p.nz;
   c->es = p.precision;
+  c->nzg = p.nz;
+  c->z_off = 0;
   // get_grid, src/ic.f90:32-69
   c->dx = (p.xr - (-p.xr)) / (double)(p.nx - 1);
   c->dy = (p.yr - (-p.yr)) / (double)(p.ny - 1);
@@ -1113,6 +1230,7 @@ void gpe_gpu_destroy(gpe_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->comm && g_nccl.ok) g_nccl.CommDestroy(c->comm);
   for (int i = 0; i < F_COUNT; i++)
     if (c->fld[i]) cudaFree(c->fld[i]);
   if (c->d_tables) cudaFree(c->d_tables);
@@ -1374,6 +1492,65 @@ int gpe_gpu_get_timing(gpe_ctx* c, gpe_timing* out) {
 int64_t gpe_gpu_launch_count(const gpe_ctx* c) { return c ? c->launches : -1; }
 
 int64_t gpe_gpu_device_bytes(const gpe_ctx* c) { return c ? c->device_bytes : -1; }
+
+int gpe_gpu_set_slab(gpe_ctx* c, int32_t nz_global, int32_t z_offset) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nz_global < 6 || z_offset < 0 || z_offset + c->nz > nz_global)
+    return fail(c, GPE_ERR_INVALID, "slab does not fit in the global z axis");
+  if (c->prm.bcs == 2 && c->nz < 4 && nz_global > c->nz)
+    return fail(c, GPE_ERR_INVALID, "reflective slabs need at least 4 planes");
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  c->nzg = nz_global;
+  c->z_off = z_offset;
+  // get_grid on the global axis, keeping this slab's planes
+  c->dz = (c->prm.zr - (-c->prm.zr)) / (double)(nz_global - 1);
+  for (int k = 0; k < c->nz; k++) c->z[k] = -c->prm.zr + (double)(z_offset + k) * c->dz;
+  if (c->d_tables) {
+    cudaFree(c->d_tables);
+    c->d_tables = nullptr;
+  }
+  rc = build_tables(c);
+  if (rc) return rc;
+  c->norm_valid = false;
+  return GPE_OK;
+}
+
+int gpe_gpu_comm_unique_id(void* id128) {
+  if (!id128) return fail(nullptr, GPE_ERR_INVALID, "id buffer is null");
+  std::string why;
+  if (!load_nccl(&why)) return fail(nullptr, GPE_ERR_CUDA, why);
+  ncclUniqueId id;
+  const ncclResult_t r = g_nccl.GetUniqueId(&id);
+  if (r != ncclSuccess)
+    return fail(nullptr, GPE_ERR_CUDA, std::string("ncclGetUniqueId: ") + g_nccl.GetErrorString(r));
+  memcpy(id128, &id, sizeof(id));
+  return GPE_OK;
+}
+
+int gpe_gpu_comm_init(gpe_ctx* c, const void* id128, int32_t rank, int32_t nranks) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!id128 || nranks < 1 || rank < 0 || rank >= nranks)
+    return fail(c, GPE_ERR_INVALID, "bad communicator arguments");
+  if (c->comm) return fail(c, GPE_ERR_INVALID, "communicator already set");
+  std::string why;
+  if (!load_nccl(&why)) return fail(c, GPE_ERR_CUDA, why);
+  ncclUniqueId id;
+  memcpy(&id, id128, sizeof(id));
+  NCCL_CHECK(c, g_nccl.CommInitRank(&c->comm, nranks, id, rank));
+  c->rank = rank;
+  c->nranks = nranks;
+  c->nbr_lo = (rank - 1 + nranks) % nranks;
+  c->nbr_hi = (rank + 1) % nranks;
+  // periodic: every rank trades both faces (one rank trades with itself);
+  // reflective: the bottom and top ranks mirror their outer faces locally
+  const bool periodic = c->prm.bcs == 1;
+  c->exch_lo = periodic || rank > 0;
+  c->exch_hi = periodic || rank < nranks - 1;
+  c->norm_valid = false;
+  return GPE_OK;
+}
 
 void* gpe_gpu_stream(const gpe_ctx* c) {
   return c ? static_cast<void*>(c->stream) : nullptr;

@@ -73,6 +73,8 @@ struct StageParams {
   const TS* stencil;    // stencil field (padded layout), warm-up planes
   TS* out[2];           // output fields (padded layout)
   int ghost_mask;       // bit o set: out[o] gets its boundary ghosts filled
+  int zg_lo, zg_hi;     // fill the z ghosts below / above locally (else a
+                        // neighbouring rank sends them)
   // Laplacian: T = sum_axes c1*(f1+f-1) + c2*(f2+f-2); L = T + c0*f0
   TC cx1, cx2, cy1, cy2, cz1, cz2, c0lap;
   // x gradient: gx1*(f1-f-1) + gx2*(f2-f-2)
@@ -398,6 +400,8 @@ __global__ void __launch_bounds__(288)
         if (near_edge(z, p.nz)) {
           int a, b;
           ghost_targets(z, p.nz, p.bcs, a, b);
+          if (a != NO_GHOST && !((a < 0) ? p.zg_lo : p.zg_hi)) a = NO_GHOST;
+          if (b != NO_GHOST && !((b < 0) ? p.zg_lo : p.zg_hi)) b = NO_GHOST;
           gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
           gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
         }

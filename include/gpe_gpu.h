@@ -190,6 +190,26 @@ int gpe_gpu_laplacian(gpe_ctx* ctx, void* out, int32_t elem_bytes);
  * src/gpe.f90:251-268 does (real_time flag used by rk45 step control). */
 int gpe_gpu_set_real_time(gpe_ctx* ctx, int32_t real_time);
 
+/* z-slab decomposition (one process per GPU).  The reference distributes
+ * its grid over a (y, z) MPI process grid with a two-plane halo
+ * (src/variables.f90:98-358) and all-reduces its sums and the rk45 error
+ * maximum (src/variables.f90:581, 772, 816; src/solve.f90:189).  Here x and
+ * y stay whole and ranks own consecutive z-slabs.
+ *
+ * gpe_gpu_set_slab: this context (created with nz = the slab's planes) holds
+ * planes z_offset .. z_offset+nz-1 of a global axis of nz_global planes
+ * (prm->zr is the global half-width).  Call before gpe_gpu_set_state. */
+int gpe_gpu_set_slab(gpe_ctx* ctx, int32_t nz_global, int32_t z_offset);
+/* A 128-byte NCCL unique id, made on one rank; the caller broadcasts it. */
+int gpe_gpu_comm_unique_id(void* id128);
+/* Join the ranks' NCCL communicator (rank r owns the r-th slab from the
+ * bottom).  From then on every kernel that writes a stencil field is
+ * followed, on the context's stream, by a send of its two boundary planes
+ * into the z-neighbours' ghost planes, and every norm / energy / rk45 error
+ * reduction by an all-reduce, so all ranks take the same rk45 decision. */
+int gpe_gpu_comm_init(gpe_ctx* ctx, const void* id128, int32_t rank,
+                      int32_t nranks);
+
 /* Per-kernel-family CUDA-event timing (off by default). */
 int gpe_gpu_set_timing(gpe_ctx* ctx, int32_t on);
 int gpe_gpu_get_timing(gpe_ctx* ctx, gpe_timing* out);

@@ -8,5 +8,6 @@ call that needs it does, and raises if it is missing.
 """
 from ._lib import GpeError, LIB_PATH, lib  # noqa: F401
 from .solver import GpeParams, GpeSolver, run_loop  # noqa: F401
+from .batch import BatchOpts, GpeBatch  # noqa: F401
 
 __all__ = ["GpeError", "GpeParams", "GpeSolver", "run_loop", "lib", "LIB_PATH"]

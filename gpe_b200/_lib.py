@@ -61,6 +61,12 @@ class GpeTimingC(ctypes.Structure):
                 ("sites", ctypes.c_int64 * 8)]
 
 
+class GpeBatchOptsC(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_int32), ("tile_y", ctypes.c_int32),
+                ("zchunk", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("use_graph", ctypes.c_int32)]
+
+
 # Every symbol include/gpe_gpu.h declares, with (restype, argtypes).
 _vp, _i32, _i64, _dp = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
@@ -96,6 +102,17 @@ SIGNATURES = {
     "gpe_gpu_host_free": (None, [_vp]),
     "gpe_gpu_norm_noalloc": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_double, _dp, _vp]),
+    "gpe_batch_default_opts": (None, [ctypes.POINTER(GpeBatchOptsC)]),
+    "gpe_batch_create": (ctypes.c_int, [ctypes.POINTER(GpeParamsC), _i32,
+                                        ctypes.POINTER(GpeBatchOptsC), ctypes.POINTER(_vp)]),
+    "gpe_batch_destroy": (None, [_vp]),
+    "gpe_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "gpe_batch_member": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_vp)]),
+    "gpe_batch_advance": (ctypes.c_int, [_vp, _i64, ctypes.c_double, ctypes.c_double, _dp]),
+    "gpe_batch_stream": (_vp, [_vp]),
+    "gpe_batch_launch_count": (_i64, [_vp]),
+    "gpe_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i32),
+                                      ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
 }
 
 _lib = None
@@ -121,4 +138,10 @@ def lib():
 def check(rc: int, ctx=None) -> None:
     if rc != GPE_OK:
         msg = lib().gpe_gpu_last_error(ctx)
+        raise GpeError(rc, msg.decode() if msg else "")
+
+
+def check_batch(rc: int, batch=None) -> None:
+    if rc != GPE_OK:
+        msg = lib().gpe_batch_last_error(batch)
         raise GpeError(rc, msg.decode() if msg else "")

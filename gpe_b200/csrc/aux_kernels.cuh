@@ -138,4 +138,33 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   }
 }
 
+// Batched ensembles: one CTA per run sums slot 0 of the partials of every
+// work item of that run (fixed item order), times scale[r]; out[r] gets the
+// value and, when series is non-null, series[r * cap + *counter] too.
+__global__ void batch_finalize_kernel(const double* __restrict__ partials,
+                                      const int* __restrict__ item_run, int nitems,
+                                      const double* __restrict__ scale,
+                                      double* __restrict__ out,
+                                      double* __restrict__ series, int cap,
+                                      const int* __restrict__ counter) {
+  __shared__ double s[256];
+  const int r = blockIdx.x;
+  double a = 0.0;
+  for (int i = threadIdx.x; i < nitems; i += blockDim.x)
+    if (item_run[i] == r) a += partials[2 * (size_t)i];
+  s[threadIdx.x] = a;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double v = s[0] * scale[r];
+    out[r] = v;
+    if (series) series[(size_t)r * cap + *counter] = v;
+  }
+}
+
+__global__ void bump_counter_kernel(int* counter) { *counter = *counter + 1; }
+
 }  // namespace gpe

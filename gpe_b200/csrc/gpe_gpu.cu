@@ -317,7 +317,31 @@ struct StageSpec {
 
 using KernelFn = const void*;
 
-// Ring depth S and tile height TY from the shared-memory budget, then the
+// Ring depth S and tile height TY from the shared-memory budget: as many
+// slots (up to 8) as fit two CTAs per SM, else one CTA per SM, else TY = 4.
+LaunchShape ring_shape(int es, int R, int np, int tile_y) {
+  LaunchShape s{};
+  int TY = tile_y > 0 ? tile_y : 8;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    s.TY = TY;
+    s.halo_box = (unsigned)((TX + 4) * (TY + 2 * R) * es);
+    s.pt_box = (unsigned)(TX * TY * es);
+    s.halo_smem = (unsigned)round_up(s.halo_box, 128);
+    s.pt_smem = (unsigned)round_up(s.pt_box, 128);
+    const size_t stage = s.halo_smem + (size_t)np * s.pt_smem;
+    int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
+    if (S < R + 3) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
+    if (S >= R + 2 || attempt == 1 || tile_y > 0) {
+      s.S = std::max(S, R + 2);
+      break;
+    }
+    TY = 4;
+  }
+  s.smem = 128 + (size_t)s.S * (s.halo_smem + (size_t)np * s.pt_smem);
+  return s;
+}
+
+// Then the
 // z-chunking from the kernel's real occupancy: among chunk counts, pick the
 // one that minimises (waves of CTAs) x (planes per CTA + pipeline fill),
 // which trades the last wave's idle SMs against the R extra halo planes and
@@ -328,25 +352,7 @@ int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, LaunchShape* out) {
     *out = hit->second;
     return GPE_OK;
   }
-  LaunchShape s{};
-  const int es = c->es;
-  int TY = c->prm.tile_y > 0 ? c->prm.tile_y : 8;
-  for (int attempt = 0; attempt < 2; attempt++) {
-    s.TY = TY;
-    s.halo_box = (unsigned)((TX + 4) * (TY + 2 * R) * es);
-    s.pt_box = (unsigned)(TX * TY * es);
-    s.halo_smem = (unsigned)round_up(s.halo_box, 128);
-    s.pt_smem = (unsigned)round_up(s.pt_box, 128);
-    const size_t stage = s.halo_smem + (size_t)np * s.pt_smem;
-    int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
-    if (S < R + 3) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
-    if (S >= R + 2 || attempt == 1 || c->prm.tile_y > 0) {
-      s.S = std::max(S, R + 2);
-      break;
-    }
-    TY = 4;
-  }
-  s.smem = 128 + (size_t)s.S * (s.halo_smem + (size_t)np * s.pt_smem);
+  LaunchShape s = ring_shape(c->es, R, np, c->prm.tile_y);
   s.ntx = (c->nx + TX - 1) / TX;
   s.nty = (c->ny + s.TY - 1) / s.TY;
   CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -381,12 +387,24 @@ int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, LaunchShape* out) {
 
 // The stage recipes that the schemes use; see stage_kernel.cuh for the
 // meaning of (NP, NOUT, EPI, AMASK, BMASK).  BMASK bit o*8+q: beta[o][q] != 0.
-template <typename TS, typename TC, int R, bool FULL>
+template <typename TS, typename TC, int R, bool FULL, bool BATCH>
 KernelFn pick_kernel(int np, int nout, int epi, int am, int bm) {
 #define GPE_CASE(NP_, NOUT_, EPI_, AM_, BM_)                                   \
   if (np == NP_ && nout == NOUT_ && epi == (EPI_) && am == AM_ && bm == BM_)   \
     return reinterpret_cast<KernelFn>(                                         \
-        &stage_kernel<TS, TC, R, NP_, NOUT_, (EPI_), AM_, BM_, FULL>);
+        &stage_kernel<TS, TC, R, NP_, NOUT_, (EPI_), AM_, BM_, FULL, BATCH>);
+  if constexpr (BATCH) {
+    // batched ensembles step with rk4
+    if constexpr (std::is_same<TS, TC>::value) {
+      GPE_CASE(0, 2, 0, 3, 0)                   // rk4 stage 1
+      GPE_CASE(0, 2, 0, 1, 0)                   // rk4 stage 1 (compensated)
+      GPE_CASE(2, 2, 0, 0, 0x201)               // rk4 stages 2, 3
+      GPE_CASE(1, 1, EPI_NORM, 0, 0x1)          // rk4 stage 4
+      if constexpr (std::is_same<TS, float>::value) {
+        GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM, 0, 0x2)   // rk4 stage 4 (compensated)
+      }
+    }
+  } else {
   if constexpr (std::is_same<TC, double>::value && !FULL) {
     GPE_CASE(0, 0, EPI_ENERGY, 0, 0)
   }
@@ -413,6 +431,7 @@ KernelFn pick_kernel(int np, int nout, int epi, int am, int bm) {
       GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM, 0, 0x2)     // rk4 stage 4
       GPE_CASE(6, 2, EPI_KAHAN | EPI_NORM | EPI_ERR, 0, 0xE)  // rkck stage 6
     }
+  }
   }
 #undef GPE_CASE
   return nullptr;
@@ -457,99 +476,144 @@ void fill_rhs_coeffs(const gpe_ctx* c, double& ar0, double& ard, double& ai,
   }
 }
 
+// The right-hand side coefficients of a context, in the form the kernels
+// take: for the plain right-hand side (no trap, sponge, gradient or sphere)
+// f = i*ai*(cL*L + (c0 + cn|u|^2)u); the kernel forms K = ai*(...) and the
+// factor i moves into the output coefficients (`fold`).
+struct RhsForm {
+  double ar0, ard, ai, cL, c0, cV, cn, U;
+  int ud, uv, us, ug;
+  bool full;
+};
+
+RhsForm rhs_form(const gpe_ctx* c) {
+  RhsForm f;
+  fill_rhs_coeffs(c, f.ar0, f.ard, f.ai, f.cL, f.c0, f.cV, f.cn, f.U, f.ud, f.uv, f.us, f.ug);
+  f.full = f.ud || f.uv || f.us || f.ug;
+  return f;
+}
+
+// Recipe bit masks of a stage (see stage_kernel.cuh).
+void recipe_masks(const StageSpec& sp, int* am, int* bm) {
+  *am = 0;
+  *bm = 0;
+  for (int o = 0; o < sp.nout; o++) {
+    if (sp.alpha[o] != 0.0) *am |= 1 << o;
+    for (int q = 0; q < sp.np; q++)
+      if (sp.beta[o][q] != 0.0) *bm |= 1 << (o * 8 + q);
+  }
+}
+
+// Per-run part of a stage launch.
 template <typename TS, typename TC>
-int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
-  const int R = c->prm.order / 2;
-  StageParams<TS, TC> p;
-  memset(&p, 0, sizeof(p));
-  p.nx = c->nx; p.ny = c->ny; p.nz = c->nz; p.Nx = c->Nx; p.Ny = c->Ny;
-  p.bcs = c->prm.bcs;
-  p.stencil = static_cast<const TS*>(c->fld[sp.stencil]);
-  for (int o = 0; o < sp.nout; o++) p.out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
-  p.ghost_mask = sp.ghost_mask;
-  p.zg_lo = c->exch_lo ? 0 : 1;
-  p.zg_hi = c->exch_hi ? 0 : 1;
+int fill_run(gpe_ctx* c, const StageSpec& sp, int R, const LaunchShape& sh,
+             RhsForm f, RunDesc<TS, TC>* rd, int force_full = -1) {
+  if (force_full >= 0) f.full = force_full != 0;
+  memset(rd, 0, sizeof(*rd));
+  int rc = get_map(c, sp.stencil, 0, sh.TY, R, &rd->maps.halo);
+  if (rc) return rc;
+  for (int q = 0; q < sp.np; q++) {
+    rc = get_map(c, sp.pt[q], 1, sh.TY, R, &rd->maps.pt[q]);
+    if (rc) return rc;
+  }
+  rd->nx = c->nx; rd->ny = c->ny; rd->nz = c->nz; rd->Nx = c->Nx; rd->Ny = c->Ny;
+  rd->ntx = sh.ntx; rd->nty = sh.nty; rd->zchunk = sh.zchunk; rd->nchunks = sh.nchunks;
+  rd->bcs = c->prm.bcs;
+  rd->zg_lo = c->exch_lo ? 0 : 1;
+  rd->zg_hi = c->exch_hi ? 0 : 1;
+  rd->stencil = static_cast<const TS*>(c->fld[sp.stencil]);
+  for (int o = 0; o < sp.nout; o++) rd->out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
   const double h2[3] = {c->dx * c->dx, c->dy * c->dy, c->dz * c->dz};
   double c1[3], c2[3];
   for (int a = 0; a < 3; a++) {
     if (R == 1) { c1[a] = 1.0 / h2[a]; c2[a] = 0.0; }
     else { c1[a] = 16.0 / (12.0 * h2[a]); c2[a] = -1.0 / (12.0 * h2[a]); }
   }
-  p.cx1 = (TC)c1[0]; p.cx2 = (TC)c2[0];
-  p.cy1 = (TC)c1[1]; p.cy2 = (TC)c2[1];
-  p.cz1 = (TC)c1[2]; p.cz2 = (TC)c2[2];
-  p.c0lap = (TC)(-2.0 * (c1[0] + c2[0] + c1[1] + c2[1] + c1[2] + c2[2]));
-  if (R == 1) { p.gx1 = (TC)(1.0 / (2.0 * c->dx)); p.gx2 = (TC)0; }
-  else { p.gx1 = (TC)(8.0 / (12.0 * c->dx)); p.gx2 = (TC)(-1.0 / (12.0 * c->dx)); }
-  double ar0, ard, ai, cL, c0, cV, cn, U;
-  int ud, uv, us, ug;
-  fill_rhs_coeffs(c, ar0, ard, ai, cL, c0, cV, cn, U, ud, uv, us, ug);
-  const bool full = ud || uv || us || ug;
-  const bool fold = !full && !(sp.epi & (EPI_LAP | EPI_ENERGY));
-  // plain right-hand side: f = i*ai*(cL*L + (c0 + cn|u|^2)u); the kernel
-  // forms K = ai*(...) and the factor i moves into the output coefficients
-  const double sc = full ? 1.0 : ai;
-  p.ar0 = (TC)ar0; p.ard = (TC)ard; p.ai = (TC)ai; p.cL = (TC)(sc * cL);
-  p.c0 = (TC)(sc * c0); p.cV = (TC)cV; p.cn = (TC)(sc * cn); p.U = (TC)U;
-  p.use_diss = ud; p.use_V = uv; p.use_sphere = us; p.use_grad = ug;
+  rd->cx1 = (TC)c1[0]; rd->cx2 = (TC)c2[0];
+  rd->cy1 = (TC)c1[1]; rd->cy2 = (TC)c2[1];
+  rd->cz1 = (TC)c1[2]; rd->cz2 = (TC)c2[2];
+  rd->c0lap = (TC)(-2.0 * (c1[0] + c2[0] + c1[1] + c2[1] + c1[2] + c2[2]));
+  if (R == 1) { rd->gx1 = (TC)(1.0 / (2.0 * c->dx)); rd->gx2 = (TC)0; }
+  else { rd->gx1 = (TC)(8.0 / (12.0 * c->dx)); rd->gx2 = (TC)(-1.0 / (12.0 * c->dx)); }
+  const double sc = f.full ? 1.0 : f.ai;
+  rd->ar0 = (TC)f.ar0; rd->ard = (TC)f.ard; rd->ai = (TC)f.ai; rd->cL = (TC)(sc * f.cL);
+  rd->c0 = (TC)(sc * f.c0); rd->cV = (TC)f.cV; rd->cn = (TC)(sc * f.cn); rd->U = (TC)f.U;
+  rd->use_diss = f.ud; rd->use_V = f.uv; rd->use_sphere = f.us; rd->use_grad = f.ug;
   for (int a = 0; a < 3; a++) {
     if (std::is_same<TC, float>::value) {
-      p.tabV[a] = reinterpret_cast<const TC*>(c->tabVf[a]);
-      p.tabD[a] = reinterpret_cast<const TC*>(c->tabDf[a]);
+      rd->tabV[a] = reinterpret_cast<const TC*>(c->tabVf[a]);
+      rd->tabD[a] = reinterpret_cast<const TC*>(c->tabDf[a]);
     } else {
-      p.tabV[a] = reinterpret_cast<const TC*>(c->tabVd[a]);
-      p.tabD[a] = reinterpret_cast<const TC*>(c->tabDd[a]);
+      rd->tabV[a] = reinterpret_cast<const TC*>(c->tabVd[a]);
+      rd->tabD[a] = reinterpret_cast<const TC*>(c->tabDd[a]);
     }
-    p.tabW[a] = c->tabW[a];
-    p.tabX[a] = c->tabX[a];
+    rd->tabW[a] = c->tabW[a];
+    rd->tabX[a] = c->tabX[a];
   }
-  const cd I(0.0, 1.0);
-  int am = 0, bm = 0;
-  for (int o = 0; o < 2; o++) {
-    p.alpha[o] = (TC)sp.alpha[o];
-    if (o < sp.nout && sp.alpha[o] != 0.0) am |= 1 << o;
-    const cd a = fold ? I * sp.a[o] : sp.a[o];
-    p.a_r[o] = (TC)a.real(); p.a_i[o] = (TC)a.imag();
-    for (int q = 0; q < MAXP; q++) {
-      p.beta[o][q] = (TC)sp.beta[o][q];
-      if (o < sp.nout && q < sp.np && sp.beta[o][q] != 0.0) bm |= 1 << (o * 8 + q);
-    }
-  }
-  for (int q = 0; q < MAXP; q++) p.ce[q] = sp.ce[q];
-  const cd cek = fold ? I * sp.cek : sp.cek;
-  p.cek_r = cek.real(); p.cek_i = cek.imag();
-  p.dt0_r = sp.dt0.real(); p.dt0_i = sp.dt0.imag();
-  p.inv_absdt = sp.inv_absdt;
-  p.eg = c->prm.g; p.emu = c->prm.mu;
-  p.partials = c->d_partials;
-  p.status = c->d_status;
-  p.wait_limit_ns = WAIT_LIMIT_NS;
+  rd->eg = c->prm.g;
+  rd->emu = c->prm.mu;
+  return GPE_OK;
+}
 
-  const bool kfull = full && !(sp.epi & (EPI_LAP | EPI_ENERGY));
-  KernelFn fn;
+// Per-launch part (recipe coefficients, ring shape).
+template <typename TS, typename TC>
+void fill_common(const StageSpec& sp, bool fold, const LaunchShape& sh,
+                 StageParams<TS, TC>* p) {
+  const cd I(0.0, 1.0);
+  p->TY = sh.TY;
+  p->stages = sh.S;
+  p->halo_box_bytes = sh.halo_box; p->pt_box_bytes = sh.pt_box;
+  p->halo_smem_bytes = sh.halo_smem; p->pt_smem_bytes = sh.pt_smem;
+  p->ghost_mask = sp.ghost_mask;
+  for (int o = 0; o < 2; o++) {
+    p->alpha[o] = (TC)sp.alpha[o];
+    const cd a = fold ? I * sp.a[o] : sp.a[o];
+    p->a_r[o] = (TC)a.real(); p->a_i[o] = (TC)a.imag();
+    for (int q = 0; q < MAXP; q++) p->beta[o][q] = (TC)sp.beta[o][q];
+  }
+  for (int q = 0; q < MAXP; q++) p->ce[q] = sp.ce[q];
+  const cd cek = fold ? I * sp.cek : sp.cek;
+  p->cek_r = cek.real(); p->cek_i = cek.imag();
+  p->dt0_r = sp.dt0.real(); p->dt0_i = sp.dt0.imag();
+  p->inv_absdt = sp.inv_absdt;
+  p->wait_limit_ns = WAIT_LIMIT_NS;
+}
+
+template <typename TS, typename TC, bool BATCH>
+KernelFn select_kernel(int R, bool kfull, const StageSpec& sp, int am, int bm) {
   if (R == 1)
-    fn = kfull ? pick_kernel<TS, TC, 1, true>(sp.np, sp.nout, sp.epi, am, bm)
-               : pick_kernel<TS, TC, 1, false>(sp.np, sp.nout, sp.epi, am, bm);
-  else
-    fn = kfull ? pick_kernel<TS, TC, 2, true>(sp.np, sp.nout, sp.epi, am, bm)
-               : pick_kernel<TS, TC, 2, false>(sp.np, sp.nout, sp.epi, am, bm);
+    return kfull ? pick_kernel<TS, TC, 1, true, BATCH>(sp.np, sp.nout, sp.epi, am, bm)
+                 : pick_kernel<TS, TC, 1, false, BATCH>(sp.np, sp.nout, sp.epi, am, bm);
+  return kfull ? pick_kernel<TS, TC, 2, true, BATCH>(sp.np, sp.nout, sp.epi, am, bm)
+               : pick_kernel<TS, TC, 2, false, BATCH>(sp.np, sp.nout, sp.epi, am, bm);
+}
+
+template <typename TS, typename TC>
+int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
+  const int R = c->prm.order / 2;
+  const RhsForm f = rhs_form(c);
+  const bool special = (sp.epi & (EPI_LAP | EPI_ENERGY)) != 0;
+  const bool fold = !f.full && !special;
+  const bool kfull = f.full && !special;
+  int am, bm;
+  recipe_masks(sp, &am, &bm);
+  KernelFn fn = select_kernel<TS, TC, false>(R, kfull, sp, am, bm);
   if (!fn) return fail(c, GPE_ERR_INVALID, "no kernel for this stage shape");
   LaunchShape sh;
   int rc = choose_shape(c, fn, R, sp.np, &sh);
   if (rc) return rc;
-  rc = get_map(c, sp.stencil, 0, sh.TY, R, &p.maps.halo);
+  StageParams<TS, TC> p;
+  memset(&p, 0, sizeof(p));
+  rc = fill_run<TS, TC>(c, sp, R, sh, f, &p.run);
   if (rc) return rc;
-  for (int q = 0; q < sp.np; q++) {
-    rc = get_map(c, sp.pt[q], 1, sh.TY, R, &p.maps.pt[q]);
-    if (rc) return rc;
-  }
-  p.ntx = sh.ntx; p.zchunk = sh.zchunk; p.TY = sh.TY; p.stages = sh.S;
-  p.halo_box_bytes = sh.halo_box; p.pt_box_bytes = sh.pt_box;
-  p.halo_smem_bytes = sh.halo_smem; p.pt_smem_bytes = sh.pt_smem;
+  fill_common<TS, TC>(sp, fold, sh, &p);
+  p.partials = c->d_partials;
+  p.status = c->d_status;
   const size_t nblk = (size_t)sh.ntx * sh.nty * sh.nchunks;
   if (nblk > c->partials_cap)
     return fail(c, GPE_ERR_INVALID, "partials buffer too small");
-  dim3 grid((unsigned)(sh.ntx * sh.nty), (unsigned)sh.nchunks, 1);
+  p.nitems = (int)nblk;
+  dim3 grid((unsigned)nblk, 1, 1);
   dim3 block(32, (unsigned)sh.TY + 1, 1);
   void* args[] = {&p};
   Launch L{};
@@ -703,32 +767,30 @@ int step_rk2(gpe_ctx* c, cd dt) {
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
-int step_rk4(gpe_ctx* c, cd dt) {
+// The four classic RK4 stages (src/solve.f90:109-154) as stage recipes.
+void rk4_specs(const gpe_ctx* c, cd dt, StageSpec sp[4]) {
   const bool K = c->prm.kahan != 0;
   // S1: u2 = psi + dt/2 f(psi); acc = [psi] + dt/6 f(psi)
-  StageSpec s1;
+  StageSpec& s1 = sp[0];
+  s1 = StageSpec();
   s1.stencil = c->psi_id; s1.nout = 2; s1.out[0] = F_UA; s1.out[1] = F_ACC;
   s1.ghost_mask = 1; s1.alpha[0] = 1.0; s1.a[0] = 0.5 * dt;
   s1.alpha[1] = K ? 0.0 : 1.0; s1.a[1] = dt / 6.0;
   s1.family = GPE_FAM_STAGE_FIRST;
-  int rc = launch_stage(c, s1);
-  if (rc) return rc;
   // S2: u3 = psi + dt/2 f(u2); acc += dt/3 f(u2)
-  StageSpec s2;
+  StageSpec& s2 = sp[1];
+  s2 = StageSpec();
   s2.stencil = F_UA; s2.np = 2; s2.pt[0] = c->psi_id; s2.pt[1] = F_ACC;
   s2.nout = 2; s2.out[0] = F_UB; s2.out[1] = F_ACC; s2.ghost_mask = 1;
   s2.beta[0][0] = 1.0; s2.a[0] = 0.5 * dt;
   s2.beta[1][1] = 1.0; s2.a[1] = dt / 3.0;
   s2.family = GPE_FAM_STAGE_MID;
-  rc = launch_stage(c, s2);
-  if (rc) return rc;
   // S3: u4 = psi + dt f(u3); acc += dt/3 f(u3)
-  StageSpec s3 = s2;
-  s3.stencil = F_UB; s3.out[0] = F_UA; s3.a[0] = dt;
-  rc = launch_stage(c, s3);
-  if (rc) return rc;
+  sp[2] = s2;
+  sp[2].stencil = F_UB; sp[2].out[0] = F_UA; sp[2].a[0] = dt;
   // S4: psi' = acc + dt/6 f(u4)   (Kahan: psi' = psi (+) (acc + dt/6 f))
-  StageSpec s4;
+  StageSpec& s4 = sp[3];
+  s4 = StageSpec();
   s4.stencil = F_UA; s4.out[0] = c->psi_id; s4.ghost_mask = 1;
   s4.family = GPE_FAM_STAGE_LAST;
   if (K) {
@@ -741,8 +803,15 @@ int step_rk4(gpe_ctx* c, cd dt) {
     s4.beta[0][0] = 1.0; s4.a[0] = dt / 6.0;
     s4.epi = EPI_NORM;
   }
-  rc = launch_stage(c, s4);
-  if (rc) return rc;
+}
+
+int step_rk4(gpe_ctx* c, cd dt) {
+  StageSpec sp[4];
+  rk4_specs(c, dt, sp);
+  for (int st = 0; st < 4; st++) {
+    const int rc = launch_stage(c, sp[st]);
+    if (rc) return rc;
+  }
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
@@ -1085,6 +1154,147 @@ int check_elem(gpe_ctx* c, int elem_bytes, const void* ptr) {
     return fail(c, GPE_ERR_INVALID, "elem_bytes must be 8 or 16");
   if (!ptr) return fail(c, GPE_ERR_INVALID, "null array");
   return GPE_OK;
+}
+
+}  // namespace
+
+// ==========================================================================
+// Batched ensembles: independent runs of uneven grids stepped by one
+// persistent launch per RK4 stage.  Each member is a full context (fields,
+// tables, tensor maps); the batch adds one work list of (run, tile, z-range)
+// items for all members, per-stage arrays of their RunDescs in device memory,
+// and a CUDA graph of one whole step (4 stage launches + per-run norm).
+
+struct gpe_batch {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<gpe_ctx*> runs;
+  gpe_batch_opts opts;
+  int es = 8, R = 1;
+  bool full = false;
+  int TY = 8;
+  WorkItem* d_items = nullptr;
+  int* d_item_run = nullptr;
+  int nitems = 0;
+  double* d_partials = nullptr;
+  double* d_scale = nullptr;
+  double* d_norm = nullptr;
+  double* d_series = nullptr;
+  size_t series_cap = 0;  // steps per run
+  int* d_counter = nullptr;
+  int* d_status = nullptr;
+  void* d_rundesc[4] = {nullptr, nullptr, nullptr, nullptr};
+  struct Stage {
+    KernelFn fn = nullptr;
+    LaunchShape sh{};
+    int grid = 0;
+    std::vector<unsigned char> params;  // StageParams bytes
+  } st[4];
+  cd prepared_dt = cd(0.0, 0.0);
+  bool prepared = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double* graph_series = nullptr;
+  int64_t launches = 0;
+  int64_t sites = 0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(gpe_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  else g_last_create_error = msg;
+  return code;
+}
+
+#define BCU(b, call)                                                          \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return bfail((b), GPE_ERR_CUDA,                                         \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+// Kernels, shapes and RunDesc arrays of the four stages for time step dt.
+template <typename TS, typename TC>
+int batch_prepare_t(gpe_batch* b, cd dt) {
+  for (int s = 0; s < 4; s++) {
+    std::vector<RunDesc<TS, TC>> rds(b->runs.size());
+    StageSpec sp0[4];
+    rk4_specs(b->runs[0], dt, sp0);
+    const StageSpec& sp = sp0[s];
+    int am, bm;
+    recipe_masks(sp, &am, &bm);
+    KernelFn fn = select_kernel<TS, TC, true>(b->R, b->full, sp, am, bm);
+    if (!fn) return bfail(b, GPE_ERR_INVALID, "no batched kernel for this stage");
+    LaunchShape sh = ring_shape(b->es, b->R, sp.np, b->TY);
+    BCU(b, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    int occ = 0;
+    BCU(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (sh.TY + 1), sh.smem));
+    if (occ < 1) return bfail(b, GPE_ERR_INVALID, "batched stage kernel cannot be resident");
+    const int per_sm = b->opts.ctas_per_sm > 0 ? std::min(b->opts.ctas_per_sm, occ) : occ;
+    const int grid = std::min(b->nitems, per_sm * b->runs[0]->num_sms);
+    for (size_t r = 0; r < b->runs.size(); r++) {
+      gpe_ctx* c = b->runs[r];
+      StageSpec spr[4];
+      rk4_specs(c, dt, spr);
+      LaunchShape shr = sh;
+      shr.ntx = (c->nx + TX - 1) / TX;
+      shr.nty = (c->ny + sh.TY - 1) / sh.TY;
+      shr.zchunk = 0;
+      shr.nchunks = 0;
+      const int rc = fill_run<TS, TC>(c, spr[s], b->R, shr, rhs_form(c), &rds[r], b->full ? 1 : 0);
+      if (rc) return bfail(b, rc, c->err);
+    }
+    BCU(b, cudaMemcpy(b->d_rundesc[s], rds.data(), sizeof(RunDesc<TS, TC>) * rds.size(),
+                      cudaMemcpyHostToDevice));
+    StageParams<TS, TC> p;
+    memset(&p, 0, sizeof(p));
+    fill_common<TS, TC>(sp, !b->full, sh, &p);
+    p.runs = static_cast<const RunDesc<TS, TC>*>(b->d_rundesc[s]);
+    p.items = b->d_items;
+    p.nitems = b->nitems;
+    p.partials = b->d_partials;
+    p.status = b->d_status;
+    b->st[s].fn = fn;
+    b->st[s].sh = sh;
+    b->st[s].grid = grid;
+    b->st[s].params.assign(reinterpret_cast<unsigned char*>(&p),
+                           reinterpret_cast<unsigned char*>(&p) + sizeof(p));
+  }
+  b->prepared_dt = dt;
+  b->prepared = true;
+  return GPE_OK;
+}
+
+int batch_prepare(gpe_batch* b, cd dt) {
+  if (b->es == 8) return batch_prepare_t<float, float>(b, dt);
+  return batch_prepare_t<double, double>(b, dt);
+}
+
+// One RK4 step of every member: 4 persistent stage launches, per-run norm
+// into d_norm and the series, step counter bump.
+int batch_enqueue_step(gpe_batch* b) {
+  for (int s = 0; s < 4; s++) {
+    auto& S = b->st[s];
+    void* args[] = {S.params.data()};
+    BCU(b, cudaLaunchKernel(S.fn, dim3((unsigned)S.grid), dim3(32, (unsigned)S.sh.TY + 1),
+                            args, S.sh.smem, b->stream));
+  }
+  batch_finalize_kernel<<<(unsigned)b->runs.size(), 256, 0, b->stream>>>(
+      b->d_partials, b->d_item_run, b->nitems, b->d_scale, b->d_norm, b->d_series,
+      (int)b->series_cap, b->d_counter);
+  bump_counter_kernel<<<1, 1, 0, b->stream>>>(b->d_counter);
+  BCU(b, cudaGetLastError());
+  return GPE_OK;
+}
+
+void batch_drop_graph(gpe_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
 }
 
 }  // namespace
@@ -1569,4 +1779,232 @@ void gpe_gpu_host_free(void* p) {
   if (p) cudaFreeHost(p);
 }
 
+// ----------------------------------------------------------------------------
+// Batched ensembles
+
+void gpe_batch_default_opts(gpe_batch_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(gpe_batch_opts);
+  o->use_graph = 1;
+}
+
+int gpe_batch_create(const gpe_params* prms, int32_t nruns, const gpe_batch_opts* opts,
+                     gpe_batch** out) {
+  if (!out || !prms || nruns < 1) return bfail(nullptr, GPE_ERR_INVALID, "bad batch arguments");
+  *out = nullptr;
+  gpe_batch_opts o;
+  gpe_batch_default_opts(&o);
+  if (opts) {
+    if (opts->struct_size != (int32_t)sizeof(gpe_batch_opts))
+      return bfail(nullptr, GPE_ERR_INVALID, "gpe_batch_opts struct_size mismatch");
+    o = *opts;
+  }
+  if (o.tile_y != 0 && o.tile_y != 4 && o.tile_y != 8)
+    return bfail(nullptr, GPE_ERR_INVALID, "tile_y must be 0, 4 or 8");
+  const gpe_params& p0 = prms[0];
+  for (int r = 0; r < nruns; r++) {
+    const gpe_params& p = prms[r];
+    if (p.scheme != GPE_SCHEME_RK4)
+      return bfail(nullptr, GPE_ERR_INVALID, "batched ensembles step with scheme rk4");
+    if (p.order != p0.order || p.bcs != p0.bcs || p.eqn_to_solve != p0.eqn_to_solve ||
+        p.precision != p0.precision || p.kahan != p0.kahan || p.device != p0.device ||
+        p.real_time != p0.real_time)
+      return bfail(nullptr, GPE_ERR_INVALID,
+                   "batch members must share order, bcs, equation, precision, kahan, "
+                   "device and time direction");
+  }
+  gpe_batch* b = new gpe_batch();
+  b->opts = o;
+  b->dev = p0.device;
+  b->es = p0.precision;
+  b->R = p0.order / 2;
+  b->TY = o.tile_y > 0 ? o.tile_y : 8;
+  auto bail = [&](int rc) {
+    g_last_create_error = b->err;
+    gpe_batch_destroy(b);
+    return rc;
+  };
+  for (int r = 0; r < nruns; r++) {
+    gpe_ctx* c = nullptr;
+    gpe_params pr = prms[r];
+    pr.tile_y = b->TY;
+    const int rc = gpe_gpu_create(&pr, &c);
+    if (rc) {
+      b->err = std::string("member ") + std::to_string(r) + ": " + g_last_create_error;
+      return bail(rc);
+    }
+    b->runs.push_back(c);
+    b->full = b->full || rhs_form(c).full;
+    b->sites += (int64_t)c->nint;
+  }
+  if (cudaSetDevice(b->dev) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    b->err = "stream creation failed";
+    return bail(GPE_ERR_CUDA);
+  }
+  // work list: (run, tile, z-range), largest first
+  std::vector<WorkItem> items;
+  std::vector<long> work;
+  for (int r = 0; r < nruns; r++) {
+    const gpe_ctx* c = b->runs[r];
+    const int ntx = (c->nx + TX - 1) / TX, nty = (c->ny + b->TY - 1) / b->TY;
+    const int zc = o.zchunk > 0 ? o.zchunk : std::min(c->nz, 64);
+    for (int z0 = 0; z0 < c->nz; z0 += zc)
+      for (int t = 0; t < ntx * nty; t++) {
+        const int tx = t % ntx, tyy = t / ntx;
+        const int z1 = std::min(z0 + zc, c->nz);
+        items.push_back(WorkItem{r, t, z0, z1});
+        work.push_back((long)(z1 - z0 + b->R) * std::min(TX, c->nx - tx * TX) *
+                       std::min(b->TY, c->ny - tyy * b->TY));
+      }
+  }
+  std::vector<size_t> order(items.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return work[x] > work[y]; });
+  std::vector<WorkItem> sorted;
+  std::vector<int> item_run;
+  for (size_t i : order) {
+    sorted.push_back(items[i]);
+    item_run.push_back(items[i].run);
+  }
+  b->nitems = (int)sorted.size();
+  std::vector<double> scale;
+  for (auto* c : b->runs) scale.push_back(cell_volume(c));
+  size_t rdsz = (b->es == 8) ? sizeof(RunDesc<float, float>) : sizeof(RunDesc<double, double>);
+  if (cudaMalloc(&b->d_items, sizeof(WorkItem) * sorted.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_item_run, sizeof(int) * item_run.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_partials, 2 * sizeof(double) * sorted.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_scale, sizeof(double) * nruns) != cudaSuccess ||
+      cudaMalloc(&b->d_norm, sizeof(double) * nruns) != cudaSuccess ||
+      cudaMalloc(&b->d_counter, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    b->err = "cudaMalloc of batch buffers failed";
+    return bail(GPE_ERR_OOM);
+  }
+  for (int s = 0; s < 4; s++)
+    if (cudaMalloc(&b->d_rundesc[s], rdsz * nruns) != cudaSuccess) {
+      cudaGetLastError();
+      b->err = "cudaMalloc of run descriptors failed";
+      return bail(GPE_ERR_OOM);
+    }
+  cudaMemcpy(b->d_items, sorted.data(), sizeof(WorkItem) * sorted.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_item_run, item_run.data(), sizeof(int) * item_run.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(b->d_scale, scale.data(), sizeof(double) * nruns, cudaMemcpyHostToDevice);
+  cudaMemset(b->d_counter, 0, sizeof(int));
+  cudaMemset(b->d_status, 0, sizeof(int));
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    b->err = "device synchronisation failed during batch create";
+    return bail(GPE_ERR_CUDA);
+  }
+  *out = b;
+  return GPE_OK;
+}
+
+void gpe_batch_destroy(gpe_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  for (auto* c : b->runs) gpe_gpu_destroy(c);
+  for (int s = 0; s < 4; s++)
+    if (b->d_rundesc[s]) cudaFree(b->d_rundesc[s]);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_item_run) cudaFree(b->d_item_run);
+  if (b->d_partials) cudaFree(b->d_partials);
+  if (b->d_scale) cudaFree(b->d_scale);
+  if (b->d_norm) cudaFree(b->d_norm);
+  if (b->d_series) cudaFree(b->d_series);
+  if (b->d_counter) cudaFree(b->d_counter);
+  if (b->d_status) cudaFree(b->d_status);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+const char* gpe_batch_last_error(const gpe_batch* b) {
+  if (!b) return g_last_create_error.c_str();
+  return b->err.c_str();
+}
+
+int gpe_batch_member(gpe_batch* b, int32_t run, gpe_ctx** ctx) {
+  if (!b || !ctx || run < 0 || run >= (int32_t)b->runs.size())
+    return bfail(b, GPE_ERR_INVALID, "no such batch member");
+  *ctx = b->runs[run];
+  return GPE_OK;
+}
+
+int gpe_batch_advance(gpe_batch* b, int64_t nsteps, double dt_re, double dt_im,
+                      double* norms) {
+  if (!b || nsteps < 0) return bfail(b, GPE_ERR_INVALID, "bad batch advance arguments");
+  BCU(b, cudaSetDevice(b->dev));
+  const cd dt(dt_re, dt_im);
+  const size_t nr = b->runs.size();
+  if ((size_t)nsteps > b->series_cap) {
+    batch_drop_graph(b);
+    if (b->d_series) cudaFree(b->d_series);
+    b->d_series = nullptr;
+    const size_t cap = std::max<size_t>((size_t)nsteps, 64);
+    BCU(b, cudaMalloc(&b->d_series, sizeof(double) * cap * nr));
+    b->series_cap = cap;
+  }
+  if (!b->prepared || dt != b->prepared_dt) {
+    batch_drop_graph(b);
+    const int rc = batch_prepare(b, dt);
+    if (rc) return rc;
+  }
+  // members' own kernels (state loads) must be done before the batch runs
+  for (auto* c : b->runs) BCU(b, cudaStreamSynchronize(c->stream));
+  BCU(b, cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
+  if (b->opts.use_graph && !b->exec) {
+    BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_enqueue_step(b);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return bfail(b, GPE_ERR_CUDA, "graph capture failed");
+    b->graph = g;
+    BCU(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+  }
+  for (int64_t k = 0; k < nsteps; k++) {
+    if (b->exec) {
+      BCU(b, cudaGraphLaunch(b->exec, b->stream));
+    } else {
+      const int rc = batch_enqueue_step(b);
+      if (rc) return rc;
+    }
+    b->launches += 6;
+  }
+  for (auto* c : b->runs) c->norm_valid = false;
+  if (norms && nsteps > 0) {
+    // series is [run][cap]: copy the first nsteps of each run
+    BCU(b, cudaMemcpy2DAsync(norms, sizeof(double) * nsteps, b->d_series,
+                             sizeof(double) * b->series_cap, sizeof(double) * nsteps, nr,
+                             cudaMemcpyDeviceToHost, b->stream));
+  }
+  BCU(b, cudaStreamSynchronize(b->stream));
+  int st = 0;
+  BCU(b, cudaMemcpy(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) return bfail(b, GPE_ERR_TIMEOUT, "device-side wait limit expired in a batched stage");
+  return GPE_OK;
+}
+
+void* gpe_batch_stream(const gpe_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+int64_t gpe_batch_launch_count(const gpe_batch* b) { return b ? b->launches : -1; }
+
+int gpe_batch_info(const gpe_batch* b, int64_t* sites, int32_t* nitems, int32_t* grid,
+                   int32_t* tile_y) {
+  if (!b) return GPE_ERR_INVALID;
+  if (sites) *sites = b->sites;
+  if (nitems) *nitems = b->nitems;
+  if (grid) *grid = b->st[1].grid;
+  if (tile_y) *tile_y = b->TY;
+  return GPE_OK;
+}
+
 }  // extern "C"
+

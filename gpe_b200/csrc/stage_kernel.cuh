@@ -62,19 +62,19 @@ struct TileMaps {
   CUtensorMap pt[MAXP];  // pointwise fields, box 64 x TY x 1
 };
 
+// Everything one run contributes to a stage launch: its geometry, fields,
+// tensor maps, discretisation coefficients and tables.
 template <typename TS, typename TC>
-struct StageParams {
-  TileMaps maps;
+struct alignas(64) RunDesc {
+  TileMaps maps;        // 64-byte aligned tensor maps (first member)
   int nx, ny, nz;       // interior extents
   int Nx, Ny;           // padded pitches (complex elements)
-  int ntx, zchunk, bcs, TY, stages;
-  unsigned int halo_box_bytes, pt_box_bytes;    // bytes one TMA box delivers
-  unsigned int halo_smem_bytes, pt_smem_bytes;  // 128-aligned slot strides
-  const TS* stencil;    // stencil field (padded layout), warm-up planes
-  TS* out[2];           // output fields (padded layout)
-  int ghost_mask;       // bit o set: out[o] gets its boundary ghosts filled
+  int ntx, nty, zchunk, nchunks;
+  int bcs;
   int zg_lo, zg_hi;     // fill the z ghosts below / above locally (else a
                         // neighbouring rank sends them)
+  const TS* stencil;    // stencil field (padded layout), warm-up planes
+  TS* out[2];           // output fields (padded layout)
   // Laplacian: T = sum_axes c1*(f1+f-1) + c2*(f2+f-2); L = T + c0*f0
   TC cx1, cx2, cy1, cy2, cz1, cz2, c0lap;
   // x gradient: gx1*(f1-f-1) + gx2*(f2-f-2)
@@ -88,6 +88,24 @@ struct StageParams {
   const TC* tabD[3];      // per-axis sponge terms (times diss_amp)
   const double* tabW[3];  // per-axis norm weights
   const double* tabX[3];  // coordinates (sphere mask)
+  double eg, emu;         // energy: g, mu
+};
+
+// A work item: run, tile (tile_x + ntx * tile_y) and z range [z0, z1).
+struct WorkItem {
+  int run, tile, z0, z1;
+};
+
+template <typename TS, typename TC>
+struct StageParams {
+  RunDesc<TS, TC> run;           // single-run launch: item i = (tile, chunk)
+  const RunDesc<TS, TC>* runs;   // batched launch: per-run descriptors
+  const WorkItem* items;         // batched launch: the work list
+  int nitems;
+  int TY, stages;
+  unsigned int halo_box_bytes, pt_box_bytes;    // bytes one TMA box delivers
+  unsigned int halo_smem_bytes, pt_smem_bytes;  // 128-aligned slot strides
+  int ghost_mask;       // bit o set: out[o] gets its boundary ghosts filled
   TC alpha[2];
   TC beta[2][MAXP];
   TC a_r[2], a_i[2];
@@ -95,8 +113,7 @@ struct StageParams {
   double ce[MAXP], cek_r, cek_i;
   double dt0_r, dt0_i;    // dt of the first attempt (psi_scal)
   double inv_absdt;       // 1/|dt| of this attempt (|f(psi)| = |k1|/|dt|)
-  double eg, emu;         // energy: g, mu
-  double* partials;       // 2 doubles per CTA
+  double* partials;       // 2 doubles per work item
   int* status;
   unsigned long long wait_limit_ns;
 };
@@ -109,10 +126,11 @@ template <int K>
 using IC = std::integral_constant<int, K>;
 
 template <typename TS, typename TC, int R, int NP, int NOUT, int EPI, int AMASK,
-          int BMASK, bool FULL>
+          int BMASK, bool FULL, bool BATCH>
 __global__ void __launch_bounds__(288)
     stage_kernel(const __grid_constant__ StageParams<TS, TC> p) {
   using V = typename VT<TC>::T;
+  using RD = RunDesc<TS, TC>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_abort, s_issued;
   __shared__ double s_red[2][32];
@@ -123,21 +141,25 @@ __global__ void __launch_bounds__(288)
   constexpr unsigned ES = 2 * sizeof(TS);   // bytes per stored complex
   const int TY = p.TY, S = p.stages;
   const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
-  const int tile_x = blockIdx.x % p.ntx, tile_y = blockIdx.x / p.ntx;
-  const int z0 = blockIdx.y * p.zchunk;
-  const int z1 = min(z0 + p.zchunk, p.nz);
-  const int niters = (z1 - z0) + R;
-  const int i0 = tile_x * TX + 2 * lane;
-  const int j = tile_y * TY + ty;
-  const bool ok0 = (i0 < p.nx) && (j < p.ny);
-  const bool ok1 = (i0 + 1 < p.nx) && (j < p.ny);
+
+  // item it -> run descriptor, tile and z range
+  auto item_of = [&](int it) -> WorkItem {
+    if (BATCH) return p.items[it];
+    const int ntiles = p.run.ntx * p.run.nty;
+    const int ch = it / ntiles;
+    const int z0 = ch * p.run.zchunk;
+    return WorkItem{0, it - ch * ntiles, z0, min(z0 + p.run.zchunk, p.run.nz)};
+  };
+  auto run_of = [&](const WorkItem& w) -> const RD& {
+    if (BATCH) return p.runs[w.run];
+    return p.run;
+  };
 
   // shared memory: full[S] and empty[S] barriers (S <= 8), then the slots
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + 8;
   unsigned char* sbase = smem + 128;
   const unsigned stride = p.halo_smem_bytes + (unsigned)NP * p.pt_smem_bytes;
-  const size_t Nx = (size_t)p.Nx, NxNy = (size_t)p.Nx * (size_t)p.Ny;
 
   if (tid == 0) {
     for (int s = 0; s < S; s++) {
@@ -150,66 +172,65 @@ __global__ void __launch_bounds__(288)
   }
   __syncthreads();
 
-  double red0 = 0.0, red1 = 0.0;
   if (ty == TY) {
     // ---------------- producer warp: lane 0 streams the planes -------------
+    // Planes of successive items follow each other through the ring, so the
+    // next item's first planes load while the current item drains.
     if (lane == 0) {
-      prefetch_tmap(&p.maps.halo);
-#pragma unroll
-      for (int qq = 0; qq < NP; qq++) prefetch_tmap(&p.maps.pt[qq]);
-      int slot = 0;
+      int slot = 0, issued = 0;
       uint32_t cyc = 0;  // completed passes over the ring
-      for (int u = 0; u < niters; u++) {
-        if (cyc > 0) {
-          // the slot's previous plane must have been released by every
-          // compute warp
-          if (!mbar_wait_bounded(&empty[slot], (cyc - 1) & 1u, p.wait_limit_ns)) {
-            s_abort = 1;
-            atomicExch(p.status, 6);
+      bool stop = false;
+      for (int it = blockIdx.x; it < p.nitems && !stop; it += gridDim.x) {
+        const WorkItem w = item_of(it);
+        const RD& rd = run_of(w);
+        const int tile_x = w.tile % rd.ntx, tile_y = w.tile / rd.ntx;
+        const int niters = (w.z1 - w.z0) + R;
+        prefetch_tmap(&rd.maps.halo);
+#pragma unroll
+        for (int qq = 0; qq < NP; qq++) prefetch_tmap(&rd.maps.pt[qq]);
+        for (int u = 0; u < niters; u++) {
+          if (cyc > 0) {
+            // the slot's previous plane must have been released by every
+            // compute warp
+            if (!mbar_wait_bounded(&empty[slot], (cyc - 1) & 1u, p.wait_limit_ns)) {
+              s_abort = 1;
+              atomicExch(p.status, 6);
+              stop = true;
+              break;
+            }
+            fence_proxy_async();
+          }
+          unsigned char* st = sbase + (size_t)slot * stride;
+          const bool with_pt = (NP > 0) && (u >= R);
+          mbar_arrive_expect_tx(&full[slot],
+                                p.halo_box_bytes + (with_pt ? NP * p.pt_box_bytes : 0u));
+          tma_load_3d(st, &rd.maps.halo, &full[slot], W * tile_x * TX,
+                      tile_y * TY + GH - R, w.z0 + u + GH);
+          if (with_pt) {
+#pragma unroll
+            for (int qq = 0; qq < NP; qq++)
+              tma_load_3d(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
+                          &rd.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
+                          tile_y * TY + GH, w.z0 + u - R + GH);
+          }
+          s_issued = ++issued;
+          if (++slot == S) {
+            slot = 0;
+            ++cyc;
+          }
+          if (*(volatile int*)&s_abort) {
+            stop = true;
             break;
           }
-          fence_proxy_async();
         }
-        unsigned char* st = sbase + (size_t)slot * stride;
-        const bool with_pt = (NP > 0) && (u >= R);
-        mbar_arrive_expect_tx(&full[slot],
-                              p.halo_box_bytes + (with_pt ? NP * p.pt_box_bytes : 0u));
-        tma_load_3d(st, &p.maps.halo, &full[slot], W * tile_x * TX,
-                    tile_y * TY + GH - R, z0 + u + GH);
-        if (with_pt) {
-#pragma unroll
-          for (int qq = 0; qq < NP; qq++)
-            tma_load_3d(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
-                        &p.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
-                        tile_y * TY + GH, z0 + u - R + GH);
-        }
-        s_issued = u + 1;
-        if (++slot == S) {
-          slot = 0;
-          ++cyc;
-        }
-        if (*(volatile int*)&s_abort) break;
       }
     }
   } else {
-  // Per-thread constants.
-  TC Vxy[2] = {TC(0), TC(0)}, Dxy[2] = {TC(0), TC(0)};
-  double Wxy[2] = {0.0, 0.0};
-  if ((FULL || (EPI & EPI_ENERGY)) && p.use_V) {
-    Vxy[0] = p.tabV[0][i0] + p.tabV[1][j];
-    Vxy[1] = p.tabV[0][i0 + 1] + p.tabV[1][j];
-  }
-  if (FULL && p.use_diss) {
-    Dxy[0] = p.tabD[0][i0] + p.tabD[1][j];
-    Dxy[1] = p.tabD[0][i0 + 1] + p.tabD[1][j];
-  }
-  if (EPI & EPI_NORM) {
-    Wxy[0] = p.tabW[0][i0] * p.tabW[1][j];
-    Wxy[1] = p.tabW[0][i0 + 1] * p.tabW[1][j];
-  }
-  const V cx1 = vsplat(p.cx1), cx2 = vsplat(p.cx2), cy1 = vsplat(p.cy1),
-          cy2 = vsplat(p.cy2), cz1 = vsplat(p.cz1), cz2 = vsplat(p.cz2),
-          c0l = vsplat(p.c0lap), cLv = vsplat(p.cL);
+  // ------------------------------ compute warps ------------------------------
+  int slot = 0, cslot = 0;
+  uint32_t phase = 0;
+  const unsigned row_off = ES * (unsigned)((ty + R) * HW + 2 * lane + 2);
+  const unsigned pt_off = ES * (unsigned)(ty * TX + 2 * lane);
   V ar[2], aix[2], alv[2], bev[2][NP > 0 ? NP : 1];
 #pragma unroll
   for (int o = 0; o < 2; o++) {
@@ -220,19 +241,61 @@ __global__ void __launch_bounds__(288)
     for (int qq = 0; qq < (NP > 0 ? NP : 1); qq++) bev[o][qq] = vsplat(p.beta[o][qq]);
   }
   const V mone = vsplat(TC(-1));
+
+  for (int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+  const WorkItem w = item_of(it);
+  const RD& rd = run_of(w);
+  const int nx = rd.nx, ny = rd.ny, nz = rd.nz, bcs = rd.bcs;
+  const int zg_lo = rd.zg_lo, zg_hi = rd.zg_hi;
+  const int tile_x = w.tile % rd.ntx, tile_y = w.tile / rd.ntx;
+  const int z0 = w.z0;
+  const int niters = (w.z1 - w.z0) + R;
+  const int i0 = tile_x * TX + 2 * lane;
+  const int j = tile_y * TY + ty;
+  const bool ok0 = (i0 < nx) && (j < ny);
+  const bool ok1 = (i0 + 1 < nx) && (j < ny);
+  const size_t Nx = (size_t)rd.Nx, NxNy = (size_t)rd.Nx * (size_t)rd.Ny;
+  TS* const outp[2] = {rd.out[0], rd.out[1]};
+  const TC c0s = rd.c0, cns = rd.cn, cVs = rd.cV, ar0 = rd.ar0, ard = rd.ard, ais = rd.ai;
+  const TC Us = rd.U, gx1 = rd.gx1, gx2 = rd.gx2;
+  const int useV = rd.use_V, useD = rd.use_diss, useS = rd.use_sphere, useG = rd.use_grad;
+  const TC* const tabVz = rd.tabV[2];
+  const TC* const tabDz = rd.tabD[2];
+  const double* const tabWz = rd.tabW[2];
+  const double eg = rd.eg, emu = rd.emu;
+  const V cx1 = vsplat(rd.cx1), cx2 = vsplat(rd.cx2), cy1 = vsplat(rd.cy1),
+          cy2 = vsplat(rd.cy2), cz1 = vsplat(rd.cz1), cz2 = vsplat(rd.cz2),
+          c0l = vsplat(rd.c0lap), cLv = vsplat(rd.cL);
+  double red0 = 0.0, red1 = 0.0;
+
+  // Per-thread constants of this item.
+  TC Vxy[2] = {TC(0), TC(0)}, Dxy[2] = {TC(0), TC(0)};
+  double Wxy[2] = {0.0, 0.0};
+  if ((FULL || (EPI & EPI_ENERGY)) && useV) {
+    Vxy[0] = rd.tabV[0][i0] + rd.tabV[1][j];
+    Vxy[1] = rd.tabV[0][i0 + 1] + rd.tabV[1][j];
+  }
+  if (FULL && useD) {
+    Dxy[0] = rd.tabD[0][i0] + rd.tabD[1][j];
+    Dxy[1] = rd.tabD[0][i0 + 1] + rd.tabD[1][j];
+  }
+  if (EPI & EPI_NORM) {
+    Wxy[0] = rd.tabW[0][i0] * rd.tabW[1][j];
+    Wxy[1] = rd.tabW[0][i0 + 1] * rd.tabW[1][j];
+  }
   // Ghost copies this thread's sites feed, as element offsets from the site
   // (x and y fixed per thread; z per plane, uniform across the CTA).
   int gxo[2][2], gyo[2];
   {
     int a, b;
     for (int e = 0; e < 2; e++) {
-      ghost_targets(i0 + e, p.nx, p.bcs, a, b);
+      ghost_targets(i0 + e, nx, bcs, a, b);
       gxo[e][0] = (a != NO_GHOST) ? a - (i0 + e) : 0;
       gxo[e][1] = (b != NO_GHOST) ? b - (i0 + e) : 0;
     }
-    ghost_targets(j, p.ny, p.bcs, a, b);
-    gyo[0] = (a != NO_GHOST) ? (a - j) * p.Nx : 0;
-    gyo[1] = (b != NO_GHOST) ? (b - j) * p.Nx : 0;
+    ghost_targets(j, ny, bcs, a, b);
+    gyo[0] = (a != NO_GHOST) ? (a - j) * rd.Nx : 0;
+    gyo[1] = (b != NO_GHOST) ? (b - j) * rd.Nx : 0;
   }
   const bool edge_xy = (gxo[0][0] | gxo[0][1] | gxo[1][0] | gxo[1][1] | gyo[0] | gyo[1]) != 0;
   // element offset of this thread's first site in plane z0
@@ -244,16 +307,13 @@ __global__ void __launch_bounds__(288)
 #pragma unroll
   for (int w = 0; w < R; w++) {
     CPair<TC> v = {vsplat(TC(0)), vsplat(TC(0))};
-    if (ok0) v = ld_cpair<TS, TC>(p.stencil + 2 * (base - (size_t)(R - w) * NxNy));
+    if (ok0) v = ld_cpair<TS, TC>(rd.stencil + 2 * (base - (size_t)(R - w) * NxNy));
     q[w] = v;
   }
 #pragma unroll
   for (int w = R; w < QN; w++) q[w] = {vsplat(TC(0)), vsplat(TC(0))};
 
-  int t = 0, slot = 0, cslot = 0;
-  uint32_t phase = 0;
-  const unsigned row_off = ES * (unsigned)((ty + R) * HW + 2 * lane + 2);
-  const unsigned pt_off = ES * (unsigned)(ty * TX + 2 * lane);
+  int t = 0;
 
   auto step = [&](auto kc) -> bool {
     constexpr int KK = decltype(kc)::value;
@@ -289,9 +349,9 @@ __global__ void __launch_bounds__(288)
       }
       TC Vz = TC(0), Dz = TC(0);
       double Wz = 0.0;
-      if ((FULL || (EPI & EPI_ENERGY)) && p.use_V) Vz = p.tabV[2][z];
-      if (FULL && p.use_diss) Dz = p.tabD[2][z];
-      if (EPI & EPI_NORM) Wz = p.tabW[2][z];
+      if ((FULL || (EPI & EPI_ENERGY)) && useV) Vz = tabVz[z];
+      if (FULL && useD) Dz = tabDz[z];
+      if (EPI & EPI_NORM) Wz = tabWz[z];
 
       V res[2][2];  // [output][site]
 #pragma unroll
@@ -318,8 +378,8 @@ __global__ void __launch_bounds__(288)
             const double d2 = fr * fr + fi * fi;
             const double kin = -(lr * fr + li * fi);
             red0 += kin + 0.5 * (d2 * d2);
-            red1 += 0.5 * kin + (double)(Vxy[e] + Vz) * d2 + 0.5 * p.eg * d2 * d2 -
-                    p.emu * d2;
+            red1 += 0.5 * kin + (double)(Vxy[e] + Vz) * d2 + 0.5 * eg * d2 * d2 -
+                    emu * d2;
           }
           continue;
         }
@@ -329,21 +389,21 @@ __global__ void __launch_bounds__(288)
         if (EPI & EPI_LAP) {
           Kv = L;
         } else if (!FULL) {
-          const TC s = fma(p.cn, a2, p.c0);
+          const TC s = fma(cns, a2, c0s);
           Kv = vfma(vsplat(s), f0, vmul(cLv, L));
         } else {
-          const TC Vs = p.use_V ? Vxy[e] + Vz : TC(0);
-          const TC s = p.c0 + p.cV * Vs + p.cn * a2;
+          const TC Vs = useV ? Vxy[e] + Vz : TC(0);
+          const TC s = c0s + cVs * Vs + cns * a2;
           const V B = vfma(vsplat(s), f0, vmul(cLv, L));
-          const TC arr = p.use_diss ? p.ar0 + p.ard * (Dxy[e] + Dz) : p.ar0;
-          Kv = vfma(vsplat(arr), B, vmul(vpair(-p.ai, p.ai), vswap(B)));
-          if (p.use_grad) {
-            V gx = vmul(vsplat(p.gx1), vfma(xm1, mone, xp1));
-            if (R == 2) gx = vfma(vsplat(p.gx2), vfma(xm2, mone, xp2), gx);
-            Kv = vfma(vsplat(p.U), gx, Kv);
+          const TC arr = useD ? ar0 + ard * (Dxy[e] + Dz) : ar0;
+          Kv = vfma(vsplat(arr), B, vmul(vpair(-ais, ais), vswap(B)));
+          if (useG) {
+            V gx = vmul(vsplat(gx1), vfma(xm1, mone, xp1));
+            if (R == 2) gx = vfma(vsplat(gx2), vfma(xm2, mone, xp2), gx);
+            Kv = vfma(vsplat(Us), gx, Kv);
           }
-          if (p.use_sphere) {
-            const double X = p.tabX[0][i0 + e], Y = p.tabX[1][j], Z = p.tabX[2][z];
+          if (useS) {
+            const double X = rd.tabX[0][i0 + e], Y = rd.tabX[1][j], Z = rd.tabX[2][z];
             const TC m = (TC)(0.5 * (1.0 + tanh(sqrt(X * X + Y * Y + Z * Z) - 10.0 - 2.0)));
             Kv = vmul(vsplat(m), Kv);
           }
@@ -397,18 +457,18 @@ __global__ void __launch_bounds__(288)
 
       if (!(EPI & EPI_ENERGY)) {
         long gzo[2] = {0, 0};
-        if (near_edge(z, p.nz)) {
+        if (near_edge(z, nz)) {
           int a, b;
-          ghost_targets(z, p.nz, p.bcs, a, b);
-          if (a != NO_GHOST && !((a < 0) ? p.zg_lo : p.zg_hi)) a = NO_GHOST;
-          if (b != NO_GHOST && !((b < 0) ? p.zg_lo : p.zg_hi)) b = NO_GHOST;
+          ghost_targets(z, nz, bcs, a, b);
+          if (a != NO_GHOST && !((a < 0) ? zg_lo : zg_hi)) a = NO_GHOST;
+          if (b != NO_GHOST && !((b < 0) ? zg_lo : zg_hi)) b = NO_GHOST;
           gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
           gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
         }
         const bool edge = edge_xy || ((gzo[0] | gzo[1]) != 0);
 #pragma unroll
         for (int o = 0; o < NOUT; o++) {
-          TS* out = p.out[o] + 2 * base;
+          TS* out = outp[o] + 2 * base;
           if (ok1) {
             st_cpair<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
                                               cvt_v<TS>(res[o][1]));
@@ -456,6 +516,36 @@ __global__ void __launch_bounds__(288)
       if (!step(IC<4>())) break;
     }
   }
+  if (t < niters) break;  // aborted
+  // Hand back the item's last R planes, still held for their x/y neighbours.
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[cslot]);
+    if (++cslot == S) cslot = 0;
+  }
+
+  if (EPI & (EPI_NORM | EPI_ERR | EPI_ENERGY)) {
+    // per-item partials; only the compute warps take part (named barrier 1)
+    red0 = warp_sum(red0);
+    red1 = (EPI & EPI_ERR) ? warp_max(red1) : warp_sum(red1);
+    if (lane == 0) {
+      s_red[0][ty] = red0;
+      s_red[1][ty] = red1;
+    }
+    named_barrier_sync(1, 32 * TY);
+    if (tid == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w2 = 0; w2 < TY; w2++) {
+        a += s_red[0][w2];
+        b = (EPI & EPI_ERR) ? fmax(b, s_red[1][w2]) : b + s_red[1][w2];
+      }
+      p.partials[2 * (size_t)it + 0] = a;
+      p.partials[2 * (size_t)it + 1] = b;
+    }
+    named_barrier_sync(1, 32 * TY);
+  }
+  }  // items
   }  // compute warps
 
   __syncthreads();
@@ -466,26 +556,6 @@ __global__ void __launch_bounds__(288)
     const int issued = s_issued;
     for (int u = max(0, issued - S); u < issued; u++)
       mbar_wait_bounded(&full[u % S], (uint32_t)((u / S) & 1), p.wait_limit_ns);
-  }
-
-  if (EPI & (EPI_NORM | EPI_ERR | EPI_ENERGY)) {
-    red0 = warp_sum(red0);
-    red1 = (EPI & EPI_ERR) ? warp_max(red1) : warp_sum(red1);
-    if (lane == 0) {
-      s_red[0][ty] = red0;
-      s_red[1][ty] = red1;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double a = 0.0, b = 0.0;
-      for (int w = 0; w < TY; w++) {
-        a += s_red[0][w];
-        b = (EPI & EPI_ERR) ? fmax(b, s_red[1][w]) : b + s_red[1][w];
-      }
-      const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
-      p.partials[2 * blk + 0] = a;
-      p.partials[2 * blk + 1] = b;
-    }
   }
 }
 

@@ -210,6 +210,39 @@ int gpe_gpu_comm_unique_id(void* id128);
 int gpe_gpu_comm_init(gpe_ctx* ctx, const void* id128, int32_t rank,
                       int32_t nranks);
 
+/* Batched ensembles (no reference counterpart; the reference runs one grid
+ * per job).  Independent runs of uneven grids, each a full member context,
+ * are stepped together with rk4: every stage is ONE persistent launch over a
+ * work list of (run, tile, z-range) items of all members, and a whole step
+ * (4 stage launches + per-run norm) is captured once in a CUDA graph and
+ * replayed.  Members share scheme (rk4), order, bcs, equation, precision,
+ * kahan, device and time direction; grids, box sizes, g, mu and trap may
+ * differ. */
+typedef struct gpe_batch gpe_batch;
+typedef struct gpe_batch_opts {
+  int32_t struct_size;  /* sizeof(gpe_batch_opts) */
+  int32_t tile_y;       /* 0 = auto (8); else 4 or 8 */
+  int32_t zchunk;       /* 0 = auto (min(nz, 64)); z-planes per work item */
+  int32_t ctas_per_sm;  /* 0 = as many as fit */
+  int32_t use_graph;    /* 1 = replay a captured CUDA graph per step */
+} gpe_batch_opts;
+void gpe_batch_default_opts(gpe_batch_opts* opts);
+int gpe_batch_create(const gpe_params* prms, int32_t nruns,
+                     const gpe_batch_opts* opts, gpe_batch** out);
+void gpe_batch_destroy(gpe_batch* batch);
+const char* gpe_batch_last_error(const gpe_batch* batch);
+/* Member context of run `run` (for set_state / get_state / norm / energy;
+ * owned by the batch). */
+int gpe_batch_member(gpe_batch* batch, int32_t run, gpe_ctx** ctx);
+/* nsteps rk4 steps of every member with time step dt; norms (HOST, may be
+ * NULL) receives nruns x nsteps values, run-major. */
+int gpe_batch_advance(gpe_batch* batch, int64_t nsteps, double dt_re,
+                      double dt_im, double* norms);
+void* gpe_batch_stream(const gpe_batch* batch);
+int64_t gpe_batch_launch_count(const gpe_batch* batch);
+int gpe_batch_info(const gpe_batch* batch, int64_t* sites, int32_t* nitems,
+                   int32_t* grid, int32_t* tile_y);
+
 /* Per-kernel-family CUDA-event timing (off by default). */
 int gpe_gpu_set_timing(gpe_ctx* ctx, int32_t on);
 int gpe_gpu_get_timing(gpe_ctx* ctx, gpe_timing* out);

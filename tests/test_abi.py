@@ -18,7 +18,7 @@ HEADER = os.path.join(ROOT, "include", "gpe_gpu.h")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = set(re.findall(r"\b(gpe_gpu_\w+)\s*\(", src))
+    names = set(re.findall(r"\b(gpe_(?:gpu|batch)_\w+)\s*\(", src))
     return names
 
 
@@ -33,7 +33,7 @@ def test_every_declared_symbol_is_exported(L):
     assert len(names) >= 20
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
                          text=True, check=True).stdout
-    exported = set(re.findall(r"\bT (gpe_gpu_\w+)", out))
+    exported = set(re.findall(r"\bT (gpe_(?:gpu|batch)_\w+)", out))
     assert names == exported, (names ^ exported)
     for n in names:
         assert hasattr(L, n)
@@ -84,3 +84,30 @@ def test_null_context_calls_are_rejected(L):
     assert L.gpe_gpu_norm(None, None) == 1
     assert L.gpe_gpu_launch_count(None) == -1
     L.gpe_gpu_destroy(None)
+
+
+def test_batch_create_validates_members_without_gpu(L):
+    p = (_lib.GpeParamsC * 2)()
+    for q in p:
+        L.gpe_gpu_default_params(ctypes.byref(q), 16, 16, 16)
+    o = _lib.GpeBatchOptsC()
+    L.gpe_batch_default_opts(ctypes.byref(o))
+    assert o.struct_size == ctypes.sizeof(_lib.GpeBatchOptsC) and o.use_graph == 1
+    h = ctypes.c_void_p()
+    # members must share order / bcs / precision
+    p[1].order = 4
+    assert L.gpe_batch_create(p, 2, ctypes.byref(o), ctypes.byref(h)) == 1 and not h
+    assert b"share" in L.gpe_batch_last_error(None)
+    p[1].order = 2
+    p[1].scheme = 3  # batches step with rk4 only
+    assert L.gpe_batch_create(p, 2, ctypes.byref(o), ctypes.byref(h)) == 1
+    p[1].scheme = 2
+    o.tile_y = 5
+    assert L.gpe_batch_create(p, 2, ctypes.byref(o), ctypes.byref(h)) == 1
+    o.tile_y = 0
+    o.struct_size = 4
+    assert L.gpe_batch_create(p, 2, ctypes.byref(o), ctypes.byref(h)) == 1
+    assert L.gpe_batch_create(p, 0, None, ctypes.byref(h)) == 1
+    assert L.gpe_batch_advance(None, 1, 0.01, 0.0, None) == 1
+    assert L.gpe_batch_launch_count(None) == -1
+    L.gpe_batch_destroy(None)

@@ -9,6 +9,14 @@ FP64 norm reduction every step; seeded random-phase initial condition
 Metric: site-updates/s (sites x steps / device time), whole job.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py --workload ensemble [--steps 500]
+
+--workload ensemble: 64 independent complex64 runs, cubic grids drawn from
+{32,48,64,96,128}^3 with seed 0, h = 0.5, harmonic trap omega ~ U[0.05, 0.15],
+random-phase IC (|k| <= 0.8) times the Thomas-Fermi profile, 2nd-order FD,
+reflective boundaries, RK4 dt = 0.01, 500 steps; all runs stepped together
+by the batched launches (autotuned launch shape), next to the same runs
+stepped one context at a time.
 
 N > 1 (launched by torchrun): every rank advances its own 512^3 replica
 (weak scaling, no data-path collective); device time is the max over ranks.
@@ -206,6 +214,144 @@ def run_reference(args):
     return 0
 
 
+ENS_RUNS = 64
+ENS_SIZES = (32, 48, 64, 96, 128)
+ENS_DT = 0.01
+ENS_KMAX = 0.8
+# complex64 without compensation: stage 1 reads psi, writes u2, acc (24 B);
+# stages 2-3 read u, psi, acc and write u', acc (40 B); stage 4 reads u4, acc
+# and writes psi (24 B)
+ENS_BYTES_PER_SITE = 128
+
+
+def ensemble_members(seed=0):
+    import numpy as np
+
+    from gpe_b200 import GpeParams
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice(ENS_SIZES, size=ENS_RUNS)
+    omegas = rng.uniform(0.05, 0.15, size=ENS_RUNS)
+    prms = []
+    for n, om in zip(sizes, omegas):
+        n = int(n)
+        xr = H * (n - 1) / 2
+        prms.append(GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4",
+                              eqn_to_solve=4, bcs=2, order=2, precision=8, kahan=False,
+                              g=1.0, mu=1.0, omx=float(om), omy=float(om), omz=float(om)))
+    return prms
+
+
+def run_ensemble(args):
+    """The batched-ensemble workload: one JSON line."""
+    import numpy as np
+    import torch
+
+    from gpe_b200 import GpeBatch, GpeSolver
+    from gpe_b200.autotune import time_steps, tune
+    from gpe_b200.ic import trapped_random_phase
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    prms = ensemble_members()
+    sites = sum(p.nx * p.ny * p.nz for p in prms)
+    host = [trapped_random_phase(torch, p.nx, H, p.omx, ENS_KMAX, 1000 + r, dev).cpu().numpy()
+            for r, p in enumerate(prms)]
+    b = GpeBatch(prms, ENS_DT)
+    b.set_states(host)
+    best, table = tune(b, steps=4)
+    b.set_states(host)
+    b.advance(args.warmup, want_norms=False)
+    b.set_states(host)
+    stream = torch.cuda.ExternalStream(b.stream_handle())
+    sampler = ClockSampler(None)
+    sampler.start()
+    time.sleep(0.3)
+    lc0 = b.launch_count()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    norms = b.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    launches = b.launch_count() - lc0
+    info = b.info()
+    final = [b[r].get_state(np.complex64) for r in range(len(prms))]
+
+    # end to end: host ICs in, all steps, norms and final states out
+    pin = [torch.from_numpy(h).pin_memory() for h in host]
+    t0 = time.perf_counter()
+    e0.record(stream)
+    b.set_states([p.numpy() for p in pin])
+    b.advance(args.steps)
+    outs = [b[r].get_state(np.complex64) for r in range(len(prms))]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    del outs
+    b.close()
+
+    # the same runs stepped one context at a time (one grid per job)
+    seq_ms = 0.0
+    seq_launches = 0
+    seq_err = 0.0
+    for r, p in enumerate(prms):
+        s = GpeSolver(p, dt=ENS_DT)
+        s.set_state(host[r])
+        s.advance(args.warmup)
+        s.set_state(host[r])
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        l0 = s.launch_count()
+        a = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.advance(args.steps)
+        z.record(st)
+        z.synchronize()
+        seq_ms += a.elapsed_time(z)
+        seq_launches += s.launch_count() - l0
+        got = s.get_state(np.complex64)
+        seq_err = max(seq_err, float(np.abs(got - final[r]).max()))
+        s.close()
+
+    peak, peak_kind = load_peaks()
+    value = sites * args.steps / (ms / 1e3)
+    gbs = ENS_BYTES_PER_SITE * sites * args.steps / (ms / 1e3) / 1e9
+    line = {
+        "metric": "site-updates/s (ensemble of 64 uneven trapped runs)", "value": value,
+        "unit": "site-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sizes, traps, phases)",
+        "config": {"workload": "64 complex64 runs, cubic n in {32,48,64,96,128} (seed 0), "
+                               "h=0.5, trap omega~U[0.05,0.15], random phase |k|<=0.8 x TF, "
+                               "order 2, reflective, RK4 dt=0.01",
+                   "sizes": sorted(p.nx for p in prms), "sites": sites,
+                   "l2": f"inputs larger than L2 ({8 * sites * 4 / 1e9:.2f} GB of fields)"},
+        "roofline": {"bound": "hbm", "kernel": "stage_kernel (batched, all four stages)",
+                     "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                     "peak_source": peak_kind, "alg_bytes_per_site_step": ENS_BYTES_PER_SITE,
+                     "traffic": None},
+        "launch": {"best": vars(best), "items": info["items"], "grid": info["grid"],
+                   "table_ms": [(vars(o), t) for o, t in table]},
+        "sequential": {"value": sites * args.steps / (seq_ms / 1e3), "ms_per_step":
+                       seq_ms / args.steps, "launches": seq_launches,
+                       "max_abs_diff_vs_batch": seq_err,
+                       "form": "each run in its own context, advanced alone, one after another"},
+        "speedup_vs_sequential": seq_ms / ms,
+        "e2e": {"value": sites * args.steps / e2e_s, "unit": "site-updates/s",
+                "h2d_bytes_per_step": 8 * sites / args.steps,
+                "d2h_bytes_per_step": (8 * sites + 8 * len(prms) * args.steps) / args.steps,
+                "form": "host ICs -> batch, all steps, per-run norms and final states to host; "
+                        "wall clock"},
+        "clocks": clocks, "gpu_launches": int(launches),
+        "final_norm_min": float(norms[:, -1].min()), "final_norm_max": float(norms[:, -1].max()),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def workload_config(ngpus, n=N_GRID):
     return {"workload": f"{n}^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
                         "(g=mu=1, V=0), complex64 psi + Kahan compensation, FP64 norm per step",
@@ -227,10 +373,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID,
                     help="cube edge (default 512; smaller sizes are for profiling captures)")
+    ap.add_argument("--workload", default="cube", choices=["cube", "ensemble"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ensemble":
+        if "--steps" not in sys.argv:
+            args.steps = 500
+        return run_ensemble(args)
 
     import numpy as np
     import torch

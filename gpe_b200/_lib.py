@@ -109,6 +109,7 @@ SIGNATURES = {
     "gpe_batch_last_error": (ctypes.c_char_p, [_vp]),
     "gpe_batch_member": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_vp)]),
     "gpe_batch_advance": (ctypes.c_int, [_vp, _i64, ctypes.c_double, ctypes.c_double, _dp]),
+    "gpe_batch_set_opts": (ctypes.c_int, [_vp, ctypes.POINTER(GpeBatchOptsC)]),
     "gpe_batch_stream": (_vp, [_vp]),
     "gpe_batch_launch_count": (_i64, [_vp]),
     "gpe_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i32),

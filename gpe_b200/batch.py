@@ -99,6 +99,13 @@ class GpeBatch:
         except Exception:
             pass
 
+    def set_opts(self, opts: BatchOpts) -> None:
+        """Re-plan the stage launches (tile height, z-planes per item, CTAs
+        per SM); states are kept."""
+        o = opts.to_c()
+        check_batch(lib().gpe_batch_set_opts(self._b, ctypes.byref(o)), self._b)
+        self.opts = opts
+
     def set_states(self, states) -> None:
         for m, s in zip(self.members, states):
             m.set_state(s)

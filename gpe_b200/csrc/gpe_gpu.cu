@@ -1290,6 +1290,68 @@ int batch_enqueue_step(gpe_batch* b) {
   return GPE_OK;
 }
 
+const char* bad_opts(const gpe_batch_opts& o) {
+  if (o.tile_y != 0 && o.tile_y != 4 && o.tile_y != 8) return "tile_y must be 0, 4 or 8";
+  if (o.zchunk < 0 || o.ctas_per_sm < 0) return "zchunk and ctas_per_sm must be >= 0";
+  return nullptr;
+}
+
+// The work list of b->opts: every member's (tile, z-range) items, sorted by
+// the sites they touch (warm-up planes included), largest first, so the
+// persistent CTAs' round-robin walk ends on the small items.
+int batch_plan(gpe_batch* b) {
+  const gpe_batch_opts& o = b->opts;
+  b->TY = o.tile_y > 0 ? o.tile_y : 8;
+  std::vector<WorkItem> items;
+  std::vector<long> work;
+  for (int r = 0; r < (int)b->runs.size(); r++) {
+    const gpe_ctx* c = b->runs[r];
+    const int ntx = (c->nx + TX - 1) / TX, nty = (c->ny + b->TY - 1) / b->TY;
+    const int zc = o.zchunk > 0 ? std::min(o.zchunk, c->nz) : std::min(c->nz, 64);
+    for (int z0 = 0; z0 < c->nz; z0 += zc)
+      for (int t = 0; t < ntx * nty; t++) {
+        const int tx = t % ntx, tyy = t / ntx;
+        const int z1 = std::min(z0 + zc, c->nz);
+        items.push_back(WorkItem{r, t, z0, z1});
+        work.push_back((long)(z1 - z0 + 2 * b->R) * std::min(TX, c->nx - tx * TX) *
+                       std::min(b->TY, c->ny - tyy * b->TY));
+      }
+  }
+  std::vector<size_t> order(items.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t x, size_t y) { return work[x] > work[y]; });
+  std::vector<WorkItem> sorted;
+  std::vector<int> item_run;
+  for (size_t i : order) {
+    sorted.push_back(items[i]);
+    item_run.push_back(items[i].run);
+  }
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_item_run) cudaFree(b->d_item_run);
+  if (b->d_partials) cudaFree(b->d_partials);
+  b->d_items = nullptr;
+  b->d_item_run = nullptr;
+  b->d_partials = nullptr;
+  b->nitems = (int)sorted.size();
+  if (cudaMalloc(&b->d_items, sizeof(WorkItem) * sorted.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_item_run, sizeof(int) * item_run.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_partials, 2 * sizeof(double) * sorted.size()) != cudaSuccess) {
+    cudaGetLastError();
+    b->err = "cudaMalloc of the batch work list failed";
+    return GPE_ERR_OOM;
+  }
+  if (cudaMemcpy(b->d_items, sorted.data(), sizeof(WorkItem) * sorted.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_item_run, item_run.data(), sizeof(int) * item_run.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    b->err = "upload of the batch work list failed";
+    return GPE_ERR_CUDA;
+  }
+  b->prepared = false;
+  return GPE_OK;
+}
+
 void batch_drop_graph(gpe_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
@@ -1800,8 +1862,7 @@ int gpe_batch_create(const gpe_params* prms, int32_t nruns, const gpe_batch_opts
       return bfail(nullptr, GPE_ERR_INVALID, "gpe_batch_opts struct_size mismatch");
     o = *opts;
   }
-  if (o.tile_y != 0 && o.tile_y != 4 && o.tile_y != 8)
-    return bfail(nullptr, GPE_ERR_INVALID, "tile_y must be 0, 4 or 8");
+  if (const char* why = bad_opts(o)) return bfail(nullptr, GPE_ERR_INVALID, why);
   const gpe_params& p0 = prms[0];
   for (int r = 0; r < nruns; r++) {
     const gpe_params& p = prms[r];
@@ -1843,39 +1904,14 @@ int gpe_batch_create(const gpe_params* prms, int32_t nruns, const gpe_batch_opts
     b->err = "stream creation failed";
     return bail(GPE_ERR_CUDA);
   }
-  // work list: (run, tile, z-range), largest first
-  std::vector<WorkItem> items;
-  std::vector<long> work;
-  for (int r = 0; r < nruns; r++) {
-    const gpe_ctx* c = b->runs[r];
-    const int ntx = (c->nx + TX - 1) / TX, nty = (c->ny + b->TY - 1) / b->TY;
-    const int zc = o.zchunk > 0 ? o.zchunk : std::min(c->nz, 64);
-    for (int z0 = 0; z0 < c->nz; z0 += zc)
-      for (int t = 0; t < ntx * nty; t++) {
-        const int tx = t % ntx, tyy = t / ntx;
-        const int z1 = std::min(z0 + zc, c->nz);
-        items.push_back(WorkItem{r, t, z0, z1});
-        work.push_back((long)(z1 - z0 + b->R) * std::min(TX, c->nx - tx * TX) *
-                       std::min(b->TY, c->ny - tyy * b->TY));
-      }
+  {
+    const int rc = batch_plan(b);
+    if (rc) return bail(rc);
   }
-  std::vector<size_t> order(items.size());
-  for (size_t i = 0; i < order.size(); i++) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return work[x] > work[y]; });
-  std::vector<WorkItem> sorted;
-  std::vector<int> item_run;
-  for (size_t i : order) {
-    sorted.push_back(items[i]);
-    item_run.push_back(items[i].run);
-  }
-  b->nitems = (int)sorted.size();
   std::vector<double> scale;
   for (auto* c : b->runs) scale.push_back(cell_volume(c));
   size_t rdsz = (b->es == 8) ? sizeof(RunDesc<float, float>) : sizeof(RunDesc<double, double>);
-  if (cudaMalloc(&b->d_items, sizeof(WorkItem) * sorted.size()) != cudaSuccess ||
-      cudaMalloc(&b->d_item_run, sizeof(int) * item_run.size()) != cudaSuccess ||
-      cudaMalloc(&b->d_partials, 2 * sizeof(double) * sorted.size()) != cudaSuccess ||
-      cudaMalloc(&b->d_scale, sizeof(double) * nruns) != cudaSuccess ||
+  if (cudaMalloc(&b->d_scale, sizeof(double) * nruns) != cudaSuccess ||
       cudaMalloc(&b->d_norm, sizeof(double) * nruns) != cudaSuccess ||
       cudaMalloc(&b->d_counter, sizeof(int)) != cudaSuccess ||
       cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess) {
@@ -1889,8 +1925,6 @@ int gpe_batch_create(const gpe_params* prms, int32_t nruns, const gpe_batch_opts
       b->err = "cudaMalloc of run descriptors failed";
       return bail(GPE_ERR_OOM);
     }
-  cudaMemcpy(b->d_items, sorted.data(), sizeof(WorkItem) * sorted.size(), cudaMemcpyHostToDevice);
-  cudaMemcpy(b->d_item_run, item_run.data(), sizeof(int) * item_run.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(b->d_scale, scale.data(), sizeof(double) * nruns, cudaMemcpyHostToDevice);
   cudaMemset(b->d_counter, 0, sizeof(int));
   cudaMemset(b->d_status, 0, sizeof(int));
@@ -1990,6 +2024,18 @@ int gpe_batch_advance(gpe_batch* b, int64_t nsteps, double dt_re, double dt_im,
   BCU(b, cudaMemcpy(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (st) return bfail(b, GPE_ERR_TIMEOUT, "device-side wait limit expired in a batched stage");
   return GPE_OK;
+}
+
+int gpe_batch_set_opts(gpe_batch* b, const gpe_batch_opts* opts) {
+  if (!b || !opts) return bfail(b, GPE_ERR_INVALID, "bad batch arguments");
+  if (opts->struct_size != (int32_t)sizeof(gpe_batch_opts))
+    return bfail(b, GPE_ERR_INVALID, "gpe_batch_opts struct_size mismatch");
+  if (const char* why = bad_opts(*opts)) return bfail(b, GPE_ERR_INVALID, why);
+  BCU(b, cudaSetDevice(b->dev));
+  BCU(b, cudaStreamSynchronize(b->stream));
+  batch_drop_graph(b);
+  b->opts = *opts;
+  return batch_plan(b);
 }
 
 void* gpe_batch_stream(const gpe_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }

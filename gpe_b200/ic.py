@@ -7,6 +7,11 @@ field is transformed to real space and rescaled to mean density 1.  The
 reference's own random_phase (src/ic.f90:190-252) seeds from the clock and
 uses an integer-index cut-off; this is the seeded variant the workloads name.
 
+trapped_random_phase: the ensemble workload's initial condition -- a
+random-phase field of |k| <= k_max times the Thomas-Fermi profile
+sqrt(max(0, 1 - V)) of the harmonic trap V = omega^2 r^2 / 2 on the grid
+x_i = -xr + i h (the reference's get_grid, src/ic.f90:32-69).
+
 vortex_line_pade: a straight vortex line along z through the origin,
 psi = r R(r) e^{i atan2(y, x)} with the Pade core R of get_rr
 (src/ic.f90:888-901).
@@ -38,6 +43,17 @@ def random_phase(torch, n: int, h: float, kmax: float, seed: int, device, dtype=
     del a
     psi = psi / torch.sqrt(torch.mean(psi.abs() ** 2))
     return psi.to(dtype).contiguous()
+
+
+def trapped_random_phase(torch, n: int, h: float, omega: float, kmax: float, seed: int, device,
+                         dtype=None):
+    """(n, n, n) complex tensor: random_phase(...) * sqrt(max(0, 1 - V))."""
+    psi = random_phase(torch, n, h, kmax, seed, device, torch.complex128)
+    xr = (n - 1) * h / 2
+    x = -xr + h * torch.arange(n, device=device, dtype=torch.float64)
+    r2 = x[None, None, :] ** 2 + x[None, :, None] ** 2 + x[:, None, None] ** 2
+    tf = torch.sqrt(torch.clamp(1.0 - 0.5 * omega * omega * r2, min=0.0))
+    return (psi * tf).to(dtype or torch.complex64).contiguous()
 
 
 def vortex_line_pade(x, y, z):

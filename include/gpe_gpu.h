@@ -238,6 +238,9 @@ int gpe_batch_member(gpe_batch* batch, int32_t run, gpe_ctx** ctx);
  * NULL) receives nruns x nsteps values, run-major. */
 int gpe_batch_advance(gpe_batch* batch, int64_t nsteps, double dt_re,
                       double dt_im, double* norms);
+/* Re-plan the launches with new options (the autotuner's knob); the members'
+ * states are kept. */
+int gpe_batch_set_opts(gpe_batch* batch, const gpe_batch_opts* opts);
 void* gpe_batch_stream(const gpe_batch* batch);
 int64_t gpe_batch_launch_count(const gpe_batch* batch);
 int gpe_batch_info(const gpe_batch* batch, int64_t* sites, int32_t* nitems,

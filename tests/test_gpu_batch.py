@@ -171,3 +171,23 @@ def test_batch_rejects_mismatched_members():
         GpeBatch([member((16, 16, 16)), member((16, 16, 16), order=4)], DT)
     with pytest.raises(GpeError):
         GpeBatch([member((16, 16, 16), precision=8), member((16, 16, 16))], DT)
+
+
+def test_autotuner_picks_a_candidate_and_keeps_the_state(tmp_path):
+    from gpe_b200.autotune import tune
+    prms = [member(n, om=0.1) for n in [(32, 32, 32), (48, 48, 48), (20, 28, 12)]]
+    psis = states(prms, 61)
+    exp, _ = singles(prms, psis, 3)
+    cands = [BatchOpts(tile_y=8, zchunk=16), BatchOpts(tile_y=4, zchunk=8, ctas_per_sm=1)]
+    cache = str(tmp_path / "tune.json")
+    with GpeBatch(prms, DT) as b:
+        b.set_states(psis)
+        best, table = tune(b, steps=2, cands=cands, cache_path=cache)
+        assert best in cands and len(table) == 2 and all(ms > 0 for _, ms in table)
+        assert b.opts == best
+        b.advance(3)
+        for r in range(len(prms)):
+            assert np.array_equal(b[r].get_state(), exp[r])
+        # a second tune of the same ensemble is served from the cache
+        best2, table2 = tune(b, cands=cands, cache_path=cache)
+        assert best2 == best and [t for _, t in table2] == [t for _, t in table]

@@ -67,8 +67,15 @@ class GpeBatchOptsC(ctypes.Structure):
                 ("use_graph", ctypes.c_int32)]
 
 
-# Every symbol include/gpe_gpu.h declares, with (restype, argtypes).
+class GpeCnnParamsC(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+                ("nz", ctypes.c_int32), ("device", ctypes.c_int32), ("train", ctypes.c_int32),
+                ("out_scale", ctypes.c_float), ("reserved", ctypes.c_int32)]
+
+
+# Every symbol include/gpe_gpu.h and include/gpe_cnn.h declare, with (restype, argtypes).
 _vp, _i32, _i64, _dp = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
 SIGNATURES = {
     "gpe_gpu_abi_version": (_i32, []),
     "gpe_gpu_default_params": (None, [ctypes.POINTER(GpeParamsC), _i32, _i32, _i32]),
@@ -114,6 +121,20 @@ SIGNATURES = {
     "gpe_batch_launch_count": (_i64, [_vp]),
     "gpe_batch_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i32),
                                       ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+    "gpe_cnn_default_params": (None, [ctypes.POINTER(GpeCnnParamsC), _i32, _i32, _i32]),
+    "gpe_cnn_create": (ctypes.c_int, [ctypes.POINTER(GpeCnnParamsC), ctypes.POINTER(_vp)]),
+    "gpe_cnn_destroy": (None, [_vp]),
+    "gpe_cnn_last_error": (ctypes.c_char_p, [_vp]),
+    "gpe_cnn_set_weights": (ctypes.c_int, [_vp, _fp, _fp]),
+    "gpe_cnn_get_weights": (ctypes.c_int, [_vp, _fp, _fp]),
+    "gpe_cnn_apply": (ctypes.c_int, [_vp, _vp]),
+    "gpe_cnn_attach": (ctypes.c_int, [_vp, _vp]),
+    "gpe_cnn_delta": (ctypes.c_int, [_vp, _vp, _vp]),
+    "gpe_cnn_grad": (ctypes.c_int, [_vp, _vp, _vp, _i32, _dp, _fp, _fp]),
+    "gpe_cnn_train_step": (ctypes.c_int, [_vp, _vp, _vp, _i32, ctypes.c_float, _dp]),
+    "gpe_cnn_adam_reset": (ctypes.c_int, [_vp]),
+    "gpe_cnn_restrict": (ctypes.c_int, [_vp, _vp, _i32]),
+    "gpe_cnn_launch_count": (_i64, [_vp]),
 }
 
 _lib = None
@@ -139,6 +160,12 @@ def lib():
 def check(rc: int, ctx=None) -> None:
     if rc != GPE_OK:
         msg = lib().gpe_gpu_last_error(ctx)
+        raise GpeError(rc, msg.decode() if msg else "")
+
+
+def check_cnn(rc: int, cnn=None) -> None:
+    if rc != GPE_OK:
+        msg = lib().gpe_cnn_last_error(cnn)
         raise GpeError(rc, msg.decode() if msg else "")
 
 

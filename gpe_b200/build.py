@@ -46,14 +46,30 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         return LIB
     cus = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
     tmp = LIB + ".tmp"
-    cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17",
-           "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-           "-I", INCLUDE, "-I", CSRC, "-o", tmp, *cus]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-I", INCLUDE, "-I", CSRC]
     if ptxas_info:
-        cmd.insert(1, "-Xptxas=-v")
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        common.insert(1, "-Xptxas=-v")
+    objs, cmds = [], []
+    for cu in cus:
+        obj = os.path.join(objdir, os.path.basename(cu)[:-3] + ".o")
+        objs.append(obj)
+        cmds.append([*common, "-c", cu, "-o", obj])
+    # translation units compile in parallel, then one link
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+        results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for r in results:
+        sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, r.args)
+    link = [nvcc_path(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
+    subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB
 

@@ -24,6 +24,7 @@
 
 #include "aux_kernels.cuh"
 #include "gpe_gpu.h"
+#include "internal.h"
 #include "stage_kernel.cuh"
 
 using cd = std::complex<double>;
@@ -172,8 +173,31 @@ struct gpe_ctx {
   std::vector<Launch> timed;
   gpe_timing acc_timing;
   std::vector<cudaEvent_t> ev_pool;
+  // enqueued after every completed step (the learned correction)
+  int (*post_step)(void*, gpe_ctx*) = nullptr;
+  void* post_arg = nullptr;
   std::string err;
 };
+
+void gpe_internal_set_post_step(gpe_ctx* c, int (*fn)(void*, gpe_ctx*), void* arg) {
+  if (!c) return;
+  c->post_step = fn;
+  c->post_arg = arg;
+}
+
+int gpe_internal_field_view(gpe_ctx* c, gpe::FieldView* v) {
+  if (!c || !v) return GPE_ERR_INVALID;
+  v->psi = c->fld[c->psi_id];
+  v->nx = c->nx; v->ny = c->ny; v->nz = c->nz; v->Nx = c->Nx; v->Ny = c->Ny;
+  v->es = c->es;
+  v->bcs = c->prm.bcs;
+  v->dev = c->dev;
+  v->single_domain = (c->nranks == 1 && c->nzg == c->nz) ? 1 : 0;
+  v->stream = c->stream;
+  v->status = c->d_status;
+  c->norm_valid = false;
+  return GPE_OK;
+}
 
 namespace {
 
@@ -948,6 +972,10 @@ int do_step(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
       return fail(c, GPE_ERR_SCHEME, "ERROR: Unrecognised time stepping scheme.");
   }
   if (rc) return rc;
+  if (c->post_step) {
+    rc = c->post_step(c->post_arg, c);
+    if (rc) return fail(c, rc, "post-step correction failed");
+  }
   if (c->prm.scheme != GPE_SCHEME_RK45) {
     tm->t = tm->t + dt.real();
     tm->im_t = tm->im_t + std::fabs(dt.imag());
@@ -959,7 +987,8 @@ int do_step(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
       info->dt_did_im = dt.imag();
     }
   }
-  c->norm_valid = true;
+  // the fused norm is of the stepped state, before any post-step correction
+  c->norm_valid = c->post_step == nullptr;
   return GPE_OK;
 }
 

@@ -1,0 +1,182 @@
+"""GPU parity of the learned correction (tcgen05 conv3d kernels) against the
+numpy oracle (oracle/cnn_ref.py) in its bfloat16-emulating mode.
+
+Tolerances: the oracle rounds to bfloat16 where the kernels store bfloat16
+and accumulates in FP64 where the tensor cores accumulate in FP32, so the
+two differ by FP32 accumulation order plus the rare bfloat16 rounding flip it
+causes: delta relative L2 <= 2e-3; loss relative 1e-4 (the loss moves by
+2 |e| |d delta| per site, e the residual, so delta's 1e-3-level differences
+reach it at the 1e-5 level); per-layer weight and
+bias gradients relative L2 <= 2e-2 (gradients pass through three more
+bfloat16 roundings)."""
+import numpy as np
+import pytest
+
+from gpe_b200 import GpeParams, GpeSolver
+from gpe_b200.cnn import CoarseCorrector, init_weights, restrict
+from oracle import cnn_ref as R
+from tests.conftest import rel_l2, random_field
+
+pytestmark = pytest.mark.gpu
+
+
+def solver(n, precision=8, h=0.5, **kw):
+    nx, ny, nz = n
+    prm = GpeParams(nx=nx, ny=ny, nz=nz, xr=(nx - 1) * h / 2, yr=(ny - 1) * h / 2,
+                    zr=(nz - 1) * h / 2, scheme="rk4", eqn_to_solve=4, bcs=1, order=2,
+                    precision=precision, g=1.0, mu=1.0, **kw)
+    return GpeSolver(prm, dt=0.02)
+
+
+def weights(seed, last=0.2):
+    w, b = init_weights(seed)
+    rng = np.random.default_rng(seed + 100)
+    w[3, :, :2, :] = rng.normal(0, last, size=(27, 2, 16))
+    b[:3] = rng.normal(0, 0.05, size=(3, 16))
+    b[3, :2] = rng.normal(0, 0.05, size=2)
+    return w, b
+
+
+SHAPES = [(32, 20, 12), (16, 8, 6), (128, 9, 6), (48, 17, 7)]
+
+
+@pytest.mark.parametrize("n", SHAPES)
+def test_delta_matches_oracle(n):
+    import torch
+    s = solver(n)
+    psi = random_field((n[2], n[1], n[0]), seed=n[0] + n[1]).astype(np.complex64)
+    s.set_state(psi)
+    w, b = weights(1)
+    with CoarseCorrector(*n, train=True, out_scale=0.05) as net:
+        net.set_weights(w, b)
+        d = net.delta(s).cpu().numpy().astype(np.float64)
+    exp, _ = R.forward(psi.astype(np.complex128), w, b, 0.05, emulate=True)
+    assert rel_l2(d[..., 0] + 1j * d[..., 1], exp[..., 0] + 1j * exp[..., 1]) < 2e-3
+    assert np.abs(d).max() > 1e-3  # the check is not vacuous
+    s.close()
+    del torch
+
+
+@pytest.mark.parametrize("n", [(32, 20, 12), (128, 16, 8)])
+def test_apply_adds_delta_and_keeps_ghosts(n):
+    s = solver(n)
+    psi = random_field((n[2], n[1], n[0]), seed=7).astype(np.complex64)
+    s.set_state(psi)
+    w, b = weights(2)
+    with CoarseCorrector(*n, out_scale=0.05) as net:
+        net.set_weights(w, b)
+        net.apply(s)
+    got = s.get_state(np.complex64).astype(np.complex128)
+    exp, _ = R.forward(psi.astype(np.complex128), w, b, 0.05, emulate=True)
+    dexp = exp[..., 0] + 1j * exp[..., 1]
+    assert rel_l2(got - psi, dexp) < 2e-3
+    # the ghost images were updated with the interior: the library's
+    # Laplacian of the corrected field equals that of the host copy
+    lap = s.laplacian(np.complex128)
+    ref = solver(n)
+    ref.set_state(got.astype(np.complex64))
+    assert rel_l2(lap, ref.laplacian(np.complex128)) < 1e-6
+    s.close()
+    ref.close()
+
+
+@pytest.mark.parametrize("n", [(32, 12, 10), (16, 16, 6)])
+def test_gradients_match_oracle(n):
+    import torch
+    s = solver(n)
+    rng = np.random.default_rng(9)
+    u = random_field((n[2], n[1], n[0]), seed=11).astype(np.complex64)
+    tgt = (u + 0.02 * (rng.normal(size=u.shape) + 1j * rng.normal(size=u.shape))).astype(np.complex64)
+    s.set_state(u)
+    w, b = weights(3)
+    with CoarseCorrector(*n, train=True, out_scale=0.05) as net:
+        net.set_weights(w, b)
+        loss, dw, db = net.grad(s, torch.from_numpy(tgt).cuda())
+    l_ref, dw_ref, db_ref = R.loss_and_grad(u.astype(np.complex128), tgt.astype(np.complex128),
+                                            w, b, 0.05, emulate=True)
+    assert loss == pytest.approx(l_ref, rel=1e-4)
+    for l in range(4):
+        assert rel_l2(dw[l], dw_ref[l]) < 2e-2, l
+        assert rel_l2(db[l], db_ref[l]) < 2e-2, l
+    # padding entries stay exactly zero
+    assert not dw[0, :, :, 2:].any() and not dw[3, :, 2:, :].any() and not db[3, 2:].any()
+    s.close()
+
+
+def test_training_reduces_the_loss():
+    import torch
+    n = (32, 16, 8)
+    s = solver(n)
+    rng = np.random.default_rng(12)
+    u = random_field((n[2], n[1], n[0]), seed=13).astype(np.complex64)
+    # a target the network can express: a smooth function of u
+    tgt = (u + 0.01 * u * np.abs(u) ** 2).astype(np.complex64)
+    t = torch.from_numpy(tgt).cuda()
+    w, b = init_weights(4)
+    with CoarseCorrector(*n, train=True, out_scale=0.05) as net:
+        net.set_weights(w, b)
+        s.set_state(u)
+        first = net.train_step(s, t, 2e-3)
+        for _ in range(60):
+            last = net.train_step(s, t, 2e-3)
+        w2, b2 = net.get_weights()
+    assert last < 0.5 * first
+    assert not w2[0, :, :, 2:].any() and not w2[3, :, 2:, :].any() and not b2[3, 2:].any()
+    s.close()
+    del rng
+
+
+def test_restriction_is_the_2x2x2_average():
+    import torch
+    n = (32, 24, 16)
+    f = solver(n, precision=16, h=0.25)
+    psi = random_field((n[2], n[1], n[0]), seed=21)
+    f.set_state(psi)
+    out = torch.zeros((n[2] // 2, n[1] // 2, n[0] // 2), dtype=torch.complex128, device="cuda")
+    restrict(f, out)
+    exp = psi.reshape(n[2] // 2, 2, n[1] // 2, 2, n[0] // 2, 2).mean(axis=(1, 3, 5))
+    assert rel_l2(out.cpu().numpy(), exp) < 1e-15
+    out32 = torch.zeros(out.shape, dtype=torch.complex64, device="cuda")
+    restrict(f, out32)
+    assert rel_l2(out32.cpu().numpy(), exp) < 1e-7
+    f.close()
+
+
+def test_attached_correction_runs_after_every_step():
+    n = (32, 16, 16)
+    psi = random_field((n[2], n[1], n[0]), seed=31).astype(np.complex64)
+    w, b = weights(5, last=0.05)
+    with CoarseCorrector(*n, out_scale=0.02) as net:
+        net.set_weights(w, b)
+        a = solver(n)
+        a.set_state(psi)
+        for _ in range(3):
+            a.solver()
+            net.apply(a)
+        m = solver(n)
+        m.set_state(psi)
+        net.attach(m)
+        m.advance(3)
+        assert np.array_equal(a.get_state(np.complex64), m.get_state(np.complex64))
+        CoarseCorrector.detach(m)
+        m.advance(1)
+        a.solver()
+        assert np.array_equal(a.get_state(np.complex64), m.get_state(np.complex64))
+        a.close()
+        m.close()
+
+
+def test_rejects_unsupported_grids_and_contexts():
+    from gpe_b200 import GpeError
+    with pytest.raises(GpeError):
+        CoarseCorrector(24, 16, 16)  # nx not a multiple of 16
+    with pytest.raises(GpeError):
+        CoarseCorrector(144, 16, 16)  # nx > 128
+    s = solver((32, 16, 16), precision=16)
+    with CoarseCorrector(32, 16, 16) as net, pytest.raises(GpeError):
+        net.apply(s)  # complex128 context
+    s.close()
+    s = solver((32, 16, 8))
+    with CoarseCorrector(32, 16, 16) as net, pytest.raises(GpeError):
+        net.apply(s)  # grid mismatch
+    s.close()

@@ -352,6 +352,108 @@ def run_ensemble(args):
     return 0
 
 
+def run_learned(args):
+    """Time to t = 50 of the learned coarse path (128^3 complex64 + Kahan RK4,
+    dt = 0.02, network correction after every step) against the plain fine
+    path (256^3, h = 0.25, complex64 + Kahan RK4 at its largest stable step
+    dt = 0.02), both timed on the device over the same number of steps."""
+    import numpy as np
+    import torch
+
+    from gpe_b200.cnn import CoarseCorrector, init_weights
+    from gpe_b200.learned import LearnedConfig, coarse_solver, fine_solver, restricted
+
+    torch.cuda.set_device(0)
+    cfg = LearnedConfig()
+    steps = args.steps
+    wpath = os.path.join(ROOT, "gpe_b200", "data", "cnn_weights.npz")
+    if os.path.exists(wpath):
+        z = np.load(wpath)
+        w, b = z["w"], z["b"]
+        wsrc = "trained (gpe_b200/data/cnn_weights.npz)"
+    else:
+        w, b = init_weights(7)
+        wsrc = "untrained (He-normal, seed 7); the time does not depend on the values"
+
+    def timed(s, k):
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        s.advance(args.warmup)
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.advance(k)
+        e.record(st)
+        e.synchronize()
+        return a.elapsed_time(e) / k
+
+    fine = fine_solver(cfg, 100, precision=8, kahan=True, dt=cfg.dt)
+    c = coarse_solver(cfg)
+    c.set_state(restricted(cfg, fine))
+    sampler = ClockSampler(None)
+    sampler.start()
+    time.sleep(0.3)
+    ms_fine = timed(fine, steps)
+    ms_plain = timed(c, steps)
+    n = cfg.coarse_n
+    net = CoarseCorrector(n, n, n, out_scale=cfg.out_scale)
+    net.set_weights(w, b)
+    st = torch.cuda.ExternalStream(c.stream_handle())
+    for _ in range(3):
+        net.apply(c)
+    a = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    lc0 = net.launch_count()
+    a.record(st)
+    for _ in range(steps):
+        net.apply(c)
+    e.record(st)
+    e.synchronize()
+    ms_net = a.elapsed_time(e) / steps
+    launches_per_apply = (net.launch_count() - lc0) / steps
+    net.attach(c)
+    ms_learned = timed(c, steps)
+    clocks = sampler.stop()
+    CoarseCorrector.detach(c)
+    net.close()
+    c.close()
+    fine.close()
+    K = int(round(cfg.t_end / cfg.dt))
+    sites_c = n ** 3
+    useful_flop = 2 * 27 * (2 * 16 + 16 * 16 + 16 * 16 + 16 * 2) * sites_c
+    issued_flop = 2 * 27 * 16 * 16 * 4 * sites_c
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        with open(pp) as f:
+            peaks = json.load(f)
+    tf_peak = float(peaks.get("bf16_tflops", 1590.0))
+    achieved = issued_flop / (ms_net / 1e3) / 1e12
+    line = {
+        "metric": "time to t=50: learned coarse path vs plain fine path", "value": ms_fine / ms_learned,
+        "unit": "x (speed-up)", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms_learned, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 network / f32 stepper",
+        "data": "synthetic (seeded random phase |k|<=1.0, held-out seed 100)",
+        "config": {"workload": "fine 256^3 h=0.25 complex64+Kahan RK4 dt=0.02 vs coarse 128^3 "
+                               "h=0.5 complex64+Kahan RK4 dt=0.02 + 4-layer 3x3x3 conv3d "
+                               "(2-16-16-16-2, GELU, bf16) after every step", "weights": wsrc},
+        "fine_ms_per_step": ms_fine, "coarse_ms_per_step": ms_plain,
+        "network_ms_per_apply": ms_net, "learned_ms_per_step": ms_learned,
+        "time_to_t50_s": {"fine": K * ms_fine / 1e3, "learned": K * ms_learned / 1e3,
+                          "coarse_plain": K * ms_plain / 1e3},
+        "roofline": {"bound": "tensor", "kernel": "conv_fwd_kernel (4 layers + input pack)",
+                     "achieved": achieved, "peak": tf_peak, "unit": "TFLOP/s",
+                     "frac": achieved / tf_peak, "issued_flop_per_apply": issued_flop,
+                     "useful_flop_per_apply": useful_flop,
+                     "useful_tflops": useful_flop / (ms_net / 1e3) / 1e12,
+                     "note": "issued = channels padded to 16 (N=16, K=16 per tap)"},
+        "gpu_launches_per_apply": launches_per_apply,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def workload_config(ngpus, n=N_GRID):
     return {"workload": f"{n}^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
                         "(g=mu=1, V=0), complex64 psi + Kahan compensation, FP64 norm per step",
@@ -373,7 +475,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID,
                     help="cube edge (default 512; smaller sizes are for profiling captures)")
-    ap.add_argument("--workload", default="cube", choices=["cube", "ensemble"])
+    ap.add_argument("--workload", default="cube", choices=["cube", "ensemble", "learned"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -382,6 +484,10 @@ def main():
         if "--steps" not in sys.argv:
             args.steps = 500
         return run_ensemble(args)
+    if args.workload == "learned":
+        if "--steps" not in sys.argv:
+            args.steps = 200
+        return run_learned(args)
 
     import numpy as np
     import torch

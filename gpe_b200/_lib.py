@@ -157,6 +157,16 @@ def lib():
     return _lib
 
 
+def torch_ready(t) -> None:
+    """Order a library call after the work torch has queued on t's device.
+
+    The library runs on its own non-blocking streams, which do not wait for
+    torch's current stream: a tensor that torch is still writing (or still
+    reading) must be finished before its pointer is handed over."""
+    import torch
+    torch.cuda.current_stream(t.device).synchronize()
+
+
 def check(rc: int, ctx=None) -> None:
     if rc != GPE_OK:
         msg = lib().gpe_gpu_last_error(ctx)

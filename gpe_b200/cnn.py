@@ -15,7 +15,7 @@ import math
 
 import numpy as np
 
-from ._lib import GpeCnnParamsC, check_cnn, lib
+from ._lib import GpeCnnParamsC, check_cnn, lib, torch_ready
 from .solver import GpeSolver
 
 LAYERS, TAPS, CH = 4, 27, 16
@@ -100,6 +100,7 @@ class CoarseCorrector:
         """delta of the solver's psi as a CUDA float32 tensor (nz, ny, nx, 2)."""
         import torch
         out = torch.empty(self.shape + (2,), dtype=torch.float32, device="cuda")
+        torch_ready(out)
         self._chk(lib().gpe_cnn_delta(self._h, s.handle, ctypes.c_void_p(out.data_ptr())))
         return out
 
@@ -110,6 +111,7 @@ class CoarseCorrector:
     def grad(self, s: GpeSolver, target):
         """(loss, dW, db) of the pair (s's psi, target CUDA tensor)."""
         t = target.contiguous()
+        torch_ready(t)
         loss = ctypes.c_double()
         dw = np.zeros((LAYERS, TAPS, CH, CH), dtype=np.float32)
         db = np.zeros((LAYERS, CH), dtype=np.float32)
@@ -119,6 +121,7 @@ class CoarseCorrector:
 
     def train_step(self, s: GpeSolver, target, lr: float) -> float:
         t = target.contiguous()
+        torch_ready(t)
         loss = ctypes.c_double()
         self._chk(lib().gpe_cnn_train_step(self._h, s.handle, ctypes.c_void_p(t.data_ptr()),
                                            self._eb(t), float(lr), ctypes.byref(loss)))
@@ -135,4 +138,5 @@ def restrict(fine: GpeSolver, out) -> None:
     """2:1 restriction (2x2x2 average) of fine's psi into `out`, a CUDA
     complex64/complex128 tensor of shape (nz/2, ny/2, nx/2)."""
     eb = 16 if str(out.dtype) == "torch.complex128" else 8
+    torch_ready(out)
     check_cnn(lib().gpe_cnn_restrict(fine.handle, ctypes.c_void_p(out.data_ptr()), eb), None)

@@ -14,7 +14,6 @@
 //                 gelu'(P_{l-1}) -> the other G buffer;
 //   Adam; repack bf16 weight tiles.
 #include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -33,7 +32,6 @@ namespace {
 
 thread_local std::string g_cnn_error;
 constexpr unsigned long long CNN_WAIT_LIMIT_NS = 2000000000ull;
-PFN_cuTensorMapEncodeTiled_v12000 g_enc = nullptr;
 
 struct Act {
   __nv_bfloat16* p = nullptr;
@@ -88,36 +86,6 @@ int cfail(gpe_cnn* n, int code, const std::string& msg) {
       return cfail((n), GPE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-int ensure_enc(gpe_cnn* n) {
-  if (g_enc) return GPE_OK;
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-          cudaSuccess ||
-      q != cudaDriverEntryPointSuccess || !fn)
-    return cfail(n, GPE_ERR_CUDA, "cuTensorMapEncodeTiled entry point not found");
-  g_enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  return GPE_OK;
-}
-
-// 5-D map of an activation buffer: dims (8, Xp, H, Yp, Zp), box (8, Xp, H, rows, 1).
-int act_map(gpe_cnn* n, const Act& a, int rows, CUtensorMap* m) {
-  int rc = ensure_enc(n);
-  if (rc) return rc;
-  cuuint64_t dims[5] = {8, (cuuint64_t)n->Xp, (cuuint64_t)a.H, (cuuint64_t)n->Yp,
-                        (cuuint64_t)n->Zp};
-  cuuint64_t strides[4] = {16, (cuuint64_t)n->Xp * 16, (cuuint64_t)a.H * n->Xp * 16,
-                           (cuuint64_t)n->Yp * a.H * n->Xp * 16};
-  cuuint32_t box[5] = {8, (cuuint32_t)n->Xp, (cuuint32_t)a.H, (cuuint32_t)rows, 1};
-  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-  CUresult r = g_enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, a.p, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS)
-    return cfail(n, GPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-  return GPE_OK;
-}
-
 size_t act_bytes(const gpe_cnn* n, int H) {
   return (size_t)n->Zp * n->Yp * H * n->Xp * 16;
 }
@@ -143,9 +111,8 @@ void conv_items(const gpe_cnn* n, int rows, int* nslab, int* nzc, int* zchunk) {
 template <int EPI>
 int launch_conv(gpe_cnn* n, cudaStream_t st, const Act& in, int layer, bool dgrad,
                 ConvParams& p) {
-  int rc = act_map(n, in, TYF + 2, &p.tmap);
-  if (rc) return rc;
-  p.w = (dgrad ? n->d_wt : n->d_wf) + (size_t)layer * NTAP * TAP_BYTES / 2;
+  p.in = in.p;
+  p.w = (dgrad ? n->d_wt : n->d_wf) + (size_t)layer * W_TILES * WT_BYTES / 2;
   p.bias = dgrad ? nullptr : n->d_b + layer * 16;
   p.nx = n->nx; p.ny = n->ny; p.nz = n->nz;
   p.Xp = n->Xp; p.Yp = n->Yp; p.Zp = n->Zp; p.Hin = in.H;
@@ -156,7 +123,7 @@ int launch_conv(gpe_cnn* n, cudaStream_t st, const Act& in, int layer, bool dgra
   p.out_scale = n->prm.out_scale;
   if (!p.status) p.status = n->d_status;
   p.wait_limit_ns = CNN_WAIT_LIMIT_NS;
-  const size_t smem = 1024 + (size_t)FSLOTS * p.slot_bytes + 4096 + NTAP * TAP_BYTES + 16 * 8 + 16;
+  const size_t smem = 1024 + (size_t)FSLOTS * p.slot_bytes + 4096 + W_TILES * WT_BYTES + F_TAIL_BYTES;
   auto fn = conv_fwd_kernel<EPI>;
   CNN_CU(n, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = std::min(p.nitems, n->num_sms);
@@ -169,10 +136,8 @@ int launch_conv(gpe_cnn* n, cudaStream_t st, const Act& in, int layer, bool dgra
 int launch_wgrad(gpe_cnn* n, cudaStream_t st, const Act& x, const Act& dy) {
   WgradParams p;
   memset(&p, 0, sizeof(p));
-  int rc = act_map(n, x, XROWS, &p.tmap_x);
-  if (rc) return rc;
-  rc = act_map(n, dy, TYW, &p.tmap_dy);
-  if (rc) return rc;
+  p.x = x.p;
+  p.dy = dy.p;
   p.nx = n->nx; p.ny = n->ny; p.nz = n->nz;
   p.Xp = n->Xp; p.Yp = n->Yp; p.Zp = n->Zp;
   p.nslab = (n->ny + TYW - 1) / TYW;
@@ -329,7 +294,7 @@ int read_loss(gpe_cnn* n, cudaStream_t st, double* loss) {
 }
 
 int repack_weights(gpe_cnn* n, cudaStream_t st) {
-  pack_weights_kernel<<<(NLAYER * NTAP * 256 + 255) / 256, 256, 0, st>>>(n->d_w, n->d_wf, n->d_wt);
+  pack_weights_kernel<<<(NLAYER * W_TILES * 2 * NSTACK * 8 + 255) / 256, 256, 0, st>>>(n->d_w, n->d_wf, n->d_wt);
   CNN_CU(n, cudaGetLastError());
   n->launches++;
   return GPE_OK;
@@ -407,8 +372,8 @@ int gpe_cnn_create(const gpe_cnn_params* p, gpe_cnn** out) {
   const size_t np = GPE_CNN_WEIGHTS + GPE_CNN_BIASES;
   int rc;
   if (cudaMalloc(&n->d_w, sizeof(float) * np) != cudaSuccess ||
-      cudaMalloc(&n->d_wf, (size_t)NLAYER * NTAP * TAP_BYTES) != cudaSuccess ||
-      cudaMalloc(&n->d_wt, (size_t)NLAYER * NTAP * TAP_BYTES) != cudaSuccess ||
+      cudaMalloc(&n->d_wf, (size_t)NLAYER * W_TILES * WT_BYTES) != cudaSuccess ||
+      cudaMalloc(&n->d_wt, (size_t)NLAYER * W_TILES * WT_BYTES) != cudaSuccess ||
       cudaMalloc(&n->d_status, sizeof(int)) != cudaSuccess) {
     n->err = "cudaMalloc failed";
     return bail(GPE_ERR_OOM);

@@ -12,12 +12,21 @@
 // operand of tap (dz, dy, dx) for 128 consecutive sites of a row is the row's
 // address + 16 * dx, with LBO = the half stride.  No im2col copy exists.
 //
-// Forward / dgrad kernel: one CTA per (y-slab of 8 rows, z-chunk) item;
-// warp 0 streams input planes (8 + 2 rows, both halves, the full padded x
-// extent) into a 4-slot ring with TMA; warp 1 issues, per output row,
-// 27 tcgen05.mma (M = 128 sites, N = 16, K = 16) into a TMEM accumulator
-// (two buffers of 8 rows x 16 columns); warps 2-9 read the accumulators back
-// (tcgen05.ld 32x32b), apply the epilogue and store.
+// Forward / dgrad kernel: one CTA per (y-slab of 6 rows, z-chunk) item;
+// warp 0 streams input planes (6 + 2 rows, both halves, the full padded x
+// extent) into a 3-slot ring -- in this layout those rows are one contiguous
+// range, fetched by a single 1-D bulk copy (a tensor-map tile with its
+// 16-byte innermost extent moved the same bytes several times slower); warp 1 issues, per input plane and
+// per (input row, dx), ONE tcgen05.mma (M = 128 sites, N = 144, K = 16)
+// whose D block covers every output site that input row feeds: 3 output
+// rows x 3 output planes x 16 channels.  A small MMA costs about 50 issue
+// cycles whatever its N, so 24 MMAs of N = 144 per plane (near the tensor
+// pipe's rate) replace 162 of N = 16.  The accumulators of three output
+// planes rotate in TMEM; when an input plane's MMAs complete, one output
+// plane is finished: warps 2-9 copy its rows to registers (tcgen05.ld
+// 32x32b), zero its slot, release it to the MMA warp, and only then run the
+// epilogue and the stores, which overlap the next plane's MMAs.  Every MMA
+// accumulates; slots are zero when a plane first receives data.
 //
 // Weight-gradient kernel: D[(dy, ci), co] += X[(row y + dy), ci, x + dx] *
 // dY[row y, co, x] summed over x in 16-site K steps; A (X) and B (dY) are
@@ -40,11 +49,31 @@ constexpr int NLAYER = 4;
 constexpr int TAP_BYTES = 2 * CH * 8 * 2;  // [2 halves][16 rows][8] bf16 = 512
 
 // forward / dgrad
-constexpr int TYF = 8;
-constexpr int FSLOTS = 4;
-constexpr int F_EPI_WARPS = 8;
+constexpr int TYF = 6;          // output rows per item
+constexpr int FSLOTS = 3;       // input planes in the shared-memory ring
+constexpr int F_GROUP_WARPS = 8;                 // one epilogue group: 2 warps per lane quarter
+constexpr int F_EPI_WARPS = 2 * F_GROUP_WARPS;   // two groups take alternate planes
 constexpr int F_THREADS = 32 * (2 + F_EPI_WARPS);
-constexpr uint32_t F_TMEM_COLS = 256;
+// Accumulators: three output planes in a rotating ring (plane z in slot
+// z mod 3), each with output rows y0-2 .. y0+TYF+1 (ACC_ROWS), column
+// (row * 3 + slot) * 16 + co.  Input row y' (box row i) of input plane j
+// feeds output rows y'-1, y', y'+1 (accumulator rows i .. i+2) of output
+// planes j-1, j, j+1 (all three slots): one contiguous block of 144 columns,
+// so a single MMA with N = 144 covers all nine (dz, dy) taps of one dx.
+constexpr int OSLOTS = 3;
+constexpr int ACC_ROWS = TYF + 4;
+constexpr int NSTACK = 3 * OSLOTS * CH;          // 144
+constexpr uint32_t F_TMEM_COLS = 512;
+static_assert(ACC_ROWS * OSLOTS * CH <= (int)F_TMEM_COLS, "accumulator ring fits TMEM");
+// B tile of one (rotation j mod 3, dx): rows n = (jrow * 3 + s) * 16 + co
+// hold tap (dz index 2 - ((s - rot + 1) mod 3), dy index 2 - jrow, dx);
+// K = 16 input channels in two halves: [2][144][8] bf16.
+constexpr int WT_BYTES = 2 * NSTACK * 8 * 2;     // 4608
+constexpr int W_TILES = 9;                       // 3 rotations x 3 dx
+constexpr int EPI_ROWS = (TYF + 1) / 2;          // rows per epilogue warp
+// after the weights: 2*FSLOTS + 5 mbarriers, TMEM address, abort flag, 16 biases
+constexpr int F_TAIL_BYTES = 256;
+static_assert((2 * FSLOTS + 5) * 8 + 16 + 64 <= F_TAIL_BYTES, "tail fits");
 
 // weight gradient
 constexpr int TYW = 2;
@@ -59,7 +88,7 @@ constexpr int NACC = 9;  // (dz, dx) accumulators
 enum Epi { EPI_GELU = 0, EPI_GELU_PRE = 1, EPI_DELTA = 2, EPI_RESID = 3, EPI_DGELU = 4 };
 
 struct ConvParams {
-  CUtensorMap tmap;                 // input activations, box (8, Xp, Hin, TYF+2, 1)
+  const __nv_bfloat16* in;          // input activations [Zp][Yp][Hin][Xp][8]
   const __nv_bfloat16* w;           // [27][2][16][8]
   const float* bias;                // [16] or null
   int nx, ny, nz, Xp, Yp, Zp, Hin;
@@ -77,8 +106,8 @@ struct ConvParams {
 };
 
 struct WgradParams {
-  CUtensorMap tmap_x;               // box (8, Xp, 2, XROWS, 1)
-  CUtensorMap tmap_dy;              // box (8, Xp, 2, TYW, 1)
+  const __nv_bfloat16* x;           // layer input [Zp][Yp][2][Xp][8]
+  const __nv_bfloat16* dy;          // gradient of the layer output, same layout
   int nx, ny, nz, Xp, Yp, Zp;
   int nslab, nzc, zchunk, nitems;
   uint32_t xslot_bytes, xbox_bytes, dslot_bytes, dbox_bytes;
@@ -87,13 +116,28 @@ struct WgradParams {
   unsigned long long wait_limit_ns;
 };
 
-// GELU from its definition x * Phi(x), Phi the standard normal CDF.
+// GELU in its tanh form (Hendrycks & Gimpel, 2016):
+//   gelu(x) = 0.5 x (1 + t),  t = tanh(u),  u = sqrt(2/pi) (x + 0.044715 x^3),
+//   gelu'(x) = 0.5 (1 + t) + 0.5 x (1 - t^2) u',  u' = sqrt(2/pi) (1 + 3 * 0.044715 x^2).
+// tanh through the hardware tanh.approx.f32 instruction (one MUFU operation,
+// relative error about 2^-11, below the bfloat16 rounding of the result).
+constexpr float GELU_C = 0.7978845608028654f;  // sqrt(2/pi)
+constexpr float GELU_A = 0.044715f;
+
+__device__ __forceinline__ float tanh_approx(float u) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return t;
+}
 __device__ __forceinline__ float gelu(float x) {
-  return 0.5f * x * (1.0f + erff(x * 0.7071067811865476f));
+  const float t = tanh_approx(GELU_C * fmaf(GELU_A * x, x * x, x));
+  const float hx = 0.5f * x;
+  return fmaf(hx, t, hx);
 }
 __device__ __forceinline__ float gelu_grad(float x) {
-  return 0.5f * (1.0f + erff(x * 0.7071067811865476f)) +
-         x * 0.3989422804014327f * expf(-0.5f * x * x);
+  const float t = tanh_approx(GELU_C * fmaf(GELU_A * x, x * x, x));
+  const float du = GELU_C * fmaf(3.0f * GELU_A * x, x, 1.0f);
+  return fmaf(0.5f * x * fmaf(-t, t, 1.0f), du, 0.5f * (1.0f + t));
 }
 
 __device__ __forceinline__ size_t act_index(int Xp, int Yp, int x, int y, int z, int h) {
@@ -105,23 +149,33 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// The interior site (x, y, z) and its periodic ghost images (halo 1).
+// The interior site (x, y, z) and its periodic ghost images (halo 1), in
+// padded coordinates.  Up to three images per axis (n = 1 has both ghosts).
 template <typename F>
 __device__ __forceinline__ void for_images(int x, int y, int z, int nx, int ny, int nz, F f) {
-  int xs[3], ys[3], zs[3];
-  int nxs = 0, nys = 0, nzs = 0;
-  xs[nxs++] = x + 1;
-  if (x == 0) xs[nxs++] = nx + 1;
-  if (x == nx - 1) xs[nxs++] = 0;
-  ys[nys++] = y + 1;
-  if (y == 0) ys[nys++] = ny + 1;
-  if (y == ny - 1) ys[nys++] = 0;
-  zs[nzs++] = z + 1;
-  if (z == 0) zs[nzs++] = nz + 1;
-  if (z == nz - 1) zs[nzs++] = 0;
-  for (int c = 0; c < nzs; c++)
-    for (int b = 0; b < nys; b++)
-      for (int a = 0; a < nxs; a++) f(xs[a], ys[b], zs[c]);
+  const int x1 = x == 0 ? nx + 1 : -1, x2 = x == nx - 1 ? 0 : -1;
+  const int y1 = y == 0 ? ny + 1 : -1, y2 = y == ny - 1 ? 0 : -1;
+  const int z1 = z == 0 ? nz + 1 : -1, z2 = z == nz - 1 ? 0 : -1;
+  if ((x1 & x2 & y1 & y2 & z1 & z2) == -1) {  // interior: no ghost image
+    f(x + 1, y + 1, z + 1);
+    return;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int zp = c == 0 ? z + 1 : (c == 1 ? z1 : z2);
+    if (zp < 0) continue;
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      const int yp = b == 0 ? y + 1 : (b == 1 ? y1 : y2);
+      if (yp < 0) continue;
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        const int xp = a == 0 ? x + 1 : (a == 1 ? x1 : x2);
+        if (xp < 0) continue;
+        f(xp, yp, zp);
+      }
+    }
+  }
 }
 
 // 16 channels of one site (two 16-byte records) into a [.][.][2][Xp][8]
@@ -167,48 +221,75 @@ __device__ __forceinline__ void set_abort(int* status, volatile int* flag, int c
 // --------------------------------------------------------------------------
 // Forward / dgrad convolution.
 
+// Global data an epilogue reads besides the accumulators: the stored
+// pre-activation (dgrad) or the solver's psi (residual).  Loaded for every
+// row of a plane before any of them is computed, so the latencies overlap.
+struct EpiAux {
+  uint4 lo, hi;
+  float2 psi;
+};
+
+__device__ __forceinline__ size_t psi_index(const ConvParams& p, int x, int y, int z) {
+  return ((size_t)(z + 2) * p.psi_Ny + (y + 2)) * p.psi_Nx + (x + 2);
+}
+
 template <int EPI>
-__device__ __forceinline__ void conv_epilogue(const ConvParams& p, const float (&acc)[16], int x,
-                                              int y, int z) {
+__device__ __forceinline__ void epi_load(const ConvParams& p, int x, int y, int z, EpiAux& a) {
+  if (EPI == EPI_DGELU) {
+    a.lo = *reinterpret_cast<const uint4*>(p.pre_in + act_index(p.Xp, p.Yp, x + 1, y + 1, z + 1, 0));
+    a.hi = *reinterpret_cast<const uint4*>(p.pre_in + act_index(p.Xp, p.Yp, x + 1, y + 1, z + 1, 1));
+  } else if (EPI == EPI_RESID) {
+    a.psi = reinterpret_cast<const float2*>(p.psi)[psi_index(p, x, y, z)];
+  }
+}
+
+template <int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvParams& p, const float (&acc)[16],
+                                              const float* bias, const EpiAux& aux, int x, int y,
+                                              int z) {
   if (EPI == EPI_GELU || EPI == EPI_GELU_PRE) {
     float pre[16], a[16];
 #pragma unroll
     for (int c = 0; c < 16; c++) {
-      pre[c] = acc[c] + p.bias[c];
+      pre[c] = acc[c] + bias[c];
       a[c] = gelu(pre[c]);
     }
     if (EPI == EPI_GELU_PRE) store_act16(p.pre_out, p.Xp, p.Yp, p.nx, p.ny, p.nz, x, y, z, pre, false);
     store_act16(p.act_out, p.Xp, p.Yp, p.nx, p.ny, p.nz, x, y, z, a, true);
   } else if (EPI == EPI_DGELU) {
-    float pre[16], g[16];
-    load_act16(p.pre_in, p.Xp, p.Yp, x, y, z, pre);
+    float g[16];
+    const uint32_t w[8] = {aux.lo.x, aux.lo.y, aux.lo.z, aux.lo.w, aux.hi.x, aux.hi.y, aux.hi.z, aux.hi.w};
 #pragma unroll
-    for (int c = 0; c < 16; c++) g[c] = acc[c] * gelu_grad(pre[c]);
+    for (int i = 0; i < 8; i++) {
+      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[i]));
+      g[2 * i] = acc[2 * i] * gelu_grad(f.x);
+      g[2 * i + 1] = acc[2 * i + 1] * gelu_grad(f.y);
+    }
     store_act16(p.act_out, p.Xp, p.Yp, p.nx, p.ny, p.nz, x, y, z, g, true);
   } else if (EPI == EPI_DELTA) {
     const size_t s = ((size_t)z * p.ny + y) * p.nx + x;
     reinterpret_cast<float2*>(p.delta)[s] =
-        make_float2((acc[0] + p.bias[0]) * p.out_scale, (acc[1] + p.bias[1]) * p.out_scale);
+        make_float2((acc[0] + bias[0]) * p.out_scale, (acc[1] + bias[1]) * p.out_scale);
   } else {  // EPI_RESID: psi += delta on the solver's field, ghosts (2, periodic) too
-    const float dr = (acc[0] + p.bias[0]) * p.out_scale;
-    const float di = (acc[1] + p.bias[1]) * p.out_scale;
+    float2 v = aux.psi;
+    v.x += (acc[0] + bias[0]) * p.out_scale;
+    v.y += (acc[1] + bias[1]) * p.out_scale;
     float2* f = reinterpret_cast<float2*>(p.psi);
-    const size_t s = ((size_t)(z + 2) * p.psi_Ny + (y + 2)) * p.psi_Nx + (x + 2);
-    float2 v = f[s];
-    v.x += dr;
-    v.y += di;
     int gx[3] = {x, NO_GHOST, NO_GHOST}, gy[3] = {y, NO_GHOST, NO_GHOST},
         gz[3] = {z, NO_GHOST, NO_GHOST};
     ghost_targets(x, p.nx, 1, gx[1], gx[2]);
     ghost_targets(y, p.ny, 1, gy[1], gy[2]);
     ghost_targets(z, p.nz, 1, gz[1], gz[2]);
+#pragma unroll
     for (int c = 0; c < 3; c++) {
       if (gz[c] == NO_GHOST) continue;
+#pragma unroll
       for (int b = 0; b < 3; b++) {
         if (gy[b] == NO_GHOST) continue;
+#pragma unroll
         for (int a = 0; a < 3; a++) {
           if (gx[a] == NO_GHOST) continue;
-          f[((size_t)(gz[c] + 2) * p.psi_Ny + (gy[b] + 2)) * p.psi_Nx + (gx[a] + 2)] = v;
+          f[psi_index(p, gx[a], gy[b], gz[c])] = v;
         }
       }
     }
@@ -221,35 +302,35 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
   unsigned char* ring = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* wsm = ring + FSLOTS * p.slot_bytes + 4096;  // 4 KB of zeros after the ring
-  uint64_t* full = reinterpret_cast<uint64_t*>(wsm + NTAP * TAP_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(wsm + W_TILES * WT_BYTES);
   uint64_t* empty = full + FSLOTS;
-  uint64_t* accf = empty + FSLOTS;
-  uint64_t* acce = accf + 2;
+  uint64_t* accf = empty + FSLOTS;  // [2] MMAs of one input plane done (per epilogue group)
+  uint64_t* acce = accf + 2;        // [2] the finished output plane's slot is drained
   uint64_t* drain = acce + 2;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+  float* bias_s = reinterpret_cast<float*>(tmem_holder + 4);  // [16], 16-byte aligned
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   {  // weights and the zero pad (generic proxy), then make them visible to the tensor core
     const uint4* src = reinterpret_cast<const uint4*>(p.w);
     uint4* dst = reinterpret_cast<uint4*>(wsm);
-    for (int i = threadIdx.x; i < NTAP * TAP_BYTES / 16; i += blockDim.x) dst[i] = src[i];
-    uint4* pad = reinterpret_cast<uint4*>(ring + FSLOTS * p.slot_bytes);
-    for (int i = threadIdx.x; i < 4096 / 16; i += blockDim.x) pad[i] = make_uint4(0, 0, 0, 0);
-    for (int s = 0; s < FSLOTS; s++) {
-      uint4* gap = reinterpret_cast<uint4*>(ring + s * p.slot_bytes + p.box_bytes);
-      for (int i = threadIdx.x; i < (int)(p.slot_bytes - p.box_bytes) / 16; i += blockDim.x)
-        gap[i] = make_uint4(0, 0, 0, 0);
-    }
+    for (int i = threadIdx.x; i < W_TILES * WT_BYTES / 16; i += blockDim.x) dst[i] = src[i];
+    // the whole ring and the pad start at zero: rows a copy leaves
+    // untouched (past the grid's last row) and over-reads stay finite
+    uint4* z = reinterpret_cast<uint4*>(ring);
+    for (int i = threadIdx.x; i < (int)(FSLOTS * p.slot_bytes + 4096) / 16; i += blockDim.x)
+      z[i] = make_uint4(0, 0, 0, 0);
   }
+  if (threadIdx.x < 16) bias_s[threadIdx.x] = p.bias ? p.bias[threadIdx.x] : 0.0f;
   if (threadIdx.x == 0) {
     for (int s = 0; s < FSLOTS; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; b++) {
-      mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 32 * F_EPI_WARPS);
+    for (int g = 0; g < 2; g++) {
+      mbar_init(&accf[g], 1);
+      mbar_init(&acce[g], 32 * F_GROUP_WARPS);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -263,10 +344,20 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
   const uint32_t tmem = *tmem_holder;
   const uint64_t lim = p.wait_limit_ns;
   const uint32_t row_bytes = (uint32_t)p.Xp * 16;
+  if (warp >= 2 && warp < 2 + F_GROUP_WARPS) {  // the accumulator ring starts at zero
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    for (int a = half; a < ACC_ROWS * OSLOTS; a += 2)
+      tc::st_32x32b_x16_zero(tmem + ((uint32_t)(32 * q) << 16) + a * 16);
+    tc::wait_st();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
 
   if (warp == 0) {
     if (lane == 0) {
-      prefetch_tmap(&p.tmap);
+      const size_t row_elems = (size_t)p.Hin * p.Xp * 8;
+      const size_t plane_elems = (size_t)p.Yp * row_elems;
       uint32_t g = 0;
       for (int it = blockIdx.x; it < p.nitems && !*abort_flag; it += gridDim.x) {
         const int slab = it % p.nslab, zc = it / p.nslab;
@@ -278,12 +369,14 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
             set_abort(p.status, abort_flag, 1);
             break;
           }
-          mbar_arrive_expect_tx(&full[slot], p.box_bytes);
-          tc::tma_load_5d(smem_u32(ring + slot * p.slot_bytes), &p.tmap, 0, 0, 0, y0, z0 + pl,
-                          smem_u32(&full[slot]));
+          // rows y0 .. y0+TYF+1 (padded) of plane z0+pl: one contiguous range
+          const uint32_t bytes = (uint32_t)min(TYF + 2, p.Yp - y0) * (uint32_t)(row_elems * 2);
+          mbar_arrive_expect_tx(&full[slot], bytes);
+          tc::bulk_load(smem_u32(ring + slot * p.slot_bytes),
+                        p.in + (size_t)(z0 + pl) * plane_elems + (size_t)y0 * row_elems, bytes,
+                        smem_u32(&full[slot]));
         }
       }
-      // every load issued must have landed before the CTA exits
       const uint32_t first = g > FSLOTS ? g - FSLOTS : 0;
       for (uint32_t q = first; q < g; q++)
         if (!mbar_wait_bounded(&full[q % FSLOTS], (q / FSLOTS) & 1, lim)) {
@@ -293,89 +386,106 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = tc::idesc_bf16_f32(128, 16, false, false);
+      const uint32_t idesc = tc::idesc_bf16_f32(128, NSTACK, false, false);
       const uint32_t lbo_a = p.Hin == 2 ? row_bytes : 0;
       const uint32_t ring_s = smem_u32(ring), w_s = smem_u32(wsm);
-      const uint64_t bdesc0 = tc::smem_desc(w_s, 256, 128);
-      uint32_t g0 = 0, waited = 0, accn = 0;
+      const uint64_t bdesc0 = tc::smem_desc(w_s, NSTACK * 16, 128);
+      const uint64_t adesc0 = tc::smem_desc(ring_s, lbo_a, 128);
+      const uint32_t row_step = (uint32_t)p.Hin * row_bytes;
+      uint32_t g = 0, e = 0;  // input planes, steps (one per input plane)
       for (int it = blockIdx.x; it < p.nitems && !*abort_flag; it += gridDim.x) {
         const int slab = it % p.nslab, zc = it / p.nslab;
         const int y0 = slab * TYF, z0 = zc * p.zchunk;
         const int nout = min(z0 + p.zchunk, p.nz) - z0;
-        const int nrows = min(TYF, p.ny - y0);
-        for (int o = 0; o < nout && !*abort_flag; o++) {
-          bool ok = true;
-          while (waited < g0 + o + 3) {
-            if (!mbar_wait_bounded(&full[waited % FSLOTS], (waited / FSLOTS) & 1, lim)) {
-              ok = false;
-              break;
-            }
-            waited++;
-          }
-          const uint32_t buf = accn & 1;
-          if (ok && accn >= 2) ok = mbar_wait_bounded(&acce[buf], ((accn >> 1) - 1) & 1, lim);
+        const int nin = min(TYF, p.ny - y0) + 2;  // input rows y0-1 .. y0+nrows
+        for (int t = 0; t < nout + 2 && !*abort_flag; t++, g++, e++) {
+          const int j = z0 - 1 + t;  // input plane (may be -1: its ghost plane)
+          bool ok = mbar_wait_bounded(&full[g % FSLOTS], (g / FSLOTS) & 1, lim);
+          if (ok && e > 0) ok = mbar_wait_bounded(&acce[(e - 1) & 1], ((e - 1) >> 1) & 1, lim);
           if (!ok) {
             set_abort(p.status, abort_flag, 1);
             break;
           }
           tc::fence_after_sync();
-          uint32_t pbase[3];
+          const uint64_t ab = adesc0 + ((g % FSLOTS) * p.slot_bytes >> 4);
+          const uint64_t bb = bdesc0 + (uint64_t)(((j + 3) % 3) * 3 * WT_BYTES / 16);
 #pragma unroll
-          for (int dz = 0; dz < 3; dz++) pbase[dz] = ring_s + ((g0 + o + dz) % FSLOTS) * p.slot_bytes;
-          for (int r = 0; r < nrows; r++) {
-            const uint32_t d = tmem + (buf * TYF + r) * 16;
+          for (int i = 0; i < TYF + 2; i++) {
+            if (i < nin) {
 #pragma unroll
-            for (int dz = 0; dz < 3; dz++)
-#pragma unroll
-              for (int dy = 0; dy < 3; dy++) {
-                const uint32_t rowa = pbase[dz] + (uint32_t)((r + dy) * p.Hin) * row_bytes;
-#pragma unroll
-                for (int dx = 0; dx < 3; dx++) {
-                  const int tap = dz * 9 + dy * 3 + dx;
-                  const uint64_t adesc = tc::smem_desc(rowa + dx * 16, lbo_a, 128);
-                  tc::mma_bf16(d, adesc, bdesc0 + (uint64_t)(tap * TAP_BYTES / 16), idesc,
-                               tap > 0 ? 1u : 0u);
-                }
-              }
+              for (int dx = 0; dx < 3; dx++)
+                tc::mma_bf16(tmem + i * (OSLOTS * CH), ab + ((i * row_step + dx * 16) >> 4),
+                             bb + (uint64_t)(dx * WT_BYTES / 16), idesc, 1u);
+            }
           }
-          tc::commit(smem_u32(&accf[buf]));
-          tc::commit(smem_u32(&empty[(g0 + o) % FSLOTS]));
-          accn++;
+          tc::commit(smem_u32(&accf[e & 1]));
+          tc::commit(smem_u32(&empty[g % FSLOTS]));
         }
-        if (*abort_flag) break;
-        tc::commit(smem_u32(&empty[(g0 + nout) % FSLOTS]));
-        tc::commit(smem_u32(&empty[(g0 + nout + 1) % FSLOTS]));
-        g0 += nout + 2;
       }
       tc::commit(smem_u32(drain));
       if (!mbar_wait_bounded(drain, 0, lim)) set_abort(p.status, abort_flag, 1);
     }
   } else {
+    // two groups of 8 warps take alternate planes (group = step parity), so
+    // a finished plane is drained while the other group still computes
     const int ew = warp - 2;
-    const int q = warp & 3, half = ew >> 2;
+    const int grp = ew / F_GROUP_WARPS;
+    const int q = warp & 3, half = (ew % F_GROUP_WARPS) >> 2;
     const int x = 32 * q + lane;
-    uint32_t accn = 0;
+    const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
+    uint32_t e = 0;
     for (int it = blockIdx.x; it < p.nitems && !*abort_flag; it += gridDim.x) {
       const int slab = it % p.nslab, zc = it / p.nslab;
       const int y0 = slab * TYF, z0 = zc * p.zchunk;
       const int nout = min(z0 + p.zchunk, p.nz) - z0;
       const int nrows = min(TYF, p.ny - y0);
-      for (int o = 0; o < nout; o++) {
-        const uint32_t buf = accn & 1;
-        if (!mbar_wait_bounded(&accf[buf], (accn >> 1) & 1, lim)) {
+      bool stop = false;
+      for (int t = 0; t < nout + 2; t++, e++) {
+        if ((int)(e & 1) != grp) continue;
+        if (!mbar_wait_bounded(&accf[grp], (e >> 1) & 1, lim)) {
           set_abort(p.status, abort_flag, 1);
+          stop = true;
           break;
         }
         tc::fence_after_sync();
-        for (int r = half; r < nrows; r += 2) {
-          float v[16];
-          tc::ld_32x32b_x16(tmem + ((uint32_t)(32 * q) << 16) + (buf * TYF + r) * 16, v);
-          if (x < p.nx) conv_epilogue<EPI>(p, v, x, y0 + r, z0 + o);
+        const int zo = z0 - 2 + t;  // output plane finished by input plane zo + 1
+        const bool real = zo >= z0;
+        const bool mine = real && x < p.nx;
+        const uint32_t so = (uint32_t)((zo + 3) % 3);
+        EpiAux aux[EPI_ROWS];
+        if (mine) {
+#pragma unroll
+          for (int k = 0; k < EPI_ROWS; k++)
+            if (half + 2 * k < nrows) epi_load<EPI>(p, x, y0 + half + 2 * k, zo, aux[k]);
         }
+        float v[EPI_ROWS][16];
+        if (real) {
+#pragma unroll
+          for (int k = 0; k < EPI_ROWS; k++) {
+            const int r = half + 2 * k;
+            if (r < nrows) tc::ld_32x32b_x16(tq + ((r + 2) * OSLOTS + so) * 16, v[k]);
+          }
+        }
+        const bool last = t == nout + 1;
+        for (int a = half; a < ACC_ROWS; a += 2) {
+          tc::st_32x32b_x16_zero(tq + (a * OSLOTS + so) * 16);
+          if (last) {  // junk of the planes past the chunk
+            tc::st_32x32b_x16_zero(tq + (a * OSLOTS + (so + 1) % 3) * 16);
+            tc::st_32x32b_x16_zero(tq + (a * OSLOTS + (so + 2) % 3) * 16);
+          }
+        }
+        tc::wait_st();
         tc::fence_before_sync();
-        mbar_arrive(&acce[buf]);
-        accn++;
+        mbar_arrive(&acce[grp]);
+        if (mine) {
+#pragma unroll
+          for (int k = 0; k < EPI_ROWS; k++) {
+            const int r = half + 2 * k;
+            if (r < nrows) conv_epilogue<EPI>(p, v[k], bias_s, aux[k], x, y0 + r, zo);
+          }
+        }
       }
+      if (stop) break;
     }
   }
   tc::fence_before_sync();
@@ -404,6 +514,12 @@ __global__ void __launch_bounds__(W_THREADS, 1) conv_wgrad_kernel(const __grid_c
   volatile int* any_flag = abort_flag + 1;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {  // rings start at zero: rows a copy leaves untouched stay finite
+    uint4* z = reinterpret_cast<uint4*>(xring);
+    const int n16 = (int)(WSLOTS * p.xslot_bytes + DSLOTS * p.dslot_bytes) / 16;
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) z[i] = make_uint4(0, 0, 0, 0);
+  }
+  fence_proxy_async();
   if (threadIdx.x == 0) {
     for (int s = 0; s < WSLOTS; s++) {
       mbar_init(&xfull[s], 1);
@@ -428,24 +544,28 @@ __global__ void __launch_bounds__(W_THREADS, 1) conv_wgrad_kernel(const __grid_c
 
   if (warp == 0) {
     if (lane == 0) {
-      prefetch_tmap(&p.tmap_x);
-      prefetch_tmap(&p.tmap_dy);
+      const size_t row_elems = (size_t)2 * p.Xp * 8;
+      const size_t plane_elems = (size_t)p.Yp * row_elems;
       uint32_t gx = 0, gd = 0;
       auto load_x = [&](int y0, int zpad) -> bool {
         const uint32_t slot = gx % WSLOTS, cyc = gx / WSLOTS;
         if (cyc > 0 && !mbar_wait_bounded(&xempty[slot], (cyc - 1) & 1, lim)) return false;
-        mbar_arrive_expect_tx(&xfull[slot], p.xbox_bytes);
-        tc::tma_load_5d(smem_u32(xring + slot * p.xslot_bytes), &p.tmap_x, 0, 0, 0, y0, zpad,
-                        smem_u32(&xfull[slot]));
+        const uint32_t bytes = (uint32_t)min(XROWS, p.Yp - y0) * (uint32_t)(row_elems * 2);
+        mbar_arrive_expect_tx(&xfull[slot], bytes);
+        tc::bulk_load(smem_u32(xring + slot * p.xslot_bytes),
+                      p.x + (size_t)zpad * plane_elems + (size_t)y0 * row_elems, bytes,
+                      smem_u32(&xfull[slot]));
         gx++;
         return true;
       };
       auto load_d = [&](int y0, int zpad) -> bool {
         const uint32_t slot = gd % DSLOTS, cyc = gd / DSLOTS;
         if (cyc > 0 && !mbar_wait_bounded(&dempty[slot], (cyc - 1) & 1, lim)) return false;
-        mbar_arrive_expect_tx(&dfull[slot], p.dbox_bytes);
-        tc::tma_load_5d(smem_u32(dring + slot * p.dslot_bytes), &p.tmap_dy, 0, 0, 0, y0 + 1, zpad,
-                        smem_u32(&dfull[slot]));
+        const uint32_t bytes = (uint32_t)min(TYW, p.Yp - (y0 + 1)) * (uint32_t)(row_elems * 2);
+        mbar_arrive_expect_tx(&dfull[slot], bytes);
+        tc::bulk_load(smem_u32(dring + slot * p.dslot_bytes),
+                      p.dy + (size_t)zpad * plane_elems + (size_t)(y0 + 1) * row_elems, bytes,
+                      smem_u32(&dfull[slot]));
         gd++;
         return true;
       };
@@ -685,17 +805,24 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g,
   w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// fp32 weights [L][27][16 co][16 ci] -> bf16 forward tiles [L][27][2][16][8]
-// (K = ci halves) and dgrad tiles (taps mirrored, co <-> ci).
+// fp32 weights [L][27][16 co][16 ci] -> bf16 B tiles [L][rot][dx][2 halves]
+// [144 rows][8] (layout of the forward kernel's stacked B operand), K =
+// input channel 8h + c.  The dgrad tiles hold the mirrored tap with co and
+// ci exchanged (the adjoint convolution).
 __global__ void pack_weights_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf,
                                     __nv_bfloat16* __restrict__ wt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= NLAYER * NTAP * 16 * 16) return;
-  const int c = i % 8, n = (i / 8) % 16, h = (i / 128) % 2, tap = (i / 256) % NTAP,
-            l = i / (256 * NTAP);
+  if (i >= NLAYER * W_TILES * 2 * NSTACK * 8) return;
+  const int c = i % 8, n = (i / 8) % NSTACK, h = (i / (8 * NSTACK)) % 2,
+            tile = (i / (16 * NSTACK)) % W_TILES, l = i / (16 * NSTACK * W_TILES);
+  const int rot = tile / 3, dx = tile % 3;
+  const int co = n % 16, sj = n / 16, s = sj % 3, jrow = sj / 3;
+  const int dz = 2 - (((s - rot + 1) % 3 + 3) % 3);
+  const int tap = dz * 9 + (2 - jrow) * 3 + dx;
+  const int k = 8 * h + c;
   const size_t base = (size_t)l * NTAP * 256;
-  wf[i] = __float2bfloat16_rn(w[base + (size_t)tap * 256 + n * 16 + (8 * h + c)]);
-  wt[i] = __float2bfloat16_rn(w[base + (size_t)(NTAP - 1 - tap) * 256 + (8 * h + c) * 16 + n]);
+  wf[i] = __float2bfloat16_rn(w[base + (size_t)tap * 256 + co * 16 + k]);
+  wt[i] = __float2bfloat16_rn(w[base + (size_t)(NTAP - 1 - tap) * 256 + k * 16 + co]);
 }
 
 // 2:1 restriction (2x2x2 average) of a solver field (2 ghosts) to a dense

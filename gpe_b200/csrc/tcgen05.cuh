@@ -94,15 +94,25 @@ __device__ __forceinline__ void ld_32x32b_x16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// 5-D tiled TMA load into this CTA's shared memory (no multicast).
-__device__ __forceinline__ void tma_load_5d(uint32_t dst_saddr, const void* tmap,
-                                            int c0, int c1, int c2, int c3, int c4,
-                                            uint32_t mbar_saddr) {
+// Zero 32 lanes x 16 columns (this thread's lane).  Complete with wait_st.
+__device__ __forceinline__ void st_32x32b_x16_zero(uint32_t taddr) {
+  const uint32_t z = 0;
   asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
-      ::"r"(dst_saddr), "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
-        "r"(mbar_saddr)
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};"
+      ::"r"(taddr), "r"(z) : "memory");
+}
+__device__ __forceinline__ void wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// 1-D bulk copy global -> this CTA's shared memory (no multicast); both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(uint32_t dst_saddr, const void* src, uint32_t bytes,
+                                          uint32_t mbar_saddr) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(dst_saddr), "l"(src), "r"(bytes), "r"(mbar_saddr)
       : "memory");
 }
 

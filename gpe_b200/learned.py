@@ -1,0 +1,280 @@
+"""Training and evaluation of the learned coarse-grid correction.
+
+Workload (seeded, synthetic): fine grid 256^3, h = 0.25, periodic, 2nd-order
+differences, equation 4 with g = mu = 1 and no trap, FP64, RK4 with
+dt_f = 0.01; initial condition the random-phase field of |k| <= 1.0
+(gpe_b200.ic.random_phase).  Coarse grid 128^3, h = 0.5: the fine field
+restricted 2:1 (2x2x2 average, which lands exactly on the coarse nodes),
+stepped with complex64 RK4 at dt = 0.02, followed by the network's
+correction after every step.
+
+Training pairs come from the fine solver itself: for a fine trajectory
+psi_f(t_k), t_k = k dt, the input is one coarse step of R psi_f(t_k) and the
+target R psi_f(t_{k+1}); the loss is mean |u + delta(u) - target|^2 and the
+network learns what the coarse step misses.  Every forward, backward and
+Adam update runs in the library's tcgen05 kernels (gpe_b200.cnn).
+
+Evaluation on held-out seeds: the same fine reference, restricted, against
+the coarse run with and without the network: relative L2 error of the
+density |psi|^2 on the coarse grid at the checkpoint times, and the drift of
+the discrete conserved energy H4 of each run.
+
+  python -m gpe_b200.learned --out results.json --weights cnn.npz
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from dataclasses import asdict, dataclass, field
+
+import numpy as np
+
+from .cnn import CoarseCorrector, init_weights, restrict
+from .ic import random_phase
+from .solver import GpeParams, GpeSolver
+
+
+@dataclass
+class LearnedConfig:
+    fine_n: int = 256
+    fine_h: float = 0.25
+    coarse_n: int = 128
+    dt: float = 0.02            # coarse step
+    fine_substeps: int = 2      # fine reference steps per coarse step (dt_f = 0.01)
+    kmax: float = 1.0
+    out_scale: float = 0.01
+    coarse_kahan: bool = True
+    train_seeds: list = field(default_factory=lambda: [0, 1, 2, 3])
+    t_train: float = 10.0
+    iters: int = 4000
+    lr: float = 1e-3
+    lr_final: float = 1e-4
+    eval_seeds: list = field(default_factory=lambda: list(range(100, 116)))
+    t_end: float = 50.0
+    checkpoints: list = field(default_factory=lambda: [1.0, 5.0, 10.0, 20.0, 50.0])
+    device: int = 0
+
+    @property
+    def coarse_h(self) -> float:
+        return self.fine_h * self.fine_n / self.coarse_n
+
+
+def params(n: int, h: float, precision: int, kahan: bool = False, device: int = 0) -> GpeParams:
+    xr = (n - 1) * h / 2
+    return GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
+                     order=2, precision=precision, kahan=kahan, g=1.0, mu=1.0, device=device)
+
+
+def fine_solver(cfg: LearnedConfig, seed: int, precision: int = 16, kahan: bool = False,
+                dt: float | None = None) -> GpeSolver:
+    import torch
+    dev = torch.device("cuda", cfg.device)
+    s = GpeSolver(params(cfg.fine_n, cfg.fine_h, precision, kahan, cfg.device),
+                  dt=dt if dt is not None else cfg.dt / cfg.fine_substeps)
+    psi = random_phase(torch, cfg.fine_n, cfg.fine_h, cfg.kmax, seed, dev,
+                       torch.complex128 if precision == 16 else torch.complex64)
+    s.set_state(psi)
+    del psi
+    return s
+
+
+def coarse_solver(cfg: LearnedConfig) -> GpeSolver:
+    return GpeSolver(params(cfg.coarse_n, cfg.coarse_h, 8, cfg.coarse_kahan, cfg.device), dt=cfg.dt)
+
+
+def restricted(cfg: LearnedConfig, fine: GpeSolver):
+    import torch
+    n = cfg.coarse_n
+    out = torch.empty((n, n, n), dtype=torch.complex64, device=torch.device("cuda", cfg.device))
+    restrict(fine, out)
+    return out
+
+
+def generate(cfg: LearnedConfig, seed: int, t_end: float):
+    """Restricted fine states at t = k dt, k = 0..K (one CUDA tensor)."""
+    import torch
+    K = int(round(t_end / cfg.dt))
+    n = cfg.coarse_n
+    seq = torch.empty((K + 1, n, n, n), dtype=torch.complex64,
+                      device=torch.device("cuda", cfg.device))
+    f = fine_solver(cfg, seed)
+    restrict(f, seq[0])
+    for k in range(K):
+        f.advance(cfg.fine_substeps)
+        restrict(f, seq[k + 1])
+    f.close()
+    return seq
+
+
+def pair_loss(u, target) -> float:
+    """Mean over sites of |u - target|^2 (the loss of the zero correction)."""
+    import torch
+    return float(torch.mean(torch.abs(u - target) ** 2).item())
+
+
+def train(cfg: LearnedConfig, net: CoarseCorrector, data, log_every: int = 500) -> dict:
+    """Adam on random pairs of the training trajectories; cosine learning
+    rate from lr to lr_final.  Returns the loss history and, every log_every
+    iterations, the loss of the zero correction on the same pair."""
+    import torch
+    rng = np.random.default_rng(1234)
+    c = coarse_solver(cfg)
+    hist, base = [], []
+    t0 = time.perf_counter()
+    for it in range(cfg.iters):
+        s = int(rng.integers(len(data)))
+        k = int(rng.integers(data[s].shape[0] - 1))
+        c.set_state(data[s][k])
+        c.solver()
+        lr = cfg.lr_final + 0.5 * (cfg.lr - cfg.lr_final) * (1 + math.cos(math.pi * it / cfg.iters))
+        loss = net.train_step(c, data[s][k + 1], lr)
+        hist.append(loss)
+        if it % log_every == 0 or it == cfg.iters - 1:
+            u = torch.empty_like(data[s][k + 1])
+            c.get_state_device(u)
+            base.append((it, k, loss, pair_loss(u, data[s][k + 1])))
+    c.close()
+    return {"loss": hist, "checks": base, "seconds": time.perf_counter() - t0}
+
+
+def density_error(a, b) -> float:
+    import torch
+    da = torch.abs(a) ** 2
+    db = torch.abs(b) ** 2
+    return float((torch.linalg.vector_norm(da - db) / torch.linalg.vector_norm(db)).item())
+
+
+def evaluate(cfg: LearnedConfig, net: CoarseCorrector | None, seeds, t_end: float,
+             checkpoints) -> list:
+    """Per seed: density errors at the checkpoints and H4 drift of the plain
+    coarse run and (when net is given) the corrected one."""
+    import torch
+    out = []
+    ck = sorted(t for t in checkpoints if t <= t_end + 1e-9)
+    for seed in seeds:
+        f = fine_solver(cfg, seed)
+        ref0 = restricted(cfg, f)
+        runs = {"plain": coarse_solver(cfg)}
+        if net is not None:
+            runs["learned"] = coarse_solver(cfg)
+            net.attach(runs["learned"])
+        h0 = {}
+        for name, c in runs.items():
+            c.set_state(ref0)
+            h0[name] = c.energy()[1]
+        hf0 = f.energy()[1]
+        rec = {"seed": seed, "t": [], "fine_H4_drift": []}
+        for name in runs:
+            rec[name] = {"density_err": [], "H4_drift": []}
+        k_done = 0
+        for t in ck:
+            k = int(round(t / cfg.dt))
+            f.advance((k - k_done) * cfg.fine_substeps)
+            ref = restricted(cfg, f)
+            rec["t"].append(t)
+            rec["fine_H4_drift"].append(abs(f.energy()[1] - hf0) / abs(hf0))
+            for name, c in runs.items():
+                c.advance(k - k_done)
+                u = torch.empty_like(ref)
+                c.get_state_device(u)
+                rec[name]["density_err"].append(density_error(u, ref))
+                rec[name]["H4_drift"].append(abs(c.energy()[1] - h0[name]) / abs(h0[name]))
+            k_done = k
+        for c in runs.values():
+            c.close()
+        f.close()
+        out.append(rec)
+    return out
+
+
+def summarize(results: list) -> dict:
+    s = {}
+    names = [k for k in results[0] if isinstance(results[0][k], dict)]
+    ts = results[0]["t"]
+    for name in names:
+        errs = np.array([r[name]["density_err"] for r in results])
+        drift = np.array([r[name]["H4_drift"] for r in results])
+        s[name] = {"t": ts, "density_err_median": np.median(errs, axis=0).tolist(),
+                   "density_err_max": errs.max(axis=0).tolist(),
+                   "H4_drift_median": np.median(drift, axis=0).tolist()}
+    s["fine_H4_drift_median"] = np.median([r["fine_H4_drift"] for r in results], axis=0).tolist()
+    return s
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description="train and evaluate the learned coarse-grid correction")
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--weights", required=True, help="npz written after training (w, b)")
+    ap.add_argument("--load", help="skip training: evaluate these weights")
+    ap.add_argument("--iters", type=int)
+    ap.add_argument("--t-train", type=float)
+    ap.add_argument("--train-seeds", type=int, help="number of training seeds (0, 1, ...)")
+    ap.add_argument("--eval-seeds", type=int, help="number of held-out seeds (100, 101, ...)")
+    ap.add_argument("--t-end", type=float)
+    ap.add_argument("--fine-n", type=int)
+    ap.add_argument("--coarse-n", type=int)
+    ap.add_argument("--lr", type=float)
+    ap.add_argument("--out-scale", type=float)
+    a = ap.parse_args(argv)
+    cfg = LearnedConfig()
+    if a.iters is not None:
+        cfg.iters = a.iters
+    if a.t_train is not None:
+        cfg.t_train = a.t_train
+    if a.train_seeds is not None:
+        cfg.train_seeds = list(range(a.train_seeds))
+    if a.eval_seeds is not None:
+        cfg.eval_seeds = list(range(100, 100 + a.eval_seeds))
+    if a.t_end is not None:
+        cfg.t_end = a.t_end
+    if a.fine_n is not None:
+        cfg.fine_n = a.fine_n
+    if a.coarse_n is not None:
+        cfg.coarse_n = a.coarse_n
+    if a.lr is not None:
+        cfg.lr, cfg.lr_final = a.lr, a.lr / 10
+    if a.out_scale is not None:
+        cfg.out_scale = a.out_scale
+    import torch
+    torch.cuda.set_device(cfg.device)
+    n = cfg.coarse_n
+    report = {"config": asdict(cfg)}
+    if a.load:
+        z = np.load(a.load)
+        w, b = z["w"], z["b"]
+    else:
+        net = CoarseCorrector(n, n, n, cfg.device, train=True, out_scale=cfg.out_scale)
+        t0 = time.perf_counter()
+        data = [generate(cfg, s, cfg.t_train) for s in cfg.train_seeds]
+        report["generate_seconds"] = time.perf_counter() - t0
+        w, b = init_weights(7)
+        net.set_weights(w, b)
+        tr = train(cfg, net, data)
+        del data
+        torch.cuda.empty_cache()
+        h = tr["loss"]
+        m = max(1, len(h) // 20)
+        report["train"] = {"seconds": tr["seconds"], "iters": cfg.iters,
+                           "loss_first": float(np.mean(h[:m])), "loss_last": float(np.mean(h[-m:])),
+                           "checks (iter, k, loss, zero-correction loss)": tr["checks"]}
+        w, b = net.get_weights()
+        np.savez_compressed(a.weights, w=w, b=b, out_scale=cfg.out_scale)
+        net.close()
+    net = CoarseCorrector(n, n, n, cfg.device, out_scale=cfg.out_scale)
+    net.set_weights(w, b)
+    t0 = time.perf_counter()
+    res = evaluate(cfg, net, cfg.eval_seeds, cfg.t_end, cfg.checkpoints)
+    report["eval_seconds"] = time.perf_counter() - t0
+    report["eval"] = res
+    report["summary"] = summarize(res)
+    net.close()
+    with open(a.out, "w") as fh:
+        json.dump(report, fh, indent=1)
+    print(json.dumps(report["summary"]))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -18,7 +18,7 @@ from dataclasses import dataclass, fields
 import numpy as np
 
 from ._lib import (GpeError, GpeParamsC, GpeStepInfoC, GpeTimeC, GpeTimingC, SCHEMES,
-                   TIMING_FAMILIES, check, lib)
+                   TIMING_FAMILIES, check, lib, torch_ready)
 
 
 @dataclass
@@ -121,6 +121,7 @@ class GpeSolver:
         """Load psi (numpy host array or CUDA torch tensor, interior layout)."""
         if hasattr(psi, "is_cuda") and psi.is_cuda:
             t = psi.contiguous()
+            torch_ready(t)
             eb = 16 if str(t.dtype) == "torch.complex128" else 8
             check(lib().gpe_gpu_set_state_device(self._ctx, ctypes.c_void_p(t.data_ptr()), eb),
                   self._ctx)
@@ -142,6 +143,7 @@ class GpeSolver:
 
     def get_state_device(self, out) -> None:
         """Copy the state into a contiguous CUDA torch tensor (complex64/128)."""
+        torch_ready(out)
         eb = 16 if str(out.dtype) == "torch.complex128" else 8
         check(lib().gpe_gpu_get_state_device(self._ctx, ctypes.c_void_p(out.data_ptr()), eb),
               self._ctx)

@@ -138,7 +138,11 @@ int gpe_gpu_grid(const gpe_ctx* ctx, double* x, double* y, double* z);
  * halo exchange did before solver() (src/gpe.f90:165-174). */
 int gpe_gpu_set_state(gpe_ctx* ctx, const void* psi, int32_t elem_bytes);
 int gpe_gpu_get_state(gpe_ctx* ctx, void* psi, int32_t elem_bytes);
-/* Same with DEVICE arrays on the context's device. */
+/* Same with DEVICE arrays on the context's device.  The copy is ordered on
+ * the context's own (non-blocking) stream only: the caller must have
+ * finished writing psi (set) or reading its previous contents (get) on its
+ * own streams before the call, e.g. with cudaStreamSynchronize.  The call
+ * returns after the copy is complete. */
 int gpe_gpu_set_state_device(gpe_ctx* ctx, const void* psi,
                              int32_t elem_bytes);
 int gpe_gpu_get_state_device(gpe_ctx* ctx, void* psi, int32_t elem_bytes);

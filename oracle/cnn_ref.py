@@ -11,8 +11,8 @@ defined for this project (include/gpe_cnn.h):
   delta = out_scale * (conv3d(a_3, W_3) + b_3)[..., 0:2]
 
 conv3d: 3x3x3, periodic, out(p)[co] = sum_tap sum_ci W[tap][co][ci] a(p + d_tap)[ci],
-tap = (dz+1)*9 + (dy+1)*3 + (dx+1).  GELU(x) = x Phi(x) (Hendrycks & Gimpel,
-2016), Phi the standard normal CDF.  Loss of a pair (u, target):
+tap = (dz+1)*9 + (dy+1)*3 + (dx+1).  GELU in its tanh form (Hendrycks &
+Gimpel, 2016): 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).  Loss of a pair (u, target):
 mean over sites of |u + delta(u) - target|^2.
 
 emulate=True mirrors the CUDA path's rounding points: weights, the packed
@@ -30,12 +30,6 @@ import numpy as np
 
 NL, NT, C = 4, 27, 16
 
-try:
-    from scipy.special import erf as _erf
-except ImportError:  # pragma: no cover
-    _erf = np.vectorize(math.erf)
-
-
 def taps():
     """(dz, dy, dx) of tap index t = (dz+1)*9 + (dy+1)*3 + (dx+1)."""
     return [(t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1) for t in range(NT)]
@@ -49,12 +43,17 @@ def bf16(x):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+_C = math.sqrt(2.0 / math.pi)
+_A = 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    return 0.5 * x * (1.0 + np.tanh(_C * (x + _A * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2 * math.pi)
+    t = np.tanh(_C * (x + _A * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _C * (1.0 + 3.0 * _A * x * x)
 
 
 def shift(a, d):

@@ -14,10 +14,18 @@ target R psi_f(t_{k+1}); the loss is mean |u + delta(u) - target|^2 and the
 network learns what the coarse step misses.  Every forward, backward and
 Adam update runs in the library's tcgen05 kernels (gpe_b200.cnn).
 
+Training inputs are also taken on-policy: up to `rollout` corrected coarse
+steps from a restricted fine state first, so the network learns to pull its
+own drift back (without this the corrected run diverges by t = 50), plus a
+little input noise.
+
 Evaluation on held-out seeds: the same fine reference, restricted, against
 the coarse run with and without the network: relative L2 error of the
 density |psi|^2 on the coarse grid at the checkpoint times, and the drift of
-the discrete conserved energy H4 of each run.
+the discrete energy H4 of each run -- next to the coarse-grid H4 of the
+restricted fine state itself, which is not conserved (energy moves below the
+coarse grid's resolution), so a corrected run that tracks the fine solution
+drifts with it.
 
   python -m gpe_b200.learned --out results.json --weights cnn.npz
 """
@@ -48,9 +56,11 @@ class LearnedConfig:
     coarse_kahan: bool = True
     train_seeds: list = field(default_factory=lambda: [0, 1, 2, 3])
     t_train: float = 10.0
-    iters: int = 4000
+    iters: int = 6000
     lr: float = 1e-3
     lr_final: float = 1e-4
+    rollout: int = 8            # on-policy inputs: up to this many corrected steps first
+    noise: float = 0.002        # std of complex Gaussian noise added to training inputs
     eval_seeds: list = field(default_factory=lambda: list(range(100, 116)))
     t_end: float = 50.0
     checkpoints: list = field(default_factory=lambda: [1.0, 5.0, 10.0, 20.0, 50.0])
@@ -116,17 +126,38 @@ def pair_loss(u, target) -> float:
 
 def train(cfg: LearnedConfig, net: CoarseCorrector, data, log_every: int = 500) -> dict:
     """Adam on random pairs of the training trajectories; cosine learning
-    rate from lr to lr_final.  Returns the loss history and, every log_every
-    iterations, the loss of the zero correction on the same pair."""
+    rate from lr to lr_final.  With cfg.rollout = M > 0, a pair's input is
+    the network's own state: m in [0, M] corrected coarse steps from
+    R psi_f(t_{k-m}) reach t_k, then one coarse step, against R psi_f(t_{k+1})
+    -- the network learns to pull its own drift back to the fine solution.
+    Returns the loss history and, every log_every iterations, the loss of
+    the zero correction on the same pair."""
     import torch
     rng = np.random.default_rng(1234)
+    gen = torch.Generator(device=data[0].device)
+    gen.manual_seed(4321)
     c = coarse_solver(cfg)
+    roll = None
+    if cfg.rollout > 0:
+        roll = coarse_solver(cfg)
+        net.attach(roll)
+    state = torch.empty_like(data[0][0])
     hist, base = [], []
     t0 = time.perf_counter()
     for it in range(cfg.iters):
         s = int(rng.integers(len(data)))
-        k = int(rng.integers(data[s].shape[0] - 1))
-        c.set_state(data[s][k])
+        m = int(rng.integers(cfg.rollout + 1)) if roll is not None else 0
+        k = int(rng.integers(m, data[s].shape[0] - 1))
+        if m > 0:
+            roll.set_state(data[s][k - m])
+            roll.advance(m)
+            roll.get_state_device(state)
+        else:
+            state.copy_(data[s][k])
+        if cfg.noise > 0:
+            z = torch.randn(state.shape, generator=gen, device=state.device, dtype=torch.complex64)
+            state.add_(cfg.noise * z)
+        c.set_state(state)
         c.solver()
         lr = cfg.lr_final + 0.5 * (cfg.lr - cfg.lr_final) * (1 + math.cos(math.pi * it / cfg.iters))
         loss = net.train_step(c, data[s][k + 1], lr)
@@ -134,8 +165,10 @@ def train(cfg: LearnedConfig, net: CoarseCorrector, data, log_every: int = 500) 
         if it % log_every == 0 or it == cfg.iters - 1:
             u = torch.empty_like(data[s][k + 1])
             c.get_state_device(u)
-            base.append((it, k, loss, pair_loss(u, data[s][k + 1])))
+            base.append((it, k, m, loss, pair_loss(u, data[s][k + 1])))
     c.close()
+    if roll is not None:
+        roll.close()
     return {"loss": hist, "checks": base, "seconds": time.perf_counter() - t0}
 
 
@@ -165,7 +198,10 @@ def evaluate(cfg: LearnedConfig, net: CoarseCorrector | None, seeds, t_end: floa
             c.set_state(ref0)
             h0[name] = c.energy()[1]
         hf0 = f.energy()[1]
-        rec = {"seed": seed, "t": [], "fine_H4_drift": []}
+        probe = coarse_solver(cfg)  # coarse-grid H4 of the restricted fine state
+        probe.set_state(ref0)
+        hr0 = probe.energy()[1]
+        rec = {"seed": seed, "t": [], "fine_H4_drift": [], "restricted_H4_drift": []}
         for name in runs:
             rec[name] = {"density_err": [], "H4_drift": []}
         k_done = 0
@@ -175,6 +211,8 @@ def evaluate(cfg: LearnedConfig, net: CoarseCorrector | None, seeds, t_end: floa
             ref = restricted(cfg, f)
             rec["t"].append(t)
             rec["fine_H4_drift"].append(abs(f.energy()[1] - hf0) / abs(hf0))
+            probe.set_state(ref)
+            rec["restricted_H4_drift"].append(abs(probe.energy()[1] - hr0) / abs(hr0))
             for name, c in runs.items():
                 c.advance(k - k_done)
                 u = torch.empty_like(ref)
@@ -184,6 +222,7 @@ def evaluate(cfg: LearnedConfig, net: CoarseCorrector | None, seeds, t_end: floa
             k_done = k
         for c in runs.values():
             c.close()
+        probe.close()
         f.close()
         out.append(rec)
     return out
@@ -200,6 +239,8 @@ def summarize(results: list) -> dict:
                    "density_err_max": errs.max(axis=0).tolist(),
                    "H4_drift_median": np.median(drift, axis=0).tolist()}
     s["fine_H4_drift_median"] = np.median([r["fine_H4_drift"] for r in results], axis=0).tolist()
+    s["restricted_H4_drift_median"] = np.median([r["restricted_H4_drift"] for r in results],
+                                                axis=0).tolist()
     return s
 
 
@@ -217,6 +258,8 @@ def main(argv=None) -> int:
     ap.add_argument("--coarse-n", type=int)
     ap.add_argument("--lr", type=float)
     ap.add_argument("--out-scale", type=float)
+    ap.add_argument("--rollout", type=int)
+    ap.add_argument("--noise", type=float)
     a = ap.parse_args(argv)
     cfg = LearnedConfig()
     if a.iters is not None:
@@ -237,6 +280,10 @@ def main(argv=None) -> int:
         cfg.lr, cfg.lr_final = a.lr, a.lr / 10
     if a.out_scale is not None:
         cfg.out_scale = a.out_scale
+    if a.rollout is not None:
+        cfg.rollout = a.rollout
+    if a.noise is not None:
+        cfg.noise = a.noise
     import torch
     torch.cuda.set_device(cfg.device)
     n = cfg.coarse_n
@@ -258,7 +305,7 @@ def main(argv=None) -> int:
         m = max(1, len(h) // 20)
         report["train"] = {"seconds": tr["seconds"], "iters": cfg.iters,
                            "loss_first": float(np.mean(h[:m])), "loss_last": float(np.mean(h[-m:])),
-                           "checks (iter, k, loss, zero-correction loss)": tr["checks"]}
+                           "checks (iter, k, m, loss, zero-correction loss)": tr["checks"]}
         w, b = net.get_weights()
         np.savez_compressed(a.weights, w=w, b=b, out_scale=cfg.out_scale)
         net.close()

@@ -454,6 +454,82 @@ def run_learned(args):
     return 0
 
 
+def c2_params(precision, kahan):
+    from gpe_b200 import GpeParams
+    n, h = 128, 0.4
+    xr = h * (n - 1) / 2
+    return GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk45", eqn_to_solve=4,
+                     bcs=2, order=4, precision=precision, kahan=kahan, g=1.0, mu=1.0)
+
+
+def c2_initial_state():
+    """Vortex ring of radius 8 in the xy-plane times the 'ring'-table Pade
+    rarefaction pulse at x0 = -10 (numpy complex128, (nz, ny, nx))."""
+    import numpy as np
+
+    from gpe_b200 import ic
+    p = c2_params(16, False)
+    x = np.linspace(-p.xr, p.xr, p.nx)
+    return ic.vortex_ring_xy(x, x, x, 0.0, 0.0, 0.0, 8.0) * ic.pade_pulse_ring(x, x, x, "ring", -10.0,
+                                                                                  0.0, 0.0, 0.0)
+
+
+def run_rkf45(args):
+    """C2: 128^3 reflective, 4th order, adaptive rkf45 (tolerance 1e-6, initial
+    dt 0.005) to t = 20, complex128 and complex64 + Kahan; steps, device time
+    and the complex64 run's density error against the complex128 run."""
+    import numpy as np
+    import torch
+
+    from gpe_b200 import GpeSolver
+    torch.cuda.set_device(0)
+    psi0 = c2_initial_state()
+    t_end = args.t_end
+    res = {}
+    finals = {}
+    sampler = ClockSampler(None)
+    sampler.start()
+    for name, prec, kahan in (("f64", 16, False), ("f32_kahan", 8, True)):
+        s = GpeSolver(c2_params(prec, kahan), dt=0.005)
+        s.set_state(psi0.astype(np.complex64) if prec == 8 else psi0)
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        steps = attempts = 0
+        n0 = s.get_norm()
+        t0 = time.perf_counter()
+        a.record(st)
+        while s.t < t_end - 1e-12:
+            info = s.solver()
+            steps += 1
+            attempts += info.attempts
+        e.record(st)
+        e.synchronize()
+        wall = time.perf_counter() - t0
+        ms = a.elapsed_time(e)
+        finals[name] = s.get_state(np.complex128)
+        res[name] = {"steps": steps, "attempts": attempts, "t": s.t, "last_dt": s.dt.real,
+                     "device_ms": ms, "wall_s": wall, "norm_rel_change": abs(s.get_norm() - n0) / n0,
+                     "site_updates_per_s": 128 ** 3 * steps / (ms / 1e3)}
+        s.close()
+    clocks = sampler.stop()
+    ra, rb = np.abs(finals["f32_kahan"]) ** 2, np.abs(finals["f64"]) ** 2
+    dens = float(np.linalg.norm(ra - rb) / np.linalg.norm(rb))
+    line = {
+        "metric": "time to t=20 (rkf45, 128^3)", "value": res["f32_kahan"]["device_ms"] / 1e3,
+        "unit": "s", "n_gpus": 1, "steps": res["f32_kahan"]["steps"], "warmup": 0,
+        "ms_per_step": res["f32_kahan"]["device_ms"] / max(res["f32_kahan"]["steps"], 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (+Kahan)",
+        "data": "synthetic (vortex ring r0=8 x Pade pulse at x0=-10)",
+        "config": {"workload": "128^3 h=0.4 reflective, order 4, rkf45 tol 1e-6, dt0=0.005, "
+                               "to t=%g, eqn 4 g=mu=1" % t_end},
+        "runs": res, "density_rel_l2_f32_vs_f64": dens, "clocks": clocks,
+        "note": "step control is on the host: every attempt reads errmax back (one sync)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def workload_config(ngpus, n=N_GRID):
     return {"workload": f"{n}^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
                         "(g=mu=1, V=0), complex64 psi + Kahan compensation, FP64 norm per step",
@@ -475,7 +551,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID,
                     help="cube edge (default 512; smaller sizes are for profiling captures)")
-    ap.add_argument("--workload", default="cube", choices=["cube", "ensemble", "learned"])
+    ap.add_argument("--workload", default="cube", choices=["cube", "ensemble", "learned", "rkf45"])
+    ap.add_argument("--t-end", type=float, default=20.0, help="rkf45 workload end time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -484,6 +561,8 @@ def main():
         if "--steps" not in sys.argv:
             args.steps = 500
         return run_ensemble(args)
+    if args.workload == "rkf45":
+        return run_rkf45(args)
     if args.workload == "learned":
         if "--steps" not in sys.argv:
             args.steps = 200

@@ -12,6 +12,15 @@ random-phase field of |k| <= k_max times the Thomas-Fermi profile
 sqrt(max(0, 1 - V)) of the harmonic trap V = omega^2 r^2 / 2 on the grid
 x_i = -xr + i h (the reference's get_grid, src/ic.f90:32-69).
 
+vortex_ring_xy: a vortex ring in the xy-plane propagating along z, the
+reference's vortex_ring with plane 'xy' (src/ic.f90:352-401): the product of
+two Pade-core line vortices at the distances d1, d2 from the ring's two
+crossings of each meridional half-plane.
+
+pade_pulse_ring: the Pade approximation of a rarefaction pulse / vortex ring
+moving along x (src/ic.f90:513-574; the constants are the reference's
+published 'ring' and 'pulse' tables).
+
 vortex_line_pade: a straight vortex line along z through the origin,
 psi = r R(r) e^{i atan2(y, x)} with the Pade core R of get_rr
 (src/ic.f90:888-901).
@@ -54,6 +63,52 @@ def trapped_random_phase(torch, n: int, h: float, omega: float, kmax: float, see
     r2 = x[None, None, :] ** 2 + x[None, :, None] ** 2 + x[:, None, None] ** 2
     tf = torch.sqrt(torch.clamp(1.0 - 0.5 * omega * omega * r2, min=0.0))
     return (psi * tf).to(dtype or torch.complex64).contiguous()
+
+
+def _rr(r):
+    """The Pade core amplitude R(r)/r of get_rr (src/ic.f90:888-901)."""
+    return np.sqrt((0.3437 + 0.0286 * r ** 2) / (1.0 + 0.3333 * r ** 2 + 0.0286 * r ** 4))
+
+
+def vortex_ring_xy(x, y, z, x0, y0, z0, r0, scal=1.0, amp=0.0, mm=0, r1=0.0, kk=0, direction=1.0):
+    """(nz, ny, nx) complex128 vortex ring of radius r0 centred at (x0, y0, z0)
+    in the xy-plane, with the optional mode-mm disturbance of amplitude amp
+    and helical kk / r1 terms of the reference."""
+    Z, Y, X = np.meshgrid(np.asarray(z), np.asarray(y), np.asarray(x), indexing="ij")
+    theta = np.arctan2(Y - y0, X - x0)
+    s = np.sqrt((X - x0) ** 2 + (Y - y0) ** 2) - r1 * np.sin(kk * theta)
+    dist = amp * np.cos(mm * theta)
+    pp = Z - r1 * np.cos(kk * theta)
+    a = scal * (pp - z0)
+    b1 = scal * (s + r0 - dist)
+    b2 = scal * (s - r0 - dist)
+    d1 = np.sqrt(a ** 2 + b1 ** 2)
+    d2 = np.sqrt(a ** 2 + b2 ** 2)
+    return _rr(d1) * (a + direction * 1j * b1) * _rr(d2) * (a - direction * 1j * b2)
+
+
+_PADE = {  # a1..a9, U, m (src/ic.f90:563-576)
+    "ring": ((-1.1, 0.0170524, 0.0289452, -0.953, -0.0049767, -0.0594346, 0.04, 0.21, 0.00612),
+             0.6, 8.97),
+    "pulse": ((-0.79792, 0.00388059, 0.00882276, -0.7981, -0.012783, -0.0574092, 0.0399, 0.199,
+               0.0058), 0.63, 8.37),
+}
+
+
+def pade_pulse_ring(x, y, z, which, x0, y0, z0, r0):
+    """(nz, ny, nx) complex128 Pade rarefaction pulse / ring moving along x."""
+    a, U, m = _PADE[which]
+    pow_ = 7.0 / 4.0
+    Z, Y, X = np.meshgrid(np.asarray(z), np.asarray(y), np.asarray(x), indexing="ij")
+    s = np.sqrt((Y - y0) ** 2 + (Z - z0) ** 2)
+    one_2u = 1.0 - 2.0 * U ** 2
+    x2 = (X - x0) ** 2
+    s2 = (s - r0) ** 2
+    q = x2 + one_2u * s2
+    denom = (1.0 + a[7] * x2 + a[6] * s2 + a[8] * q ** 2) ** pow_
+    uu = 1.0 + (a[0] + a[2] * x2 + a[1] * s2 + m * a[8] ** pow_ * U * (2.0 * x2 - one_2u * s2)) * q / denom
+    vv = (X - x0) * (a[3] + a[5] * x2 + a[4] * s2 - m * a[8] ** pow_ * q ** 2) / denom
+    return uu + 1j * vv
 
 
 def vortex_line_pade(x, y, z):

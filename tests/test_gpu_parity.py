@@ -289,3 +289,28 @@ def test_timing_and_launch_count():
     t = g.timing()
     assert t["stage_mid"]["launches"] == 6 and t["stage_mid"]["ms"] > 0
     g.close()
+
+
+def test_c2_rkf45_configuration_matches_oracle():
+    """128^3, h=0.4, reflective, order 4, rkf45 from the ring x pulse state:
+    the first three adaptive steps (psi, accepted dt, attempts) against the
+    oracle."""
+    import bench
+    psi = bench.c2_initial_state()
+    p = bench.c2_params(16, False)
+    g = GpeSolver(p, dt=0.005)
+    g.set_state(psi)
+    o = oracle.Oracle(oracle.OracleParams(nx=p.nx, ny=p.ny, nz=p.nz, xr=p.xr, yr=p.yr, zr=p.zr,
+                                          scheme="rk45", eqn_to_solve=4, bcs=2, order=4,
+                                          g=1.0, mu=1.0))
+    tm = oracle.OraTime(0.0, 0.0, 0.005, 0.0, 0)
+    q = psi
+    for _ in range(3):
+        info = g.solver()
+        q, em, att = o.solver(q, tm)
+        assert info.attempts == att
+        assert g.dt == pytest.approx(complex(tm.dt_re, tm.dt_im), rel=1e-8)
+        # t sums the accepted steps, which agree to the rk45 dt tolerance
+        assert g.t == pytest.approx(tm.t, rel=1e-8)
+    assert rel_l2(g.get_state(), q) < 1e-9
+    g.close()

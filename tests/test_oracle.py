@@ -250,3 +250,20 @@ def test_drive_imaginary_time_renorm():
     psi, rec = oracle.drive(o, psi, tm, 5, renorm=True)
     assert o.get_norm(psi) == pytest.approx(1.0, rel=1e-12)
     assert len(rec) == 5 and tm.p == 5
+
+
+def test_product_ring_and_pulse_ics_match_the_oracle():
+    """gpe_b200.ic's ring and pulse initial conditions (used by the rkf45
+    workload) against the oracle's restatement of src/ic.f90."""
+    from gpe_b200 import ic
+    n = (20, 18, 16)
+    xr, yr, zr = 12.0, 11.0, 9.0
+    o = oracle.Oracle(oracle.OracleParams(nx=n[0], ny=n[1], nz=n[2], xr=xr, yr=yr, zr=zr))
+    x, y, z = (np.linspace(-xr, xr, n[0]), np.linspace(-yr, yr, n[1]), np.linspace(-zr, zr, n[2]))
+    got = ic.vortex_ring_xy(x, y, z, 0.5, -0.3, 0.2, 6.0, amp=0.4, mm=3, r1=0.7, kk=2)
+    exp = o.ic_vortex_ring("xy", 0.5, -0.3, 0.2, 6.0, amp=0.4, mm=3, r1=0.7, kk=2)
+    np.testing.assert_allclose(got, exp, rtol=1e-13, atol=1e-14)
+    for which in ("ring", "pulse"):
+        got = ic.pade_pulse_ring(x, y, z, which, -4.0, 0.5, -0.5, 1.5)
+        exp = o.ic_pade_pulse_ring(which, -4.0, 0.5, -0.5, 1.5)
+        np.testing.assert_allclose(got, exp, rtol=1e-13, atol=1e-14)

@@ -52,6 +52,7 @@ struct gpe_cnn {
   float* d_b = nullptr;      // fp32 [4][16]
   __nv_bfloat16* d_wf = nullptr;
   __nv_bfloat16* d_wt = nullptr;
+  __nv_bfloat16* d_wf2 = nullptr;  // last layer, N = 32 layout
   unsigned char* d_mask = nullptr;  // [weights + biases]
   float* d_grad = nullptr;   // [weights + biases]
   float* d_m = nullptr;
@@ -102,7 +103,7 @@ uint32_t round1k(uint32_t b) { return (b + 1023u) & ~1023u; }
 // Items of a conv launch: y-slabs of TYF rows x z-chunks, about one per SM.
 void conv_items(const gpe_cnn* n, int rows, int* nslab, int* nzc, int* zchunk) {
   *nslab = (n->ny + rows - 1) / rows;
-  int want = std::max(1, n->num_sms / *nslab);
+  int want = std::max(1, F_CTAS_PER_SM * n->num_sms / *nslab);
   want = std::min(want, n->nz);
   *zchunk = (n->nz + want - 1) / want;
   *nzc = (n->nz + *zchunk - 1) / *zchunk;
@@ -111,8 +112,11 @@ void conv_items(const gpe_cnn* n, int rows, int* nslab, int* nzc, int* zchunk) {
 template <int EPI>
 int launch_conv(gpe_cnn* n, cudaStream_t st, const Act& in, int layer, bool dgrad,
                 ConvParams& p) {
+  // the last layer's 2 output channels use the N = 32 kernel
+  constexpr int CO = (EPI == EPI_RESID || EPI == EPI_DELTA) ? 2 : 16;
   p.in = in.p;
-  p.w = (dgrad ? n->d_wt : n->d_wf) + (size_t)layer * W_TILES * WT_BYTES / 2;
+  p.w = CO == 2 ? n->d_wf2
+                : (dgrad ? n->d_wt : n->d_wf) + (size_t)layer * W_TILES * WT_BYTES / 2;
   p.bias = dgrad ? nullptr : n->d_b + layer * 16;
   p.nx = n->nx; p.ny = n->ny; p.nz = n->nz;
   p.Xp = n->Xp; p.Yp = n->Yp; p.Zp = n->Zp; p.Hin = in.H;
@@ -123,10 +127,11 @@ int launch_conv(gpe_cnn* n, cudaStream_t st, const Act& in, int layer, bool dgra
   p.out_scale = n->prm.out_scale;
   if (!p.status) p.status = n->d_status;
   p.wait_limit_ns = CNN_WAIT_LIMIT_NS;
-  const size_t smem = 1024 + (size_t)FSLOTS * p.slot_bytes + 4096 + W_TILES * WT_BYTES + F_TAIL_BYTES;
-  auto fn = conv_fwd_kernel<EPI>;
+  const size_t smem = 1024 + (size_t)FSLOTS * p.slot_bytes + 4096 +
+                      W_TILES * OutShape<CO>::WTB + F_TAIL_BYTES;
+  auto fn = conv_fwd_kernel<EPI, CO>;
   CNN_CU(n, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = std::min(p.nitems, n->num_sms);
+  const int grid = std::min(p.nitems, F_CTAS_PER_SM * n->num_sms);
   fn<<<grid, F_THREADS, smem, st>>>(p);
   CNN_CU(n, cudaGetLastError());
   n->launches++;
@@ -296,7 +301,9 @@ int read_loss(gpe_cnn* n, cudaStream_t st, double* loss) {
 int repack_weights(gpe_cnn* n, cudaStream_t st) {
   pack_weights_kernel<<<(NLAYER * W_TILES * 2 * NSTACK * 8 + 255) / 256, 256, 0, st>>>(n->d_w, n->d_wf, n->d_wt);
   CNN_CU(n, cudaGetLastError());
-  n->launches++;
+  pack_out2_kernel<<<(W_TILES * 2 * OutShape<2>::NB * 8 + 255) / 256, 256, 0, st>>>(n->d_w, n->d_wf2);
+  CNN_CU(n, cudaGetLastError());
+  n->launches += 2;
   return GPE_OK;
 }
 
@@ -374,6 +381,7 @@ int gpe_cnn_create(const gpe_cnn_params* p, gpe_cnn** out) {
   if (cudaMalloc(&n->d_w, sizeof(float) * np) != cudaSuccess ||
       cudaMalloc(&n->d_wf, (size_t)NLAYER * W_TILES * WT_BYTES) != cudaSuccess ||
       cudaMalloc(&n->d_wt, (size_t)NLAYER * W_TILES * WT_BYTES) != cudaSuccess ||
+      cudaMalloc(&n->d_wf2, (size_t)W_TILES * OutShape<2>::WTB) != cudaSuccess ||
       cudaMalloc(&n->d_status, sizeof(int)) != cudaSuccess) {
     n->err = "cudaMalloc failed";
     return bail(GPE_ERR_OOM);
@@ -427,7 +435,7 @@ void gpe_cnn_destroy(gpe_cnn* n) {
   if (!n) return;
   cudaSetDevice(n->dev);
   cudaDeviceSynchronize();
-  void* ptrs[] = {n->d_w, n->d_wf, n->d_wt, n->d_mask, n->d_grad, n->d_m, n->d_v,
+  void* ptrs[] = {n->d_w, n->d_wf, n->d_wt, n->d_wf2, n->d_mask, n->d_grad, n->d_m, n->d_v,
                   n->A0.p, n->A1.p, n->A2.p, n->T[0].p, n->T[1].p, n->T[2].p, n->T[3].p,
                   n->P[0].p, n->P[1].p, n->P[2].p, n->GA.p, n->GB.p, n->d_delta,
                   n->d_wpart, n->d_bpart, n->d_lpart, n->d_status};

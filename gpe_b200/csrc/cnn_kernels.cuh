@@ -49,28 +49,47 @@ constexpr int NLAYER = 4;
 constexpr int TAP_BYTES = 2 * CH * 8 * 2;  // [2 halves][16 rows][8] bf16 = 512
 
 // forward / dgrad
-constexpr int TYF = 6;          // output rows per item
-constexpr int FSLOTS = 3;       // input planes in the shared-memory ring
-constexpr int F_GROUP_WARPS = 8;                 // one epilogue group: 2 warps per lane quarter
-constexpr int F_EPI_WARPS = 2 * F_GROUP_WARPS;   // two groups take alternate planes
+constexpr int TYF = 4;          // output rows per item
+constexpr int FSLOTS = 2;       // input planes in the shared-memory ring
+constexpr int F_EPI_WARPS = 8;  // one epilogue group: 2 warps per lane quarter
 constexpr int F_THREADS = 32 * (2 + F_EPI_WARPS);
+constexpr int F_CTAS_PER_SM = 2;  // one CTA's MMAs overlap the other's drain
 // Accumulators: three output planes in a rotating ring (plane z in slot
-// z mod 3), each with output rows y0-2 .. y0+TYF+1 (ACC_ROWS), column
+// z mod 3), each with the TYF output rows of the slab, column
 // (row * 3 + slot) * 16 + co.  Input row y' (box row i) of input plane j
-// feeds output rows y'-1, y', y'+1 (accumulator rows i .. i+2) of output
-// planes j-1, j, j+1 (all three slots): one contiguous block of 144 columns,
-// so a single MMA with N = 144 covers all nine (dz, dy) taps of one dx.
+// feeds output rows y'-1, y', y'+1 of output planes j-1, j, j+1 (all three
+// slots): for an interior input row one contiguous block of 144 columns,
+// so a single MMA with N = 144 covers all nine (dz, dy) taps of one dx; the
+// slab's first two and last two input rows feed only one or two of its
+// rows and use N = 48 / 96 with the matching part of B.
 constexpr int OSLOTS = 3;
-constexpr int ACC_ROWS = TYF + 4;
+constexpr int ACC_ROWS = TYF;
 constexpr int NSTACK = 3 * OSLOTS * CH;          // 144
-constexpr uint32_t F_TMEM_COLS = 512;
+constexpr uint32_t F_TMEM_COLS = 256;
 static_assert(ACC_ROWS * OSLOTS * CH <= (int)F_TMEM_COLS, "accumulator ring fits TMEM");
 // B tile of one (rotation j mod 3, dx): rows n = (jrow * 3 + s) * 16 + co
 // hold tap (dz index 2 - ((s - rot + 1) mod 3), dy index 2 - jrow, dx);
 // K = 16 input channels in two halves: [2][144][8] bf16.
 constexpr int WT_BYTES = 2 * NSTACK * 8 * 2;     // 4608
 constexpr int W_TILES = 9;                       // 3 rotations x 3 dx
-constexpr int EPI_ROWS = (TYF + 1) / 2;          // rows per epilogue warp
+// Per output-channel count: accumulator columns per (row, slot) and the
+// MMA's N.  The last layer has 2 output channels: 9 x 2 = 18 columns padded
+// to N = 32 (the 14 extra B rows are zero; they add exact zeros to columns
+// of the next rows, which accumulate in the same MMA stream).
+template <int CO>
+struct OutShape {
+  static constexpr int CW = CO;
+  static constexpr int NB = CO == 16 ? NSTACK : 32;  // rows of one B tile
+  static constexpr int WTB = 2 * NB * 8 * 2;
+  // N of an MMA feeding `cnt` (1..3) of the slab's rows, rounded up to 16
+  __host__ __device__ static constexpr int n_of(int cnt) {
+    return CO == 16 ? 48 * cnt : ((6 * cnt + 15) / 16) * 16;
+  }
+};
+static_assert(OutShape<2>::NB >= 9 * 2, "padded N holds the 18 real columns");
+// every MMA's D block (padded N included) stays inside the allocation
+static_assert((TYF - 1) * OSLOTS * 2 + 32 <= (int)F_TMEM_COLS, "padded blocks fit");
+constexpr int EPI_ROWS = TYF / 2;                // rows per epilogue warp
 // after the weights: 2*FSLOTS + 5 mbarriers, TMEM address, abort flag, 16 biases
 constexpr int F_TAIL_BYTES = 256;
 static_assert((2 * FSLOTS + 5) * 8 + 16 + 64 <= F_TAIL_BYTES, "tail fits");
@@ -296,17 +315,19 @@ __device__ __forceinline__ void conv_epilogue(const ConvParams& p, const float (
   }
 }
 
-template <int EPI>
-__global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_constant__ ConvParams p) {
+template <int EPI, int CO>
+__global__ void __launch_bounds__(F_THREADS, F_CTAS_PER_SM)
+conv_fwd_kernel(const __grid_constant__ ConvParams p) {
+  constexpr int CW = OutShape<CO>::CW, NB = OutShape<CO>::NB, WTB = OutShape<CO>::WTB;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* ring = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* wsm = ring + FSLOTS * p.slot_bytes + 4096;  // 4 KB of zeros after the ring
-  uint64_t* full = reinterpret_cast<uint64_t*>(wsm + W_TILES * WT_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(wsm + W_TILES * WTB);
   uint64_t* empty = full + FSLOTS;
-  uint64_t* accf = empty + FSLOTS;  // [2] MMAs of one input plane done (per epilogue group)
-  uint64_t* acce = accf + 2;        // [2] the finished output plane's slot is drained
-  uint64_t* drain = acce + 2;
+  uint64_t* accf = empty + FSLOTS;  // MMAs of one input plane done
+  uint64_t* acce = accf + 1;        // the finished output plane's slot is drained
+  uint64_t* drain = acce + 1;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
   float* bias_s = reinterpret_cast<float*>(tmem_holder + 4);  // [16], 16-byte aligned
@@ -315,7 +336,7 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
   {  // weights and the zero pad (generic proxy), then make them visible to the tensor core
     const uint4* src = reinterpret_cast<const uint4*>(p.w);
     uint4* dst = reinterpret_cast<uint4*>(wsm);
-    for (int i = threadIdx.x; i < W_TILES * WT_BYTES / 16; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < W_TILES * WTB / 16; i += blockDim.x) dst[i] = src[i];
     // the whole ring and the pad start at zero: rows a copy leaves
     // untouched (past the grid's last row) and over-reads stay finite
     uint4* z = reinterpret_cast<uint4*>(ring);
@@ -328,10 +349,8 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int g = 0; g < 2; g++) {
-      mbar_init(&accf[g], 1);
-      mbar_init(&acce[g], 32 * F_GROUP_WARPS);
-    }
+    mbar_init(accf, 1);
+    mbar_init(acce, 32 * F_EPI_WARPS);
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -344,9 +363,9 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
   const uint32_t tmem = *tmem_holder;
   const uint64_t lim = p.wait_limit_ns;
   const uint32_t row_bytes = (uint32_t)p.Xp * 16;
-  if (warp >= 2 && warp < 2 + F_GROUP_WARPS) {  // the accumulator ring starts at zero
+  if (warp >= 2) {  // the whole allocation starts at zero
     const int q = warp & 3, half = (warp - 2) >> 2;
-    for (int a = half; a < ACC_ROWS * OSLOTS; a += 2)
+    for (int a = half; a < (int)F_TMEM_COLS / 16; a += 2)
       tc::st_32x32b_x16_zero(tmem + ((uint32_t)(32 * q) << 16) + a * 16);
     tc::wait_st();
   }
@@ -386,10 +405,13 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = tc::idesc_bf16_f32(128, NSTACK, false, false);
+      constexpr int BROW = OSLOTS * CW;  // B rows / D columns per output row
+      const uint32_t idesc1 = tc::idesc_bf16_f32(128, OutShape<CO>::n_of(1), false, false);
+      const uint32_t idesc2 = tc::idesc_bf16_f32(128, OutShape<CO>::n_of(2), false, false);
+      const uint32_t idesc3 = tc::idesc_bf16_f32(128, OutShape<CO>::n_of(3), false, false);
       const uint32_t lbo_a = p.Hin == 2 ? row_bytes : 0;
       const uint32_t ring_s = smem_u32(ring), w_s = smem_u32(wsm);
-      const uint64_t bdesc0 = tc::smem_desc(w_s, NSTACK * 16, 128);
+      const uint64_t bdesc0 = tc::smem_desc(w_s, NB * 16, 128);
       const uint64_t adesc0 = tc::smem_desc(ring_s, lbo_a, 128);
       const uint32_t row_step = (uint32_t)p.Hin * row_bytes;
       uint32_t g = 0, e = 0;  // input planes, steps (one per input plane)
@@ -401,24 +423,31 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
         for (int t = 0; t < nout + 2 && !*abort_flag; t++, g++, e++) {
           const int j = z0 - 1 + t;  // input plane (may be -1: its ghost plane)
           bool ok = mbar_wait_bounded(&full[g % FSLOTS], (g / FSLOTS) & 1, lim);
-          if (ok && e > 0) ok = mbar_wait_bounded(&acce[(e - 1) & 1], ((e - 1) >> 1) & 1, lim);
+          if (ok && e > 0) ok = mbar_wait_bounded(acce, (e - 1) & 1, lim);
           if (!ok) {
             set_abort(p.status, abort_flag, 1);
             break;
           }
           tc::fence_after_sync();
           const uint64_t ab = adesc0 + ((g % FSLOTS) * p.slot_bytes >> 4);
-          const uint64_t bb = bdesc0 + (uint64_t)(((j + 3) % 3) * 3 * WT_BYTES / 16);
+          const uint64_t bb = bdesc0 + (uint64_t)(((j + 3) % 3) * 3 * WTB / 16);
 #pragma unroll
           for (int i = 0; i < TYF + 2; i++) {
+            // input row i feeds slab rows i-2 .. i: keep those inside [0, TYF)
+            const int jlo = i < 2 ? 2 - i : 0;
+            const int jhi = i > TYF - 1 ? TYF + 1 - i : 2;
+            const int cnt = jhi - jlo + 1;
+            const uint32_t idesc = cnt == 3 ? idesc3 : (cnt == 2 ? idesc2 : idesc1);
+            const uint32_t d = tmem + (uint32_t)((i - 2 + jlo) * BROW);
+            const uint64_t b = bb + (uint64_t)(jlo * BROW * 16 / 16);
             if (i < nin) {
 #pragma unroll
               for (int dx = 0; dx < 3; dx++)
-                tc::mma_bf16(tmem + i * (OSLOTS * CH), ab + ((i * row_step + dx * 16) >> 4),
-                             bb + (uint64_t)(dx * WT_BYTES / 16), idesc, 1u);
+                tc::mma_bf16(d, ab + ((i * row_step + dx * 16) >> 4), b + (uint64_t)(dx * WTB / 16),
+                             idesc, 1u);
             }
           }
-          tc::commit(smem_u32(&accf[e & 1]));
+          tc::commit(smem_u32(accf));
           tc::commit(smem_u32(&empty[g % FSLOTS]));
         }
       }
@@ -426,11 +455,7 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
       if (!mbar_wait_bounded(drain, 0, lim)) set_abort(p.status, abort_flag, 1);
     }
   } else {
-    // two groups of 8 warps take alternate planes (group = step parity), so
-    // a finished plane is drained while the other group still computes
-    const int ew = warp - 2;
-    const int grp = ew / F_GROUP_WARPS;
-    const int q = warp & 3, half = (ew % F_GROUP_WARPS) >> 2;
+    const int q = warp & 3, half = (warp - 2) >> 2;
     const int x = 32 * q + lane;
     const uint32_t tq = tmem + ((uint32_t)(32 * q) << 16);
     uint32_t e = 0;
@@ -441,8 +466,7 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
       const int nrows = min(TYF, p.ny - y0);
       bool stop = false;
       for (int t = 0; t < nout + 2; t++, e++) {
-        if ((int)(e & 1) != grp) continue;
-        if (!mbar_wait_bounded(&accf[grp], (e >> 1) & 1, lim)) {
+        if (!mbar_wait_bounded(accf, e & 1, lim)) {
           set_abort(p.status, abort_flag, 1);
           stop = true;
           break;
@@ -463,20 +487,25 @@ __global__ void __launch_bounds__(F_THREADS, 1) conv_fwd_kernel(const __grid_con
 #pragma unroll
           for (int k = 0; k < EPI_ROWS; k++) {
             const int r = half + 2 * k;
-            if (r < nrows) tc::ld_32x32b_x16(tq + ((r + 2) * OSLOTS + so) * 16, v[k]);
+            if (r < nrows) {
+              if (CW == 16) tc::ld_32x32b_x16(tq + (r * OSLOTS + so) * CW, v[k]);
+              else tc::ld_32x32b_x2(tq + (r * OSLOTS + so) * CW, v[k]);
+            }
           }
         }
         const bool last = t == nout + 1;
         for (int a = half; a < ACC_ROWS; a += 2) {
-          tc::st_32x32b_x16_zero(tq + (a * OSLOTS + so) * 16);
-          if (last) {  // junk of the planes past the chunk
-            tc::st_32x32b_x16_zero(tq + (a * OSLOTS + (so + 1) % 3) * 16);
-            tc::st_32x32b_x16_zero(tq + (a * OSLOTS + (so + 2) % 3) * 16);
+#pragma unroll
+          for (int ds = 0; ds < 3; ds++) {
+            if (ds > 0 && !last) break;  // at the chunk's end: junk of the planes past it
+            const uint32_t col = (a * OSLOTS + (so + ds) % 3) * CW;
+            if (CW == 16) tc::st_32x32b_x16_zero(tq + col);
+            else tc::st_32x32b_x2_zero(tq + col);
           }
         }
         tc::wait_st();
         tc::fence_before_sync();
-        mbar_arrive(&acce[grp]);
+        mbar_arrive(acce);
         if (mine) {
 #pragma unroll
           for (int k = 0; k < EPI_ROWS; k++) {
@@ -823,6 +852,25 @@ __global__ void pack_weights_kernel(const float* __restrict__ w, __nv_bfloat16* 
   const size_t base = (size_t)l * NTAP * 256;
   wf[i] = __float2bfloat16_rn(w[base + (size_t)tap * 256 + co * 16 + k]);
   wt[i] = __float2bfloat16_rn(w[base + (size_t)(NTAP - 1 - tap) * 256 + k * 16 + co]);
+}
+
+// The last layer (2 output channels) in the N = 32 layout of
+// conv_fwd_kernel<*, 2>: [rot][dx][2 halves][32 rows][8], row n = (jrow*3 + s)*2
+// + co for n < 18, zero rows above.
+__global__ void pack_out2_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf2) {
+  constexpr int NB = OutShape<2>::NB;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W_TILES * 2 * NB * 8) return;
+  const int c = i % 8, n = (i / 8) % NB, h = (i / (8 * NB)) % 2, tile = i / (16 * NB);
+  const int rot = tile / 3, dx = tile % 3;
+  float v = 0.0f;
+  if (n < 18) {
+    const int co = n % 2, sj = n / 2, s = sj % 3, jrow = sj / 3;
+    const int dz = 2 - (((s - rot + 1) % 3 + 3) % 3);
+    const int tap = dz * 9 + (2 - jrow) * 3 + dx;
+    v = w[(size_t)(NLAYER - 1) * NTAP * 256 + (size_t)tap * 256 + co * 16 + 8 * h + c];
+  }
+  wf2[i] = __float2bfloat16_rn(v);
 }
 
 // 2:1 restriction (2x2x2 average) of a solver field (2 ghosts) to a dense

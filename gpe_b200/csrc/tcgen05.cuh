@@ -94,6 +94,21 @@ __device__ __forceinline__ void ld_32x32b_x16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 2 columns: this thread's lane, columns 0-1 into v[0], v[1].
+__device__ __forceinline__ void ld_32x32b_x2(uint32_t taddr, float (&v)[16]) {
+  uint32_t r0, r1;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
+               : "=r"(r0), "=r"(r1) : "r"(taddr) : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  v[0] = __uint_as_float(r0);
+  v[1] = __uint_as_float(r1);
+}
+__device__ __forceinline__ void st_32x32b_x2_zero(uint32_t taddr) {
+  const uint32_t z = 0;
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%1};" ::"r"(taddr), "r"(z)
+               : "memory");
+}
+
 // Zero 32 lanes x 16 columns (this thread's lane).  Complete with wait_st.
 __device__ __forceinline__ void st_32x32b_x16_zero(uint32_t taddr) {
   const uint32_t z = 0;

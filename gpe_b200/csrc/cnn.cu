@@ -178,7 +178,7 @@ int check_view(gpe_cnn* n, const FieldView& v) {
 }
 
 int pack_input(gpe_cnn* n, const FieldView& v, const Act& dst) {
-  pack_input_kernel<float><<<n->ew_blocks, 256, 0, v.stream>>>(
+  pack_input_kernel<float><<<n->Zp * n->Yp, 128, 0, v.stream>>>(
       static_cast<const float*>(v.psi), v.Nx, v.Ny, n->nx, n->ny, n->nz, dst.p, dst.H);
   CNN_CU(n, cudaGetLastError());
   n->launches++;

@@ -712,25 +712,27 @@ __global__ void __launch_bounds__(W_THREADS, 1) conv_wgrad_kernel(const __grid_c
 // Element-wise and reduction kernels.
 
 // Solver field (2 ghosts, pitches Nx, Ny; complex of TS) -> first-layer input
-// (channels Re, Im, 0, ...; H halves), ghosts included.
+// (channels Re, Im, 0, ...; H halves), ghosts included.  Every padded site
+// reads its periodic interior source (the solver keeps only the face ghosts
+// a star stencil needs, not edges and corners): one block per padded (y, z)
+// row, consecutive threads along x.
 template <typename TS>
 __global__ void pack_input_kernel(const TS* __restrict__ psi, int Nx, int Ny, int nx, int ny,
                                   int nz, __nv_bfloat16* __restrict__ act, int H) {
   const int Xp = nx + 2, Yp = ny + 2;
-  const size_t n = (size_t)nx * ny * nz;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-       s += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(s % nx);
-    const size_t t = s / nx;
-    const int y = (int)(t % ny), z = (int)(t / ny);
-    const size_t q = ((size_t)(z + 2) * Ny + (y + 2)) * Nx + (x + 2);
-    uint4 lo = make_uint4(pack_bf16x2((float)psi[2 * q], (float)psi[2 * q + 1]), 0, 0, 0);
-    const uint4 zero = make_uint4(0, 0, 0, 0);
-    for_images(x, y, z, nx, ny, nz, [&](int xp, int yp, int zp) {
-      const size_t b = (((size_t)zp * Yp + yp) * H * Xp) * 8;
-      *reinterpret_cast<uint4*>(act + b + (size_t)xp * 8) = lo;
-      if (H == 2) *reinterpret_cast<uint4*>(act + b + ((size_t)Xp + xp) * 8) = zero;
-    });
+  const int row = blockIdx.x;  // zp * Yp + yp
+  const int yp = row % Yp, zp = row / Yp;
+  const int y = yp == 0 ? ny - 1 : (yp == ny + 1 ? 0 : yp - 1);
+  const int z = zp == 0 ? nz - 1 : (zp == nz + 1 ? 0 : zp - 1);
+  const size_t q0 = ((size_t)(z + 2) * Ny + (y + 2)) * Nx + 2;
+  __nv_bfloat16* dst = act + (size_t)row * H * Xp * 8;
+  const uint4 zero = make_uint4(0, 0, 0, 0);
+  for (int xp = threadIdx.x; xp < Xp; xp += blockDim.x) {
+    const int x = xp == 0 ? nx - 1 : (xp == nx + 1 ? 0 : xp - 1);
+    const size_t q = q0 + x;
+    *reinterpret_cast<uint4*>(dst + (size_t)xp * 8) =
+        make_uint4(pack_bf16x2((float)psi[2 * q], (float)psi[2 * q + 1]), 0, 0, 0);
+    if (H == 2) *reinterpret_cast<uint4*>(dst + ((size_t)Xp + xp) * 8) = zero;
   }
 }
 

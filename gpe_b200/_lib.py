@@ -93,6 +93,7 @@ SIGNATURES = {
     "gpe_gpu_advance": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(GpeTimeC), _dp]),
     "gpe_gpu_norm": (ctypes.c_int, [_vp, _dp]),
     "gpe_gpu_energy": (ctypes.c_int, [_vp, _dp, _dp]),
+    "gpe_gpu_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
     "gpe_gpu_renormalise": (ctypes.c_int, [_vp, ctypes.c_double]),
     "gpe_gpu_rhs": (ctypes.c_int, [_vp, _vp, _i32]),
     "gpe_gpu_laplacian": (ctypes.c_int, [_vp, _vp, _i32]),

@@ -167,4 +167,75 @@ __global__ void batch_finalize_kernel(const double* __restrict__ partials,
 
 __global__ void bump_counter_kernel(int* counter) { *counter = *counter + 1; }
 
+// mass (src/variables.f90:590-610) and momentum (:615-694) in one pass:
+// per block, [4] partials = { sum |psi|^2, and for d = x, y, z the weighted
+// sum of (Re psi - 1) Im(d conj psi) - Im psi Re(d psi) }.  First
+// derivatives use the face ghosts: c1 (f+1 - f-1) + c2 (f+2 - f-2).
+template <typename TS>
+__global__ void diag_kernel(const TS* __restrict__ f, Geom g, double c1x, double c2x,
+                            double c1y, double c2y, double c1z, double c2z,
+                            const double* __restrict__ wx, const double* __restrict__ wy,
+                            const double* __restrict__ wz, double* __restrict__ partials) {
+  __shared__ double red[4][32];
+  const size_t n = (size_t)g.nx * g.ny * g.nz;
+  const size_t sx = 1, sy = (size_t)g.Nx, sz = (size_t)g.Nx * g.Ny;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const size_t r = q / g.nx;
+    const int j = (int)(r % g.ny);
+    const int k = (int)(r / g.ny);
+    const size_t pi = padded_index(g, i, j, k);
+    const double re = (double)f[2 * pi], im = (double)f[2 * pi + 1];
+    acc[0] += re * re + im * im;
+    const size_t st[3] = {sx, sy, sz};
+    const double c1[3] = {c1x, c1y, c1z}, c2[3] = {c2x, c2y, c2z};
+    const double w = (wx[i] * wy[j]) * wz[k];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const size_t p1 = pi + st[a], m1 = pi - st[a], p2 = pi + 2 * st[a], m2 = pi - 2 * st[a];
+      double dr = c1[a] * ((double)f[2 * p1] - (double)f[2 * m1]);
+      double di = c1[a] * ((double)f[2 * p1 + 1] - (double)f[2 * m1 + 1]);
+      if (c2[a] != 0.0) {
+        dr += c2[a] * ((double)f[2 * p2] - (double)f[2 * m2]);
+        di += c2[a] * ((double)f[2 * p2 + 1] - (double)f[2 * m2 + 1]);
+      }
+      // Im(d conj psi) = -Im(d psi)
+      acc[1 + a] += w * (-(re - 1.0) * di - im * dr);
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const double t = warp_sum(acc[v]);
+    if ((threadIdx.x & 31) == 0) red[v][threadIdx.x >> 5] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[threadIdx.x][w];
+    partials[4 * (size_t)blockIdx.x + threadIdx.x] = t;
+  }
+}
+
+// [nblk][4] partials -> out[0..3] * scale, fixed order (one CTA of 256).
+__global__ void diag_finalize_kernel(const double* __restrict__ partials, int nblk, double scale,
+                                     double* __restrict__ out) {
+  __shared__ double s[4][256];
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+    for (int v = 0; v < 4; v++) a[v] += partials[4 * (size_t)b + v];
+#pragma unroll
+  for (int v = 0; v < 4; v++) s[v][threadIdx.x] = a[v];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+#pragma unroll
+      for (int v = 0; v < 4; v++) s[v][threadIdx.x] += s[v][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0] * scale;
+}
+
 }  // namespace gpe

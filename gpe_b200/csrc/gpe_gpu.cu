@@ -1686,6 +1686,43 @@ int gpe_gpu_norm(gpe_ctx* c, double* norm) {
   return GPE_OK;
 }
 
+int gpe_gpu_diagnostics(gpe_ctx* c, double* mass, double* mom) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!mass || !mom) return fail(c, GPE_ERR_INVALID, "null output");
+  const Geom g = geom(c);
+  const int nb = (int)std::min<size_t>((size_t)elementwise_blocks(c->nint), c->partials_cap / 2);
+  double c1[3], c2[3];
+  const double h[3] = {c->dx, c->dy, c->dz};
+  for (int a = 0; a < 3; a++) {
+    if (c->prm.order == 2) { c1[a] = 1.0 / (2.0 * h[a]); c2[a] = 0.0; }
+    else { c1[a] = 8.0 / (12.0 * h[a]); c2[a] = -1.0 / (12.0 * h[a]); }
+  }
+  if (c->es == 8)
+    diag_kernel<float><<<nb, 256, 0, c->stream>>>((const float*)c->fld[c->psi_id], g, c1[0], c2[0],
+                                                  c1[1], c2[1], c1[2], c2[2], c->tabW[0],
+                                                  c->tabW[1], c->tabW[2], c->d_partials);
+  else
+    diag_kernel<double><<<nb, 256, 0, c->stream>>>((const double*)c->fld[c->psi_id], g, c1[0],
+                                                   c2[0], c1[1], c2[1], c1[2], c2[2], c->tabW[0],
+                                                   c->tabW[1], c->tabW[2], c->d_partials);
+  CU_CHECK(c, cudaGetLastError());
+  diag_finalize_kernel<<<1, 256, 0, c->stream>>>(c->d_partials, nb, cell_volume(c), c->d_scal + 4);
+  CU_CHECK(c, cudaGetLastError());
+  c->launches += 2;
+  rc = allreduce_scalars(c, 4, 4, 0);
+  if (rc) return rc;
+  double v[4];
+  rc = read_scalars(c, v, 4, 4);
+  if (rc) return rc;
+  *mass = v[0];
+  mom[0] = v[1];
+  mom[1] = v[2];
+  mom[2] = v[3];
+  if (!std::isfinite(v[0])) return fail(c, GPE_ERR_NAN, "non-finite mass");
+  return GPE_OK;
+}
+
 int gpe_gpu_energy(gpe_ctx* c, double* E, double* H4) {
   int rc = check_ctx(c);
   if (rc) return rc;

@@ -202,6 +202,33 @@ class GpeSolver:
         check(lib().gpe_gpu_energy(self._ctx, ctypes.byref(e), ctypes.byref(h)), self._ctx)
         return e.value, h.value
 
+    def save_end_state(self, path: str) -> None:
+        """Checkpoint in the reference's end_state.dat format (src/io.f90:840-862)."""
+        from .restart import write_end_state
+        pr = 8 if self.prm.precision == 16 else 4
+        write_end_state(path, self.get_state(np.complex128 if pr == 8 else np.complex64),
+                        self.p, self.t, self.im_t, self.dt, pr)
+
+    def load_end_state(self, path: str) -> None:
+        """Restart from an end_state.dat file (src/ic.f90:117-186)."""
+        from .restart import read_end_state, restart_time_state
+        pr = 8 if self.prm.precision == 16 else 4
+        st = read_end_state(path, pr, expect=(self.prm.nx, self.prm.ny, self.prm.nz))
+        sch = self.prm.scheme if isinstance(self.prm.scheme, str) else \
+            {v: k for k, v in SCHEMES.items()}.get(self.prm.scheme, "rk4")
+        self.p, self.t, self.im_t, self.dt = restart_time_state(st, bool(self.prm.real_time), sch,
+                                                               self.dt)
+        self.set_state(st.psi)
+
+    def diagnostics(self) -> tuple[float, np.ndarray]:
+        """mass and momentum (src/variables.f90:590-694) -> (M, (Px, Py, Pz))."""
+        m = ctypes.c_double()
+        mom = np.zeros(3)
+        check(lib().gpe_gpu_diagnostics(self._ctx, ctypes.byref(m),
+                                        mom.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              self._ctx)
+        return m.value, mom
+
     def renormalise(self, norm: float) -> None:
         """renormalise (src/variables.f90:698-709)."""
         check(lib().gpe_gpu_renormalise(self._ctx, float(norm)), self._ctx)

@@ -181,6 +181,11 @@ int gpe_gpu_norm(gpe_ctx* ctx, double* norm);
  * sum [0.5 Re(-lap psi conj psi) + V|psi|^2 + 0.5 g|psi|^4 - mu|psi|^2]
  * dx dy dz, which that equation conserves (no reference counterpart). */
 int gpe_gpu_energy(gpe_ctx* ctx, double* E, double* H4);
+/* mass (src/variables.f90:590-610: plain sum of |psi|^2 dx dy dz) and
+ * momentum (:615-694: per axis the extended-Simpson integral of
+ * (Re psi - 1) Im(d conj psi) - Im psi Re(d psi)) of the resident state, in
+ * one device pass with FP64 sums; mom has 3 entries. */
+int gpe_gpu_diagnostics(gpe_ctx* ctx, double* mass, double* mom);
 
 /* renormalise (src/variables.f90:698-709): psi = sqrt(nn) psi / sqrt(norm). */
 int gpe_gpu_renormalise(gpe_ctx* ctx, double norm);

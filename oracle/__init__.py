@@ -83,6 +83,10 @@ def lib():
         L.ora_energy.argtypes = [vp, dp]
         L.ora_hamiltonian4.restype = ctypes.c_double
         L.ora_hamiltonian4.argtypes = [vp, dp]
+        L.ora_mass.restype = ctypes.c_double
+        L.ora_mass.argtypes = [vp, dp]
+        L.ora_momentum.restype = None
+        L.ora_momentum.argtypes = [vp, dp, dp]
         L.ora_renormalise.argtypes = [vp, dp, ctypes.c_double]
         L.ora_get_rr.restype = ctypes.c_double
         L.ora_get_rr.argtypes = [ctypes.c_double]
@@ -188,6 +192,15 @@ class Oracle:
     def deriv(self, psi, axis: int, second: bool):
         a = _c128(psi); out = np.empty_like(a)
         lib().ora_deriv(self._h, axis, 1 if second else 0, _dp(a), _dp(out)); return out
+
+    def mass(self, psi) -> float:
+        a = _c128(psi); return float(lib().ora_mass(self._h, _dp(a)))
+
+    def momentum(self, psi):
+        a = _c128(psi)
+        out = np.zeros(3)
+        lib().ora_momentum(self._h, _dp(a), _dp(out))
+        return out
 
     def get_norm(self, psi) -> float:
         a = _c128(psi); return float(lib().ora_get_norm(self._h, _dp(a)))

@@ -757,6 +757,73 @@ double ora_get_norm(ora_ctx* c, const double* psi_) {
   return s * c->dz;
 }
 
+/* integrate_x / integrate_y / integrate_z (src/variables.f90:713-823) of a
+ * real interior field: the extended-Simpson rule as get_norm applies it. */
+static double integrate_xyz(ora_ctx* c, const double* f) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  double* int_x = (double*)xcalloc((size_t)ny * nz, sizeof(double));
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++) {
+      const double* r = &f[IX(c, 0, j, k)];
+      double s = 0.0;
+      for (int i = 3; i <= nx - 4; i++) s += r[i];
+      int_x[(size_t)k * ny + j] = (W1 * r[0] + W2 * r[1] + W3 * r[2] + s + W3 * r[nx - 3] +
+                                   W2 * r[nx - 2] + W1 * r[nx - 1]) * c->dx;
+    }
+  double tot = 0.0;
+  for (int k = 0; k < nz; k++) {
+    double sy = 0.0;
+    for (int j = 0; j < ny; j++) {
+      double v = int_x[(size_t)k * ny + j], tv = v;
+      if (j == 0) tv = W1 * v;
+      if (j == 1) tv = W2 * v;
+      if (j == 2) tv = W3 * v;
+      if (j == ny - 3) tv = W3 * v;
+      if (j == ny - 2) tv = W2 * v;
+      if (j == ny - 1) tv = W1 * v;
+      sy += tv;
+    }
+    double v = sy * c->dy, tv = v;
+    if (k == 0) tv = W1 * v;
+    if (k == 1) tv = W2 * v;
+    if (k == 2) tv = W3 * v;
+    if (k == nz - 3) tv = W3 * v;
+    if (k == nz - 2) tv = W2 * v;
+    if (k == nz - 1) tv = W1 * v;
+    tot += tv;
+  }
+  free(int_x);
+  return tot * c->dz;
+}
+
+/* mass (src/variables.f90:590-610): plain sum of |psi|^2 times dx dy dz. */
+double ora_mass(ora_ctx* c, const double* psi_) {
+  const cplx* psi = (const cplx*)psi_;
+  const size_t n = (size_t)c->nx * c->ny * c->nz;
+  double s = 0.0;
+  for (size_t q = 0; q < n; q++) s += creal(psi[q]) * creal(psi[q]) + cimag(psi[q]) * cimag(psi[q]);
+  return s * c->dx * c->dy * c->dz;
+}
+
+/* momentum (src/variables.f90:615-694): for each axis d,
+ * integral of (Re psi - 1) Im(d conj(psi)) - Im psi Re(d psi). */
+void ora_momentum(ora_ctx* c, const double* psi_, double mom[3]) {
+  const cplx* psi = (const cplx*)psi_;
+  const size_t n = (size_t)c->nx * c->ny * c->nz;
+  cplx* d = (cplx*)xcalloc(n, sizeof(cplx));
+  double* f = (double*)xcalloc(n, sizeof(double));
+  for (int a = 0; a < 3; a++) {
+    ora_deriv(c, a, 0, psi_, (double*)d);
+    for (size_t q = 0; q < n; q++) {
+      const cplx dstar = conj(d[q]); /* deriv of conj(psi): the stencil is real */
+      f[q] = (creal(psi[q]) - 1.0) * cimag(dstar) - cimag(psi[q]) * creal(d[q]);
+    }
+    mom[a] = integrate_xyz(c, f);
+  }
+  free(d);
+  free(f);
+}
+
 double ora_energy(ora_ctx* c, const double* psi_) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
   to_haloed(c, (const cplx*)psi_, c->in_h);

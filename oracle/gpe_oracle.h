@@ -85,6 +85,9 @@ double ora_energy(ora_ctx* c, const double* psi);
  * drift): sum[ 0.5 Re(-lap psi . conj psi) + V|psi|^2 + 0.5 g|psi|^4
  * - mu|psi|^2 ] dx dy dz. */
 double ora_hamiltonian4(ora_ctx* c, const double* psi);
+/* mass (src/variables.f90:590-610) and momentum (:615-694). */
+double ora_mass(ora_ctx* c, const double* psi);
+void ora_momentum(ora_ctx* c, const double* psi, double mom[3]);
 /* renormalise (src/variables.f90:698-709): psi = sqrt(nn)*psi/sqrt(norm). */
 void ora_renormalise(ora_ctx* c, double* psi, double norm);
 

@@ -314,3 +314,40 @@ def test_c2_rkf45_configuration_matches_oracle():
         assert g.t == pytest.approx(tm.t, rel=1e-8)
     assert rel_l2(g.get_state(), q) < 1e-9
     g.close()
+
+
+@pytest.mark.parametrize("order,bcs,precision", [(2, 1, 16), (4, 1, 16), (4, 2, 16), (2, 2, 8)])
+def test_mass_and_momentum_match_oracle(order, bcs, precision):
+    n = (70, 13, 11)
+    g, o = pair(n, (8.0, 4.0, 3.5), "rk4", 4, bcs, order, True, precision=precision)
+    psi = random_field((n[2], n[1], n[0]), seed=order * 10 + bcs)
+    if precision == 8:
+        psi = psi.astype(np.complex64).astype(np.complex128)
+    g.set_state(psi)
+    m, mom = g.diagnostics()
+    tol = 1e-12 if precision == 16 else 1e-6
+    assert m == pytest.approx(o.mass(psi), rel=tol)
+    np.testing.assert_allclose(mom, o.momentum(psi), rtol=tol, atol=tol * np.abs(mom).max())
+    g.close()
+
+
+def test_checkpoint_round_trip_through_the_solver(tmp_path):
+    n = (40, 12, 10)
+    g, o = pair(n, (8.0, 4.0, 3.5), "rk4", 4, 1, 4, True)
+    psi = random_field((n[2], n[1], n[0]), seed=5)
+    g.dt = 0.01
+    g.set_state(psi)
+    g.advance(3)
+    g.p = 3
+    f = str(tmp_path / "end_state.dat")
+    g.save_end_state(f)
+    g.advance(2)
+    ref = g.get_state()
+    h, _ = pair(n, (8.0, 4.0, 3.5), "rk4", 4, 1, 4, True)
+    h.dt = 0.01
+    h.load_end_state(f)
+    assert (h.p, h.t) == (3, pytest.approx(0.03))
+    h.advance(2)
+    assert np.array_equal(h.get_state(), ref)
+    g.close()
+    h.close()

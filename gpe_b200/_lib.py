@@ -94,6 +94,7 @@ SIGNATURES = {
     "gpe_gpu_norm": (ctypes.c_int, [_vp, _dp]),
     "gpe_gpu_energy": (ctypes.c_int, [_vp, _dp, _dp]),
     "gpe_gpu_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
+    "gpe_gpu_wait_probe": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "gpe_gpu_renormalise": (ctypes.c_int, [_vp, ctypes.c_double]),
     "gpe_gpu_rhs": (ctypes.c_int, [_vp, _vp, _i32]),
     "gpe_gpu_laplacian": (ctypes.c_int, [_vp, _vp, _i32]),

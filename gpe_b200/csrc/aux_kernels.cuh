@@ -167,6 +167,19 @@ __global__ void batch_finalize_kernel(const double* __restrict__ partials,
 
 __global__ void bump_counter_kernel(int* counter) { *counter = *counter + 1; }
 
+// Failure-detection probe: waits, bounded by limit_ns, on an mbarrier phase
+// that nothing completes, then records the timeout in *status exactly as
+// the stage kernels do.
+__global__ void wait_probe_kernel(unsigned long long limit_ns, int* status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0, limit_ns)) atomicExch(status, 1);
+}
+
 // mass (src/variables.f90:590-610) and momentum (:615-694) in one pass:
 // per block, [4] partials = { sum |psi|^2, and for d = x, y, z the weighted
 // sum of (Re psi - 1) Im(d conj psi) - Im psi Re(d psi) }.  First

@@ -1686,6 +1686,18 @@ int gpe_gpu_norm(gpe_ctx* c, double* norm) {
   return GPE_OK;
 }
 
+int gpe_gpu_wait_probe(gpe_ctx* c, uint64_t limit_ns) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (limit_ns == 0 || limit_ns > 1000000000ull)
+    return fail(c, GPE_ERR_INVALID, "wait probe limit must be in (0, 1 s]");
+  wait_probe_kernel<<<1, 32, 0, c->stream>>>(limit_ns, c->d_status);
+  CU_CHECK(c, cudaGetLastError());
+  c->launches++;
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
 int gpe_gpu_diagnostics(gpe_ctx* c, double* mass, double* mom) {
   int rc = check_ctx(c);
   if (rc) return rc;

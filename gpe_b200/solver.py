@@ -220,6 +220,10 @@ class GpeSolver:
                                                                self.dt)
         self.set_state(st.psi)
 
+    def wait_probe(self, limit_ns: int) -> None:
+        """Failure-detection self-test: raises GpeError(GPE_ERR_TIMEOUT)."""
+        check(lib().gpe_gpu_wait_probe(self._ctx, int(limit_ns)), self._ctx)
+
     def diagnostics(self) -> tuple[float, np.ndarray]:
         """mass and momentum (src/variables.f90:590-694) -> (M, (Px, Py, Pz))."""
         m = ctypes.c_double()
@@ -279,11 +283,17 @@ class GpeSolver:
 
 
 def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool = False,
-             record=None):
+             record=None, run_dir: str | None = None):
     """The per-step bookkeeping of the reference time loop (src/gpe.f90:134-278)
     with an explicit step count: solver, get_norm + relnorm (equation 4),
     imaginary-to-real switch at relnorm < 1e-12 (:251-268), renormalise.
+    With run_dir, the loop also keeps the reference's cooperative controls:
+    it stops, writing run_dir/end_state.dat, when the file RUNNING is absent
+    before a step (:136-159), and when a file SAVE appears after a step it
+    writes a snapshot run_dir/snapshot_<p>.dat in the same format and
+    deletes SAVE (the reference writes an IDL surface there, src/io.f90:1566).
     Returns the list of (t, im_t, norm, relnorm) after each step."""
+    import os
     prm = s.prm
     out = [] if record is None else record
     prev_norm = 1.0
@@ -293,7 +303,13 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
             s.renormalise(prev_norm)
     norm = 0.0
     for _ in range(nsteps):
+        if run_dir is not None and not os.path.exists(os.path.join(run_dir, "RUNNING")):
+            s.save_end_state(os.path.join(run_dir, "end_state.dat"))
+            break
         s.solver()
+        if run_dir is not None and os.path.exists(os.path.join(run_dir, "SAVE")):
+            s.save_end_state(os.path.join(run_dir, "snapshot_%07d.dat" % (s.p + 1)))
+            os.remove(os.path.join(run_dir, "SAVE"))
         relnorm = 0.0
         if prm.eqn_to_solve == 4:
             norm = s.get_norm()

@@ -187,6 +187,13 @@ int gpe_gpu_energy(gpe_ctx* ctx, double* E, double* H4);
  * one device pass with FP64 sums; mom has 3 entries. */
 int gpe_gpu_diagnostics(gpe_ctx* ctx, double* mass, double* mom);
 
+/* Failure-detection self-test (no reference counterpart): runs, on the
+ * context's stream, a device wait on a flag that nothing sets, bounded by
+ * limit_ns (at most 1 s) with the same bounded-wait code as the stage
+ * kernels; returns GPE_ERR_TIMEOUT read back from the device status word,
+ * after which the context is still usable. */
+int gpe_gpu_wait_probe(gpe_ctx* ctx, uint64_t limit_ns);
+
 /* renormalise (src/variables.f90:698-709): psi = sqrt(nn) psi / sqrt(norm). */
 int gpe_gpu_renormalise(gpe_ctx* ctx, double norm);
 

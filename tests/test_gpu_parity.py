@@ -351,3 +351,38 @@ def test_checkpoint_round_trip_through_the_solver(tmp_path):
     assert np.array_equal(h.get_state(), ref)
     g.close()
     h.close()
+
+
+def test_device_wait_timeout_is_reported_and_the_context_survives():
+    """A device wait on a flag nothing sets runs out after 20 ms, the status
+    reaches the host as GPE_ERR_TIMEOUT, and the same context then steps
+    exactly as before."""
+    from gpe_b200 import GpeError
+    n = (24, 10, 8)
+    g, o = pair(n, (6.0, 3.0, 2.5), "rk4", 4, 1, 2, True)
+    psi = random_field((n[2], n[1], n[0]), seed=3)
+    g.dt = 0.01
+    g.set_state(psi)
+    with pytest.raises(GpeError) as e:
+        g.wait_probe(20_000_000)
+    assert e.value.code == 6
+    g.solver()
+    tm = oracle.OraTime(0.0, 0.0, 0.01, 0.0, 0)
+    exp, _, _ = o.solver(psi, tm)
+    assert rel_l2(g.get_state(), exp) < 1e-12
+    g.close()
+
+
+def test_non_finite_state_is_reported():
+    from gpe_b200 import GpeError
+    n = (24, 10, 8)
+    g, _ = pair(n, (6.0, 3.0, 2.5), "rk4", 4, 1, 2, True)
+    psi = random_field((n[2], n[1], n[0]), seed=4)
+    psi[3, 4, 5] = np.nan
+    g.dt = 0.01
+    g.set_state(psi)
+    g.solver()
+    with pytest.raises(GpeError) as e:
+        g.get_norm()
+    assert e.value.code == 5
+    g.close()

@@ -153,6 +153,17 @@ __device__ __forceinline__ float gelu(float x) {
   const float hx = 0.5f * x;
   return fmaf(hx, t, hx);
 }
+// Two values at once on the packed FP32x2 pipe: u = x (C + C A x^2),
+// gelu = h + h t with h = x / 2, t = tanh(u) (two scalar MUFU operations).
+__device__ __forceinline__ float2 gelu2(float2 x) {
+  const float2 x2 = __fmul2_rn(x, x);
+  const float2 k = __ffma2_rn(make_float2(GELU_C * GELU_A, GELU_C * GELU_A), x2,
+                              make_float2(GELU_C, GELU_C));
+  const float2 u = __fmul2_rn(x, k);
+  const float2 t = make_float2(tanh_approx(u.x), tanh_approx(u.y));
+  const float2 h = __fmul2_rn(x, make_float2(0.5f, 0.5f));
+  return __ffma2_rn(h, t, h);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
   const float t = tanh_approx(GELU_C * fmaf(GELU_A * x, x * x, x));
   const float du = GELU_C * fmaf(3.0f * GELU_A * x, x, 1.0f);
@@ -269,9 +280,13 @@ __device__ __forceinline__ void conv_epilogue(const ConvParams& p, const float (
   if (EPI == EPI_GELU || EPI == EPI_GELU_PRE) {
     float pre[16], a[16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) {
-      pre[c] = acc[c] + bias[c];
-      a[c] = gelu(pre[c]);
+    for (int c = 0; c < 16; c += 2) {
+      const float2 v = __fadd2_rn(make_float2(acc[c], acc[c + 1]), make_float2(bias[c], bias[c + 1]));
+      const float2 g = gelu2(v);
+      pre[c] = v.x;
+      pre[c + 1] = v.y;
+      a[c] = g.x;
+      a[c + 1] = g.y;
     }
     if (EPI == EPI_GELU_PRE) store_act16(p.pre_out, p.Xp, p.Yp, p.nx, p.ny, p.nz, x, y, z, pre, false);
     store_act16(p.act_out, p.Xp, p.Yp, p.nx, p.ny, p.nz, x, y, z, a, true);

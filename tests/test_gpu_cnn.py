@@ -2,9 +2,10 @@
 numpy oracle (oracle/cnn_ref.py) in its bfloat16-emulating mode.
 
 Tolerances: the oracle rounds to bfloat16 where the kernels store bfloat16
-and accumulates in FP64 where the tensor cores accumulate in FP32, so the
-two differ by FP32 accumulation order plus the rare bfloat16 rounding flip it
-causes: delta relative L2 <= 2e-3; loss relative 1e-4 (the loss moves by
+and accumulates in FP64 where the tensor cores accumulate in FP32; the
+kernels evaluate GELU's tanh with tanh.approx (relative error about 2^-11),
+the oracle exactly.  The two differ by those plus the bfloat16 rounding
+flips they cause: delta relative L2 <= 3e-3; loss relative 1e-4 (the loss moves by
 2 |e| |d delta| per site, e the residual, so delta's 1e-3-level differences
 reach it at the 1e-5 level); per-layer weight and
 bias gradients relative L2 <= 2e-2 (gradients pass through three more
@@ -51,7 +52,7 @@ def test_delta_matches_oracle(n):
         net.set_weights(w, b)
         d = net.delta(s).cpu().numpy().astype(np.float64)
     exp, _ = R.forward(psi.astype(np.complex128), w, b, 0.05, emulate=True)
-    assert rel_l2(d[..., 0] + 1j * d[..., 1], exp[..., 0] + 1j * exp[..., 1]) < 2e-3
+    assert rel_l2(d[..., 0] + 1j * d[..., 1], exp[..., 0] + 1j * exp[..., 1]) < 3e-3
     assert np.abs(d).max() > 1e-3  # the check is not vacuous
     s.close()
     del torch
@@ -69,7 +70,7 @@ def test_apply_adds_delta_and_keeps_ghosts(n):
     got = s.get_state(np.complex64).astype(np.complex128)
     exp, _ = R.forward(psi.astype(np.complex128), w, b, 0.05, emulate=True)
     dexp = exp[..., 0] + 1j * exp[..., 1]
-    assert rel_l2(got - psi, dexp) < 2e-3
+    assert rel_l2(got - psi, dexp) < 3e-3
     # the ghost images were updated with the interior: the library's
     # Laplacian of the corrected field equals that of the host copy
     lap = s.laplacian(np.complex128)

@@ -10,6 +10,7 @@ Metric: site-updates/s (sites x steps / device time), whole job.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
   python bench.py --workload ensemble [--steps 500]
+  python bench.py --workload spectrum [--grid 512] [--steps 20]
 
 --workload ensemble: 64 independent complex64 runs, cubic grids drawn from
 {32,48,64,96,128}^3 with seed 0, h = 0.5, harmonic trap omega ~ U[0.05, 0.15],
@@ -530,6 +531,127 @@ def run_rkf45(args):
     return 0
 
 
+def spectrum_cpu_sample(n: int = 128, min_seconds: float = 10.0, max_calls: int = 20):
+    """Times the vectorised oracle (numpy, one thread: pocketfft backward
+    transform, condensate row, spectrum) on an n^3 random-phase state;
+    returns (sites/s, calls, seconds)."""
+    import numpy as np
+
+    from oracle import spectral_ref as ref
+    xr = 0.5 * (n - 1)
+    ph = ref.splitmix_phases(0, n ** 3).reshape(n, n, n)
+    psi = ref.random_phase_fast(n, n, n, 0.75, 0.75, ph)
+    calls = 0
+    t0 = time.perf_counter()
+    while True:
+        _, a = ref.condensed_fast(psi, xr, xr, xr)
+        ref.spectrum_fast(a)
+        calls += 1
+        el = time.perf_counter() - t0
+        if (el >= min_seconds and calls >= 2) or calls >= max_calls:
+            break
+    return n ** 3 * calls / el, calls, el
+
+
+def run_spectrum(args):
+    """condensed_particles + spectrum of a resident 512^3 complex128 state
+    (the reference's random_phase example parameters nv = enerv = 0.75 on a
+    512^3 grid): one call = pack psi, backward cuFFT Z2Z, the spectrum
+    reduction pass and its finaliser.  Metric: sites/s."""
+    import numpy as np
+    import torch
+
+    from gpe_b200 import GpeParams, GpeSolver, lib
+    from gpe_b200._lib import check
+    torch.cuda.set_device(0)
+    n = args.grid
+    xr = 0.5 * (n - 1)
+    prm = GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
+                    order=2, precision=16, g=1.0, mu=1.0)
+    s = GpeSolver(prm, dt=0.01)
+    amp, kc2 = s.random_phase(0.75, 0.75, 0)
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    for _ in range(args.warmup):
+        c = s.condensed_particles()
+    props = torch.cuda.get_device_properties(0)
+    uuid = str(getattr(props, "uuid", "") or "")
+    sampler = ClockSampler(uuid[-12:] if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+    s.set_timing(True)
+    s.timing()
+    lc0 = s.launch_count()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        c = s.condensed_particles()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.launch_count() - lc0
+    fam = s.timing()
+    s.set_timing(False)
+    clocks = sampler.stop()
+    sites = n ** 3
+    value = sites * args.steps / (ms / 1e3)
+    peak, peak_kind = load_peaks()
+    d = fam["spectrum"]
+    per_launch_ms = d["ms"] / max(d["launches"], 1)
+    alg_bytes = 16 * sites  # one read of the transformed complex128 field
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    traffic = load_traffic().get("spectrum_kernel")
+    roofline = {"bound": "hbm", "kernel": "spectrum_kernel<double>", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "per_launch_ms": per_launch_ms, "families": fam}
+
+    # end to end: pinned host state in, condensed_particles, row + spectra out
+    nb = sites * 16
+    L = lib()
+    hin = L.gpe_gpu_host_alloc(nb)
+    a_in = np.ctypeslib.as_array(ctypes.cast(hin, ctypes.POINTER(ctypes.c_double)), (2 * sites,))
+    a_in[:] = s.get_state().view(np.float64).ravel()
+    ke = max(1, args.e2e_steps)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ke):
+        check(L.gpe_gpu_set_state(s.handle, ctypes.c_void_p(hin), 16), s.handle)
+        s.condensed_particles()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / ke
+    L.gpe_gpu_host_free(ctypes.c_void_p(hin))
+    e2e = {"value": sites / (e2e_ms / 1e3), "unit": "sites/s", "h2d_bytes_per_step": nb,
+           "d2h_bytes_per_step": 8 * (21 + n // 2), "ms_per_step": e2e_ms,
+           "form": "gpe_gpu_set_state (pinned host psi) + gpe_gpu_condensed_particles "
+                   "(row, eta, nharm, F to host), per call"}
+    s.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        v, calls, el = spectrum_cpu_sample()
+        cpu = {"value": v, "unit": "sites/s", "cores": 1, "kind": "port",
+               "sample": f"{calls} calls on a 128^3 random-phase state (vectorised numpy oracle: "
+                         f"backward FFT, condensate row, spectrum), 1 thread, {el:.1f} s"}
+    line = {
+        "metric": "condensed_particles + spectrum throughput", "value": value, "unit": "sites/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (random_phase IC, nv = enerv = 0.75, SplitMix64 seed 0)",
+        "config": {"workload": f"{n}^3 complex128 state: pack, backward cuFFT Z2Z, spectrum "
+                               "reduction + finaliser per call",
+                   "comp_amp": amp, "kc2": kc2,
+                   "l2": f"state {16 * sites / 1e9:.2f} GB > L2, no flush needed"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps,
+        "n0_over_V": c.row["n0_over_V"], "eta": c.eta.tolist(), "nharm": c.nharm.tolist(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def workload_config(ngpus, n=N_GRID):
     return {"workload": f"{n}^3 periodic grid, h=0.5, 4th-order FD, RK4 dt=0.005, equation 4 "
                         "(g=mu=1, V=0), complex64 psi + Kahan compensation, FP64 norm per step",
@@ -551,7 +673,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=N_GRID,
                     help="cube edge (default 512; smaller sizes are for profiling captures)")
-    ap.add_argument("--workload", default="cube", choices=["cube", "ensemble", "learned", "rkf45"])
+    ap.add_argument("--workload", default="cube",
+                    choices=["cube", "ensemble", "learned", "rkf45", "spectrum"])
     ap.add_argument("--t-end", type=float, default=20.0, help="rkf45 workload end time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -563,6 +686,10 @@ def main():
         return run_ensemble(args)
     if args.workload == "rkf45":
         return run_rkf45(args)
+    if args.workload == "spectrum":
+        if "--steps" not in sys.argv:
+            args.steps = 20
+        return run_spectrum(args)
     if args.workload == "learned":
         if "--steps" not in sys.argv:
             args.steps = 200

@@ -19,7 +19,7 @@ STATUS_NAMES = {
 }
 SCHEMES = {"euler": 0, "rk2": 1, "rk4": 2, "rk45": 3}
 TIMING_FAMILIES = ["stage_first", "stage_mid", "stage_last", "reduce", "energy", "copy", "other",
-                   "unused"]
+                   "spectrum"]
 
 
 class GpeError(RuntimeError):
@@ -95,6 +95,13 @@ SIGNATURES = {
     "gpe_gpu_energy": (ctypes.c_int, [_vp, _dp, _dp]),
     "gpe_gpu_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
     "gpe_gpu_wait_probe": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "gpe_gpu_get_site": (ctypes.c_int, [_vp, _i32, _i32, _i32, _dp]),
+    "gpe_gpu_random_phase": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_uint64, _dp, _dp]),
+    "gpe_gpu_condensed_particles": (ctypes.c_int, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int64),
+                                                   _dp, _i32]),
+    "gpe_gpu_filtered_field": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vp, _i32,
+                                              _i32]),
     "gpe_gpu_renormalise": (ctypes.c_int, [_vp, ctypes.c_double]),
     "gpe_gpu_rhs": (ctypes.c_int, [_vp, _vp, _i32]),
     "gpe_gpu_laplacian": (ctypes.c_int, [_vp, _vp, _i32]),

@@ -68,7 +68,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         sys.stderr.write(r.stdout + r.stderr)
         if r.returncode != 0:
             raise subprocess.CalledProcessError(r.returncode, r.args)
-    link = [nvcc_path(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
+    link = [nvcc_path(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-ldl"]
     subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB

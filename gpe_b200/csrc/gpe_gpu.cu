@@ -176,6 +176,7 @@ struct gpe_ctx {
   // enqueued after every completed step (the learned correction)
   int (*post_step)(void*, gpe_ctx*) = nullptr;
   void* post_arg = nullptr;
+  std::unique_ptr<gpe::Extension> ext;
   std::string err;
 };
 
@@ -195,8 +196,17 @@ int gpe_internal_field_view(gpe_ctx* c, gpe::FieldView* v) {
   v->single_domain = (c->nranks == 1 && c->nzg == c->nz) ? 1 : 0;
   v->stream = c->stream;
   v->status = c->d_status;
+  v->dx = c->dx; v->dy = c->dy; v->dz = c->dz;
+  v->xr = c->prm.xr; v->yr = c->prm.yr; v->zr = c->prm.zr;
+  v->stage = c->d_stage;
   c->norm_valid = false;
   return GPE_OK;
+}
+
+std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c) { return c->ext; }
+
+void gpe_internal_count_launches(gpe_ctx* c, int64_t n) {
+  if (c) c->launches += n;
 }
 
 namespace {
@@ -1104,12 +1114,8 @@ int alloc_field(gpe_ctx* c, int id) {
   return GPE_OK;
 }
 
-int stage_in(gpe_ctx* c, const void* src, int elem_bytes, bool device) {
-  const size_t bytes = c->nint * (size_t)elem_bytes;
-  CU_CHECK(c, cudaMemcpyAsync(c->d_stage, src, bytes,
-                              device ? cudaMemcpyDeviceToDevice
-                                     : cudaMemcpyHostToDevice,
-                              c->stream));
+// d_stage (dense, elements of elem_bytes) -> psi with ghosts.
+int load_stage(gpe_ctx* c, int elem_bytes) {
   Launch L{};
   begin_timed(c, L, GPE_FAM_COPY, (int64_t)c->nint);
   const Geom g = geom(c);
@@ -1140,7 +1146,17 @@ int stage_in(gpe_ctx* c, const void* src, int elem_bytes, bool device) {
   return exchange_ghosts(c, c->psi_id);
 }
 
-int stage_out(gpe_ctx* c, int field, void* dst, int elem_bytes, bool device) {
+int stage_in(gpe_ctx* c, const void* src, int elem_bytes, bool device) {
+  const size_t bytes = c->nint * (size_t)elem_bytes;
+  CU_CHECK(c, cudaMemcpyAsync(c->d_stage, src, bytes,
+                              device ? cudaMemcpyDeviceToDevice
+                                     : cudaMemcpyHostToDevice,
+                              c->stream));
+  return load_stage(c, elem_bytes);
+}
+
+// field -> d_stage (dense, elements of elem_bytes).
+int pack_stage(gpe_ctx* c, int field, int elem_bytes) {
   Launch L{};
   begin_timed(c, L, GPE_FAM_COPY, (int64_t)c->nint);
   const Geom g = geom(c);
@@ -1164,6 +1180,12 @@ int stage_out(gpe_ctx* c, int field, void* dst, int elem_bytes, bool device) {
   CU_CHECK(c, cudaGetLastError());
   end_timed(c, L);
   c->launches++;
+  return GPE_OK;
+}
+
+int stage_out(gpe_ctx* c, int field, void* dst, int elem_bytes, bool device) {
+  int rc = pack_stage(c, field, elem_bytes);
+  if (rc) return rc;
   CU_CHECK(c, cudaMemcpyAsync(dst, c->d_stage, c->nint * (size_t)elem_bytes,
                               device ? cudaMemcpyDeviceToDevice
                                      : cudaMemcpyDeviceToHost,
@@ -1186,6 +1208,22 @@ int check_elem(gpe_ctx* c, int elem_bytes, const void* ptr) {
 }
 
 }  // namespace
+
+int gpe_internal_fail(gpe_ctx* c, int code, const std::string& msg) { return fail(c, code, msg); }
+void gpe_internal_time_begin(gpe_ctx* c, gpe::TimedRegion* r, int family, int64_t sites) {
+  Launch L{};
+  begin_timed(c, L, family, sites);
+  r->a = L.a;
+  r->b = L.b;
+  r->family = family;
+  r->sites = sites;
+}
+void gpe_internal_time_end(gpe_ctx* c, gpe::TimedRegion* r) {
+  if (!r->a) return;
+  Launch L{r->family, r->a, r->b, r->sites};
+  end_timed(c, L);
+}
+int gpe_internal_load_stage(gpe_ctx* c) { return load_stage(c, c->es); }
 
 // ==========================================================================
 // Batched ensembles: independent runs of uneven grids stepped by one
@@ -1531,6 +1569,7 @@ void gpe_gpu_destroy(gpe_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  c->ext.reset();
   if (c->comm && g_nccl.ok) g_nccl.CommDestroy(c->comm);
   for (int i = 0; i < F_COUNT; i++)
     if (c->fld[i]) cudaFree(c->fld[i]);
@@ -1599,6 +1638,29 @@ int gpe_gpu_get_state_device(gpe_ctx* c, void* psi, int32_t elem_bytes) {
   rc = check_elem(c, elem_bytes, psi);
   if (rc) return rc;
   return stage_out(c, c->psi_id, psi, elem_bytes, true);
+}
+
+int gpe_gpu_get_site(gpe_ctx* c, int32_t i, int32_t j, int32_t k, double* re_im) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!re_im) return fail(c, GPE_ERR_INVALID, "null output");
+  if (i < 0 || i >= c->nx || j < 0 || j >= c->ny || k < 0 || k >= c->nz)
+    return fail(c, GPE_ERR_INVALID, "site outside the grid");
+  const size_t q = ((size_t)(k + 2) * c->Ny + (size_t)(j + 2)) * c->Nx + (size_t)(i + 2);
+  unsigned char buf[16];
+  CU_CHECK(c, cudaMemcpyAsync(buf, static_cast<const unsigned char*>(c->fld[c->psi_id]) +
+                                       q * (size_t)c->es,
+                              (size_t)c->es, cudaMemcpyDeviceToHost, c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  if (c->es == 8) {
+    float f[2];
+    memcpy(f, buf, sizeof(f));
+    re_im[0] = f[0];
+    re_im[1] = f[1];
+  } else {
+    memcpy(re_im, buf, 2 * sizeof(double));
+  }
+  return GPE_OK;
 }
 
 int gpe_gpu_solver(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {

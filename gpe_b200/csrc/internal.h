@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 
 #include "gpe_gpu.h"
@@ -21,6 +22,23 @@ struct FieldView {
   int single_domain;
   cudaStream_t stream;
   int* status;  // the context's device status word (wait timeouts)
+  double dx, dy, dz;  // grid spacings, 2 xr / (nx - 1) etc.
+  double xr, yr, zr;  // box half-widths
+  void* stage;        // dense staging buffer, nx ny nz elements of 16 bytes
+};
+
+// A timed region on a context's stream (recorded only while the context's
+// timing is on; collected by gpe_gpu_get_timing under `family`).
+struct TimedRegion {
+  cudaEvent_t a = nullptr, b = nullptr;
+  int family = 0;
+  int64_t sites = 0;
+};
+
+// Per-context state of another translation unit, owned by the context and
+// deleted with it (with the context's device current, its stream drained).
+struct Extension {
+  virtual ~Extension() = default;
 };
 
 }  // namespace gpe
@@ -31,3 +49,14 @@ int gpe_internal_field_view(gpe_ctx* c, gpe::FieldView* v);
 // c's stream); null detaches.
 void gpe_internal_set_post_step(gpe_ctx* c, int (*fn)(void*, gpe_ctx*), void* arg);
 void gpe_internal_set_last_error(const std::string& msg);
+// Records msg as the context's last error and returns code.
+int gpe_internal_fail(gpe_ctx* c, int code, const std::string& msg);
+// The context's extension slot.
+std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c);
+// Dense staging buffer (x fastest, elements of the field's own es bytes) ->
+// psi with the boundary ghosts filled; invalidates the cached norm.
+int gpe_internal_load_stage(gpe_ctx* c);
+void gpe_internal_time_begin(gpe_ctx* c, gpe::TimedRegion* r, int family, int64_t sites);
+void gpe_internal_time_end(gpe_ctx* c, gpe::TimedRegion* r);
+// Adds n to the context's launch counter (kernels enqueued by other units).
+void gpe_internal_count_launches(gpe_ctx* c, int64_t n);

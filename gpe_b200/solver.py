@@ -13,6 +13,8 @@ reference would call emergency_stop (src/error.f90:24-46).
 from __future__ import annotations
 
 import ctypes
+import math
+import os
 from dataclasses import dataclass, fields
 
 import numpy as np
@@ -148,6 +150,14 @@ class GpeSolver:
         check(lib().gpe_gpu_get_state_device(self._ctx, ctypes.c_void_p(out.data_ptr()), eb),
               self._ctx)
 
+    def get_site(self, i: int, j: int, k: int) -> complex:
+        """psi at interior site (i, j, k): the save_time point value."""
+        v = np.zeros(2)
+        check(lib().gpe_gpu_get_site(self._ctx, int(i), int(j), int(k),
+                                     v.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              self._ctx)
+        return complex(v[0], v[1])
+
     # ---- the reference's hot-path procedures --------------------------------
     def _tm(self) -> GpeTimeC:
         return GpeTimeC(self.t, self.im_t, self.dt.real, self.dt.imag, self.p, 0)
@@ -233,6 +243,22 @@ class GpeSolver:
               self._ctx)
         return m.value, mom
 
+    # ---- spectral initial condition and diagnostics (cuFFT) ------------------
+    def random_phase(self, nv: float, enerv: float, seed: int = 0):
+        """random_phase initial condition (src/ic.f90:190-269) -> (comp_amp, kc2)."""
+        from . import spectral
+        return spectral.random_phase(self, nv, enerv, seed)
+
+    def condensed_particles(self):
+        """condensed_particles + spectrum (src/io.f90:315-404, 632-725)."""
+        from . import spectral
+        return spectral.condensed_particles(self)
+
+    def filtered_field(self, filter_kc: float, m: float = 1.0, out=None):
+        """The filtered field of filtered_surface (src/io.f90:533-628)."""
+        from . import spectral
+        return spectral.filtered_field(self, filter_kc, m, out)
+
     def renormalise(self, norm: float) -> None:
         """renormalise (src/variables.f90:698-709)."""
         check(lib().gpe_gpu_renormalise(self._ctx, float(norm)), self._ctx)
@@ -282,18 +308,91 @@ class GpeSolver:
         return int(lib().gpe_gpu_device_bytes(self._ctx))
 
 
+@dataclass
+class OutputParams:
+    """io_params of run.in (src/parameters.f90:57-90) that drive the loop's
+    output cadence (src/gpe.f90:176-226)."""
+    save_rate: int = 10        # energy.dat, psi_time.dat, norm.dat every save_rate steps
+    save_rate2: float = 50.0   # idl_surface (save_3d) every save_rate2 time units
+    save_rate3: float = 50.0   # condensed_particles every save_rate3 time units
+    p_save: float = 10.0       # end_state every p_save time units
+    save_3d: bool = True
+    save_spectrum: bool = True
+    save_filter: bool = False
+    filter_kc: float = 10.0
+
+
+def _modulo(a: float, p: float) -> float:
+    """Fortran modulo: a - floor(a / p) p."""
+    return a - math.floor(a / p) * p
+
+
+def _pr_bytes(prm) -> int:
+    return 8 if prm.precision == 16 else 4
+
+
+def _idl_surface(s, run_dir):
+    from . import output
+    output.write_idl_surface(run_dir, s.p, s.t, s.im_t, s.get_state(), s.grid(),
+                             pr_bytes=_pr_bytes(s.prm))
+
+
+def _end_state(s, run_dir):
+    from . import output
+    d = os.path.join(run_dir, output.proc_dir(0))
+    os.makedirs(d, exist_ok=True)
+    s.save_end_state(os.path.join(d, "end_state.dat"))
+
+
+def _cadence_outputs(s, run_dir, io: OutputParams, counters: dict) -> None:
+    """The writes before solver in the reference loop (src/gpe.f90:176-226),
+    on the current state."""
+    from . import output
+    prm = s.prm
+    t_all = s.t + s.im_t
+    adt = abs(s.dt)
+    if _modulo(t_all, adt * io.save_rate) < adt:
+        E, _ = s.energy()
+        output.append(os.path.join(run_dir, "energy.dat"),
+                      output.energy_line(s.t, s.im_t, E, prm.nx * prm.ny * prm.nz))
+        v = s.get_site(prm.nx // 2, prm.ny // 2, prm.nz // 2)
+        output.append(os.path.join(run_dir, "psi_time.dat"), output.psi_time_line(s.t, s.im_t, v))
+    if t_all >= io.save_rate3 * counters["m"]:
+        c = s.condensed_particles()
+        output.append(os.path.join(run_dir, "mass.dat"), output.mass_line(s.t, s.im_t, c.row))
+        if io.save_spectrum:
+            output.write_spectrum(run_dir, s.p, s.t, c)
+        if io.save_filter:
+            f = s.filtered_field(io.filter_kc, 1.0)
+            output.write_filtered_surface(run_dir, s.p, s.t, f, s.grid(),
+                                          pr_bytes=_pr_bytes(prm))
+        counters["m"] += 1
+    if t_all >= io.save_rate2 * counters["n"]:
+        if io.save_3d:
+            _idl_surface(s, run_dir)
+        counters["n"] += 1
+    if t_all >= io.p_save * counters["ps"]:
+        _end_state(s, run_dir)
+        counters["ps"] += 1
+
+
 def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool = False,
-             record=None, run_dir: str | None = None):
+             record=None, run_dir: str | None = None, outputs: OutputParams | None = None):
     """The per-step bookkeeping of the reference time loop (src/gpe.f90:134-278)
     with an explicit step count: solver, get_norm + relnorm (equation 4),
     imaginary-to-real switch at relnorm < 1e-12 (:251-268), renormalise.
     With run_dir, the loop also keeps the reference's cooperative controls:
-    it stops, writing run_dir/end_state.dat, when the file RUNNING is absent
-    before a step (:136-159), and when a file SAVE appears after a step it
-    writes a snapshot run_dir/snapshot_<p>.dat in the same format and
-    deletes SAVE (the reference writes an IDL surface there, src/io.f90:1566).
+    it stops, writing run_dir/proc00/end_state.dat, when the file RUNNING is
+    absent before a step (:136-159), and when a file SAVE appears after a
+    step it writes the IDL surface run_dir/proc00/densNNNNNNN.dat and deletes
+    SAVE (save_run, src/io.f90:1566-1595).  With outputs as well, it writes
+    the reference's files at its cadence: energy.dat and psi_time.dat (and
+    norm.dat after the step) every save_rate steps, condensed_particles
+    (mass.dat, spectra, filtered surface) every save_rate3, idl_surface every
+    save_rate2 and end_state every p_save time units, the counters starting
+    from the current time (:126-128).
     Returns the list of (t, im_t, norm, relnorm) after each step."""
-    import os
+    from . import output
     prm = s.prm
     out = [] if record is None else record
     prev_norm = 1.0
@@ -301,26 +400,42 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
         prev_norm = s.get_norm()
         if renorm:
             s.renormalise(prev_norm)
+    counters = {}
+    if outputs is not None:
+        counters = {"ps": int(s.t / outputs.p_save), "n": int(s.t / outputs.save_rate2),
+                    "m": int(s.t / outputs.save_rate3)}
     norm = 0.0
     for _ in range(nsteps):
         if run_dir is not None and not os.path.exists(os.path.join(run_dir, "RUNNING")):
-            s.save_end_state(os.path.join(run_dir, "end_state.dat"))
+            _end_state(s, run_dir)
             break
+        if outputs is not None and run_dir is not None:
+            _cadence_outputs(s, run_dir, outputs, counters)
         s.solver()
         if run_dir is not None and os.path.exists(os.path.join(run_dir, "SAVE")):
-            s.save_end_state(os.path.join(run_dir, "snapshot_%07d.dat" % (s.p + 1)))
+            _idl_surface(s, run_dir)
             os.remove(os.path.join(run_dir, "SAVE"))
         relnorm = 0.0
         if prm.eqn_to_solve == 4:
             norm = s.get_norm()
             relnorm = abs((norm - prev_norm) / prev_norm)
             out.append((s.t, s.im_t, norm, relnorm))
+            if outputs is not None and run_dir is not None and \
+                    _modulo(s.t + s.im_t, abs(s.dt) * outputs.save_rate) < abs(s.dt):
+                output.append(os.path.join(run_dir, "norm.dat"),
+                              output.norm_line(s.t, s.im_t, norm, relnorm))
         if prm.eqn_to_solve == 4 and not prm.real_time:
             if relnorm < 1e-12:
                 if stop_imag:
                     break
                 s.set_real_time(True)
                 s.im_t = 0.0
+                if outputs is not None:
+                    counters = {"ps": int(s.t / outputs.p_save),
+                                "n": int(s.t / outputs.save_rate2),
+                                "m": int(s.t / outputs.save_rate3)}
+                    if outputs.save_3d and run_dir is not None:
+                        _idl_surface(s, run_dir)
                 s.dt = complex(abs(s.dt.imag), abs(s.dt.real))
             if renorm:
                 s.renormalise(norm)

@@ -112,7 +112,8 @@ typedef struct gpe_timing {
 #define GPE_FAM_REDUCE 3       /* reduction finalisers */
 #define GPE_FAM_ENERGY 4
 #define GPE_FAM_COPY 5         /* state pack/unpack, ghost fill, scale */
-#define GPE_FAM_OTHER 6
+#define GPE_FAM_OTHER 6        /* cuFFT transforms and the rest */
+#define GPE_FAM_SPECTRUM 7     /* spectrum / condensate reduction pass */
 
 typedef struct gpe_ctx gpe_ctx;
 
@@ -146,6 +147,11 @@ int gpe_gpu_get_state(gpe_ctx* ctx, void* psi, int32_t elem_bytes);
 int gpe_gpu_set_state_device(gpe_ctx* ctx, const void* psi,
                              int32_t elem_bytes);
 int gpe_gpu_get_state_device(gpe_ctx* ctx, void* psi, int32_t elem_bytes);
+
+/* psi at the interior site (i, j, k) of this context (k counts the
+ * context's own planes) into re_im[2] (HOST): the point value save_time
+ * writes to psi_time.dat (src/io.f90:147-195), without copying the field. */
+int gpe_gpu_get_site(gpe_ctx* ctx, int32_t i, int32_t j, int32_t k, double* re_im);
 
 /* One call of solver(var_in, var_out) (src/solve.f90:25-53) on the
  * resident state: advances psi by one step of the configured scheme and
@@ -186,6 +192,43 @@ int gpe_gpu_energy(gpe_ctx* ctx, double* E, double* H4);
  * (Re psi - 1) Im(d conj psi) - Im psi Re(d psi)) of the resident state, in
  * one device pass with FP64 sums; mom has 3 entries. */
 int gpe_gpu_diagnostics(gpe_ctx* ctx, double* mass, double* mom);
+
+/* Spectral initial condition and diagnostics on cuFFT (single-domain
+ * contexts; a z-slab context returns GPE_ERR_INVALID).  Transforms follow
+ * the reference's fft (src/ic.f90:905-1000): 'forward' = exp(-i k.x),
+ * 'backward' = exp(+i k.x), both scaled by 1/sqrt(nx ny nz); the integer
+ * wavenumber of index i along an axis of n points is i for
+ * i <= (n-1)/2 + 1 and n - i above (src/ic.f90:221-238).  libcufft.so.11 is
+ * opened on first use; without it the calls return GPE_ERR_CUDA.
+ *
+ * gpe_gpu_random_phase replaces ics' random_phase (src/ic.f90:190-252) with
+ * get_kc_amp (:256-269): every mode with |k|^2 <= kc2 gets amplitude
+ * comp_amp and phase 2 pi phi, all others zero, and psi is the forward
+ * transform, ghosts filled.  phi for the mode at dense index
+ * q = (k ny + j) nx + i is the top 53 bits of SplitMix64(seed + (q+1) G),
+ * G = 0x9E3779B97F4A7C15, times 2^-53 (the reference draws Fortran
+ * random_number from a clock seed; this is reproducible).  *amp_out and
+ * *kc2_out (may be NULL) receive comp_amp and kc2. */
+int gpe_gpu_random_phase(gpe_ctx* ctx, double nv, double enerv, uint64_t seed,
+                         double* amp_out, double* kc2_out);
+
+/* condensed_particles (src/io.f90:315-404) and spectrum (:632-725) of the
+ * resident state in one pass over its backward transform a:
+ *   row[0..6] = M/(8 xr yr zr), n0/V, M, n0, temp, temp2, H/V (columns 3-9
+ *     of mass.dat; M = sum |psi|^2 dx dy dz, here by Parseval over a);
+ *   eta[7], nharm[7] = mean occupation and mode count of the 7 logarithmic
+ *     shells (spectrum*.dat);
+ *   F[nf] = the integral distribution function F(kk), kk = 1..nf, nf = nx/2
+ *     (idf*.dat; nf must equal nx/2).
+ * Any output pointer may be NULL (HOST arrays). */
+int gpe_gpu_condensed_particles(gpe_ctx* ctx, double* row, double* eta,
+                                int64_t* nharm, double* F, int32_t nf);
+
+/* filtered_surface (src/io.f90:533-628): a = backward transform of psi,
+ * a(k) *= max(1 - m |k|^2 / filter_kc^2, 0), out = forward transform
+ * (interior layout, x fastest; HOST when device_out = 0, else DEVICE). */
+int gpe_gpu_filtered_field(gpe_ctx* ctx, double filter_kc, double m, void* out,
+                           int32_t elem_bytes, int32_t device_out);
 
 /* Failure-detection self-test (no reference counterpart): runs, on the
  * context's stream, a device wait on a flag that nothing sets, bounded by

@@ -628,6 +628,24 @@ def run_spectrum(args):
            "d2h_bytes_per_step": 8 * (21 + n // 2), "ms_per_step": e2e_ms,
            "form": "gpe_gpu_set_state (pinned host psi) + gpe_gpu_condensed_particles "
                    "(row, eta, nharm, F to host), per call"}
+
+    # vortex line length of the same state (gpe_gpu_linelength), its own line
+    s.linelength()
+    s.set_timing(True)
+    s.timing()
+    e0.record(stream)
+    kl = 5
+    for _ in range(kl):
+        length = s.linelength()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    lfam = s.timing()
+    s.set_timing(False)
+    line_ms = e0.elapsed_time(e1) / kl
+    cells_ms = lfam["other"]["ms"] / max(lfam["other"]["launches"], 1)
+    linelen = {"length": length, "ms_per_call": line_ms, "sites_per_s": sites / (line_ms / 1e3),
+               "cells_kernel_ms": cells_ms,
+               "cells_kernel_gbs": 16 * sites / (cells_ms / 1e3) / 1e9}
     s.close()
     cpu = None
     if not args.no_cpu_baseline:
@@ -635,6 +653,15 @@ def run_spectrum(args):
         cpu = {"value": v, "unit": "sites/s", "cores": 1, "kind": "port",
                "sample": f"{calls} calls on a 128^3 random-phase state (vectorised numpy oracle: "
                          f"backward FFT, condensate row, spectrum), 1 thread, {el:.1f} s"}
+        import oracle
+        from oracle import spectral_ref as ref
+        m = 128
+        ph = ref.splitmix_phases(0, m ** 3).reshape(m, m, m)
+        small = ref.random_phase_fast(m, m, m, 0.75, 0.75, ph)
+        t0 = time.perf_counter()
+        oracle.linelength(small, 1.0)
+        linelen["cpu_sites_per_s"] = m ** 3 / (time.perf_counter() - t0)
+        linelen["cpu_sample"] = "oracle linelength (C, 1 thread) on a 128^3 random-phase state"
     line = {
         "metric": "condensed_particles + spectrum throughput", "value": value, "unit": "sites/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -647,6 +674,7 @@ def run_spectrum(args):
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps,
         "n0_over_V": c.row["n0_over_V"], "eta": c.eta.tolist(), "nharm": c.nharm.tolist(),
+        "linelength": linelen,
     }
     print(json.dumps(line), flush=True)
     return 0

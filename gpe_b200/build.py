@@ -19,6 +19,9 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libgpe_gpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# per-file flags: the line-length cells follow the reference's arithmetic
+# operation by operation, so nothing may be contracted into an FMA
+EXTRA = {"vortex.cu": ["-fmad=false"]}
 
 
 def nvcc_path() -> str:
@@ -56,7 +59,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     for cu in cus:
         obj = os.path.join(objdir, os.path.basename(cu)[:-3] + ".o")
         objs.append(obj)
-        cmds.append([*common, "-c", cu, "-o", obj])
+        cmds.append([*common, *EXTRA.get(os.path.basename(cu), []), "-c", cu, "-o", obj])
     # translation units compile in parallel, then one link
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:

@@ -176,7 +176,7 @@ struct gpe_ctx {
   // enqueued after every completed step (the learned correction)
   int (*post_step)(void*, gpe_ctx*) = nullptr;
   void* post_arg = nullptr;
-  std::unique_ptr<gpe::Extension> ext;
+  std::unique_ptr<gpe::Extension> ext[GPE_EXT_SLOTS];
   std::string err;
 };
 
@@ -203,7 +203,9 @@ int gpe_internal_field_view(gpe_ctx* c, gpe::FieldView* v) {
   return GPE_OK;
 }
 
-std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c) { return c->ext; }
+std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c, int slot) {
+  return c->ext[slot];
+}
 
 void gpe_internal_count_launches(gpe_ctx* c, int64_t n) {
   if (c) c->launches += n;
@@ -1569,7 +1571,7 @@ void gpe_gpu_destroy(gpe_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  c->ext.reset();
+  for (auto& e : c->ext) e.reset();
   if (c->comm && g_nccl.ok) g_nccl.CommDestroy(c->comm);
   for (int i = 0; i < F_COUNT; i++)
     if (c->fld[i]) cudaFree(c->fld[i]);

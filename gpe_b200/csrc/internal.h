@@ -51,8 +51,9 @@ void gpe_internal_set_post_step(gpe_ctx* c, int (*fn)(void*, gpe_ctx*), void* ar
 void gpe_internal_set_last_error(const std::string& msg);
 // Records msg as the context's last error and returns code.
 int gpe_internal_fail(gpe_ctx* c, int code, const std::string& msg);
-// The context's extension slot.
-std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c);
+// The context's extension slots (0 spectral, 1 vortex line length).
+constexpr int GPE_EXT_SPECTRAL = 0, GPE_EXT_VORTEX = 1, GPE_EXT_SLOTS = 2;
+std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c, int slot);
 // Dense staging buffer (x fastest, elements of the field's own es bytes) ->
 // psi with the boundary ghosts filled; invalidates the cached norm.
 int gpe_internal_load_stage(gpe_ctx* c);

@@ -123,7 +123,7 @@ int prepare(gpe_ctx* c, FieldView* v, Spectral** out) {
                              "spectral calls need a single-domain context (the whole grid)");
   std::call_once(g_fft_once, load_cufft);
   if (!g_fft.ok) return gpe_internal_fail(c, GPE_ERR_CUDA, g_fft.why);
-  auto& slot = gpe_internal_extension(c);
+  auto& slot = gpe_internal_extension(c, GPE_EXT_SPECTRAL);
   if (!slot) slot.reset(new Spectral());
   Spectral* s = static_cast<Spectral*>(slot.get());
   if (!s->has_plan) {
@@ -172,13 +172,13 @@ int exec(gpe_ctx* c, Spectral* s, const FieldView& v, int dir) {
   return GPE_OK;
 }
 
-template <typename T>
+template <typename T, int E>
 int launch_spectrum(gpe_ctx* c, Spectral* s, const FieldView& v, const SpecArgs& a,
                     const SpecFinal& f0, size_t smem, int64_t sites) {
-  SP_CU(c, cudaFuncSetAttribute(spectrum_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SP_CU(c, cudaFuncSetAttribute(spectrum_kernel<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem));
   int per_sm = 1, sms = 148;
-  SP_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spectrum_kernel<T>, S_THREADS,
+  SP_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spectrum_kernel<T, E>, S_THREADS,
                                                          smem));
   SP_CU(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v.dev));
   const long long nrows = (long long)v.ny * v.nz;
@@ -203,7 +203,7 @@ int launch_spectrum(gpe_ctx* c, Spectral* s, const FieldView& v, const SpecArgs&
   const T* buf = static_cast<const T*>(v.stage);
   TimedRegion t1, t2;
   gpe_internal_time_begin(c, &t1, GPE_FAM_SPECTRUM, sites);
-  spectrum_kernel<T><<<nblk, S_THREADS, smem, v.stream>>>(buf, args);
+  spectrum_kernel<T, E><<<nblk, S_THREADS, smem, v.stream>>>(buf, args);
   SP_CU(c, cudaGetLastError());
   gpe_internal_time_end(c, &t1);
   gpe_internal_time_begin(c, &t2, GPE_FAM_REDUCE, 0);
@@ -259,8 +259,16 @@ int spectrum_pass(gpe_ctx* c, Spectral* s, const FieldView& v) {
   f.cell = v.dx * v.dy * v.dz;
   f.box8 = 8.0 * v.xr * v.yr * v.zr;
   const int64_t sites = (int64_t)v.nx * v.ny * v.nz;
-  if (v.es == 16) return launch_spectrum<double>(c, s, v, a, f, smem, sites);
-  return launch_spectrum<float>(c, s, v, a, f, smem, sites);
+  // sites per lane: a warp pass (32 E sites) about half a row, 2 to 8
+  const int half = (v.nx + 1) / 2;
+  if (v.es == 16) {
+    if (half <= 64) return launch_spectrum<double, 2>(c, s, v, a, f, smem, sites);
+    if (half <= 128) return launch_spectrum<double, 4>(c, s, v, a, f, smem, sites);
+    return launch_spectrum<double, 8>(c, s, v, a, f, smem, sites);
+  }
+  if (half <= 64) return launch_spectrum<float, 2>(c, s, v, a, f, smem, sites);
+  if (half <= 128) return launch_spectrum<float, 4>(c, s, v, a, f, smem, sites);
+  return launch_spectrum<float, 8>(c, s, v, a, f, smem, sites);
 }
 
 }  // namespace

@@ -101,18 +101,30 @@ struct Shells {
   int dn[NSHELLS + 1];
 };
 
-// Shell index of k2 >= 1 (NSHELLS for none); `hi` = on the |k| >= 2 pi side.
-__device__ __forceinline__ int shell_of(int k2, const Shells& t, bool& hi) {
-  hi = k2 >= t.up[0];
+// Shell index of k2 >= 1 (NSHELLS for none) as 0..7 on the |k| < 2 pi side
+// and 8..15 on the other, so equal codes mean one interval of k2.
+__device__ __forceinline__ int shell_code(int k2, const int* up, const int* dn) {
   int s = 0;
-  if (hi) {
+  if (k2 >= up[0]) {
 #pragma unroll
-    for (int q = 1; q <= NSHELLS; q++) s += (k2 >= t.up[q]) ? 1 : 0;
-  } else {
-#pragma unroll
-    for (int q = 1; q <= NSHELLS; q++) s += (k2 <= t.dn[q]) ? 1 : 0;
+    for (int q = 1; q <= NSHELLS; q++) s += (k2 >= up[q]) ? 1 : 0;
+    return 8 + s;
   }
+#pragma unroll
+  for (int q = 1; q <= NSHELLS; q++) s += (k2 <= dn[q]) ? 1 : 0;
   return s;
+}
+
+// 1/d by Newton-Raphson iteration r <- r + r (1 - d r) from the hardware's
+// approximate reciprocal; three steps take any start within 2^-10 to full
+// double precision.  d is a normal nonzero double wherever the result is
+// used (d = 0 is discarded by the caller).
+__device__ __forceinline__ double recip_newton(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+#pragma unroll
+  for (int q = 0; q < 3; q++) r = fma(r, fma(-d, r, 1.0), r);
+  return r;
 }
 
 struct SpecArgs {
@@ -130,15 +142,15 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
-constexpr int S_E = 8;  // consecutive sites per lane: a warp covers 256 sites per pass
 constexpr int S_NONE = 0x7fffffff;
 
 // One pass over the unnormalised backward transform: Parseval mass, the
 // temperature denominator sum (k2+rho0)/(k2^2+2 rho0 k2) over the
 // finite-difference symbol (src/io.f90:347-366), shell sums and counts, and
 // the F bins.  Warps own whole x-rows and walk each row in its two halves
-// (i up to (nx-1)/2+1, then the rest), along each of which |k| and so the F
-// bin is monotone in i.  A lane takes 8 consecutive sites: equal-bin runs
+// (i below (nx-1)/2+1, then the rest), along each of which |k| and so the F
+// bin is monotone in i.  A lane takes S_E consecutive sites (32 S_E about
+// half a row, at most 256 sites per pass): equal-bin runs
 // inside the lane are summed in registers, a run strictly inside the lane is
 // the only one with its bin and goes straight to the warp's bin array, and
 // the runs at lane edges are joined across lanes by one segmented warp scan.
@@ -146,9 +158,9 @@ constexpr int S_NONE = 0x7fffffff;
 // atomics and the sums come out the same bit for bit on every run.  Shells
 // change rarely along a row: a lane whose first and last site share a shell
 // (and side) adds its sum once.
-template <typename T>
-__global__ void __launch_bounds__(S_THREADS, 3) spectrum_kernel(const T* __restrict__ a,
-                                                                 SpecArgs p) {
+template <typename T, int S_E>
+__global__ void __launch_bounds__(S_THREADS, S_E <= 4 ? 4 : 3) spectrum_kernel(
+    const T* __restrict__ a, SpecArgs p) {
   extern __shared__ double smem_f[];            // [S_WARPS][nf]
   __shared__ double eta_s[S_WARPS][32][NSHELLS];  // per lane
   __shared__ int cnt_s[S_WARPS][32][NSHELLS];
@@ -165,12 +177,24 @@ __global__ void __launch_bounds__(S_THREADS, 3) spectrum_kernel(const T* __restr
   }
   __syncthreads();
 
+  __shared__ int sh_up[NSHELLS + 1], sh_dn[NSHELLS + 1];
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q <= NSHELLS; q++) {
+      sh_up[q] = p.shells.up[q];
+      sh_dn[q] = p.shells.dn[q];
+    }
+  }
+  __syncthreads();
+
+  // sums are of |buffer|^2; the finaliser applies the transform's 1/N
   const V2 a0 = reinterpret_cast<const V2*>(a)[0];
   const double rho0 = (((double)a0.x * a0.x + (double)a0.y * a0.y) * p.inv_n) * p.inv_v;
   const double two_rho0 = 2.0 * rho0;
   const double m12 = -(1.0 / 12.0);
   double mass = 0.0, tot = 0.0;
-  const int h = min((nx - 1) / 2 + 1, nx - 1);
+  // |k| rises along i < h and falls from h on (h = (nx-1)/2 + 1 is the peak)
+  const int h = min((nx - 1) / 2 + 1, nx);
   const long long nrows = (long long)p.ny * p.nz;
   for (long long row = (long long)blockIdx.x * S_WARPS + warp; row < nrows;
        row += (long long)gridDim.x * S_WARPS) {
@@ -180,7 +204,7 @@ __global__ void __launch_bounds__(S_THREADS, 3) spectrum_kernel(const T* __restr
     const double azk = __ldg(p.az + k);
     const V2* arow = reinterpret_cast<const V2*>(a) + (size_t)row * nx;
     for (int half = 0; half < 2; half++) {
-      const int start = half ? h + 1 : 0, end = half ? nx - 1 : h;
+      const int start = half ? h : 0, end = half ? nx - 1 : h - 1;
       for (int base = start; base <= end; base += 32 * S_E) {
         const int i0 = base + lane * S_E;
         V2 v[S_E];
@@ -189,68 +213,63 @@ __global__ void __launch_bounds__(S_THREADS, 3) spectrum_kernel(const T* __restr
           v[e].x = v[e].y = (T)0;
           if (i0 + e <= end) v[e] = arow[i0 + e];
         }
-        // shells: one decision for the lane when its ends agree
+        // shells: k2 is monotone along the lane's sites, so equal shell codes
+        // at its two ends put every site in that shell
         const int ilast = min(i0 + S_E - 1, end);
         const int k2f = (int)index_k2(i0, nx) + c2, k2l = (int)index_k2(ilast, nx) + c2;
-        bool hf = false, hl = false;
         const bool any = i0 <= end;
-        const int sf = (any && k2f > 0) ? shell_of(k2f, p.shells, hf) : -1;
-        const int sl = (any && k2l > 0) ? shell_of(k2l, p.shells, hl) : -2;
-        const bool one_shell = (sf == sl) && (hf == hl);
+        const int sf = (any && k2f > 0) ? shell_code(k2f, sh_up, sh_dn) : -1;
+        const int sl = (any && k2l > 0) ? shell_code(k2l, sh_up, sh_dn) : -2;
+        const bool one_shell = sf == sl;
         double lane_sum = 0.0;
         int lane_cnt = 0;
-        // F runs
+        // F runs: current (cb, cv), first (fb, fv)
         int cb = S_NONE, fb = S_NONE;
         double cv = 0.0, fv = 0.0;
         bool split = false;
 #pragma unroll
         for (int e = 0; e < S_E; e++) {
           const int i = i0 + e;
-          int b = S_NONE;
-          double pw = 0.0;
-          if (i <= end) {
-            pw = ((double)v[e].x * v[e].x + (double)v[e].y * v[e].y) * p.inv_n;
-            mass += pw;
-            const double k2p = m12 * ((__ldg(p.ax + i) + ayz) + azk);
-            if (k2p != 0.0) tot += (k2p + rho0) / (k2p * k2p + two_rho0 * k2p);
-            const int k2 = (int)index_k2(i, nx) + c2;
-            if (k2 > 0) {
-              if (one_shell) {
-                lane_sum += pw;
-                lane_cnt++;
-              } else {
-                bool hs;
-                const int s = shell_of(k2, p.shells, hs);
-                if (s < NSHELLS) {
-                  eta_s[warp][lane][s] += pw;
-                  cnt_s[warp][lane][s]++;
-                }
-              }
-              const int bb = ceil_sqrt(k2);
-              if (bb <= nf) b = bb;
+          const bool valid = i <= end;
+          const double pw = (double)v[e].x * v[e].x + (double)v[e].y * v[e].y;
+          mass += pw;  // zero past the end
+          const int ic = min(i, nx - 1);
+          const double k2p = m12 * ((__ldg(p.ax + ic) + ayz) + azk);
+          const double term = (k2p + rho0) * recip_newton(k2p * (k2p + two_rho0));
+          tot += (valid && k2p != 0.0) ? term : 0.0;
+          const int k2 = (int)index_k2(ic, nx) + c2;
+          const bool live = valid && k2 > 0;
+          if (one_shell) {
+            lane_sum += live ? pw : 0.0;
+            lane_cnt += live ? 1 : 0;
+          } else if (live) {
+            const int s = shell_code(k2, sh_up, sh_dn) & 7;
+            if (s < NSHELLS) {
+              eta_s[warp][lane][s] += pw;
+              cnt_s[warp][lane][s]++;
             }
           }
+          const int bb = ceil_sqrt(k2);
+          const int b = (live && bb <= nf) ? bb : S_NONE;
           const double val = (b != S_NONE) ? pw : 0.0;
           if (e == 0) {
             cb = b;
             cv = val;
-          } else if (b == cb) {
-            cv += val;
           } else {
-            if (!split) {
-              fb = cb;
-              fv = cv;
-              split = true;
-            } else if (cb != S_NONE) {
-              fw[cb - 1] += cv;  // a run inside the lane: no other lane has this bin
-            }
+            const bool same = b == cb;
+            const bool first = !same && !split;
+            const bool inner = !same && split && cb != S_NONE;
+            if (inner) fw[cb - 1] += cv;  // a run inside the lane: no other lane has this bin
+            fb = first ? cb : fb;
+            fv = first ? cv : fv;
+            split = split || !same;
+            cv = same ? cv + val : val;
             cb = b;
-            cv = val;
           }
         }
-        if (one_shell && sf >= 0 && sf < NSHELLS && lane_cnt > 0) {
-          eta_s[warp][lane][sf] += lane_sum;
-          cnt_s[warp][lane][sf] += lane_cnt;
+        if (one_shell && sf >= 0 && (sf & 7) < NSHELLS && lane_cnt > 0) {
+          eta_s[warp][lane][sf & 7] += lane_sum;
+          cnt_s[warp][lane][sf & 7] += lane_cnt;
         }
         const int lb = cb;
         const double lv = cv;
@@ -350,7 +369,7 @@ __global__ void __launch_bounds__(F_FIN_THREADS) spectrum_finalize_kernel(
   const double a0r = (double)a0.x, a0i = (double)a0.y;
   const double V = f.volume_v;
   const double n0 = (a0r * a0r + a0i * a0i) * f.inv_n;
-  const double M = col[0] * f.cell;
+  const double M = (col[0] * f.inv_n) * f.cell;
   const double tot = col[1];
   const double temp = (M - n0) / tot;
   const double E0 = (1.0 / (2.0 * V)) * (M * M + (M - n0) * (M - n0));
@@ -365,14 +384,14 @@ __global__ void __launch_bounds__(F_FIN_THREADS) spectrum_finalize_kernel(
   o[5] = temp2;
   o[6] = H / V;
   for (int m = 0; m < NSHELLS; m++) {
-    const double s = col[2 + m], n = col[2 + NSHELLS + m];
+    const double s = col[2 + m] * f.inv_n, n = col[2 + NSHELLS + m];
     o[7 + m] = (s == 0.0) ? 0.0 : s / n;
     o[14 + m] = n;
   }
   double run = 0.0;
   for (int b = 0; b < f.nf; b++) {
     run += col[HEAD + b];
-    o[21 + b] = run;
+    o[21 + b] = run * f.inv_n;
   }
 }
 

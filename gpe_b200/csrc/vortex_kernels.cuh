@@ -1,0 +1,430 @@
+// vortex_kernels.cuh -- total vortex line length (linelength,
+// src/variables.f90:879-1145) on the resident padded field.
+//
+// Cells (i, j, k), 1 <= i <= nx-2 (likewise j, k), in the reference's loop
+// order (k outer, i inner).  On each of a cell's 6 faces the zero lines of
+// Re psi and Im psi are located by linear interpolation along the face edges
+// and intersected; the first two points found on the cell's faces give a
+// segment.  The reference keeps its point arrays x(1:6), y(1:6), z(1:6) from
+// cell to cell, so a cell that finds one point measures to the x(2) left by
+// the last earlier cell that found two: that carried value is resolved here
+// by block scans in loop order (the cells of a block are contiguous), a
+// per-block "last x(2)" chained across blocks, and a pass over each block's
+// cells that came before its first writer.  The arithmetic is compiled
+// without FMA contraction and in the reference's order, so every cell's
+// points and segment equal a sequential evaluation bit for bit; only the
+// final sum is reassociated (a fixed tree, the same on every run).
+#pragma once
+
+#include <cstdint>
+
+namespace gpe {
+namespace vortex {
+
+constexpr int L_THREADS = 256;
+constexpr int L_WARPS = L_THREADS / 32;
+constexpr int L_CAP = 64;  // unresolved one-point cells kept per block
+
+struct Pt {
+  double x, y, z;
+};
+
+struct CellOut {
+  int skip;     // the cell ended on a zero plane / zero edge ("cycle iloop")
+  double add;   // 0.5 or 0.25 for those
+  int npts;     // points written to x(1..) before the cell ended
+  Pt p1, p2;
+};
+
+template <typename T> struct C2;
+template <> struct C2<double> { using type = double2; };
+template <> struct C2<float> { using type = float2; };
+
+// Accepted zero points of one component along the 4 edges of a face: the
+// first two (the only ones used) and their count.  An exact zero at a
+// corner writes the reference's xu(lu) without advancing lu and is always
+// overwritten before it is read, so it has no effect here.
+__device__ __forceinline__ int edge_zeros(const double w[5], double& x1, double& y1, double& x2,
+                                          double& y2) {
+  int cnt = 0;
+  double px = 0.0, py = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const double a = w[q], b = w[q + 1];
+    if (a != 0.0 && a * b < 0.0) {
+      double cx, cy;
+      if (q == 0) {
+        cx = fabs(a / (a - b));
+        cy = 0.0;
+      } else if (q == 1) {
+        cx = 1.0;
+        cy = fabs(a / (a - b));
+      } else if (q == 2) {
+        cx = fabs(b / (a - b));
+        cy = 1.0;
+      } else {
+        cx = 0.0;
+        cy = fabs(b / (a - b));
+      }
+      if (cnt == 0 || cx != px || cy != py) {
+        if (cnt == 0) {
+          x1 = cx;
+          y1 = cy;
+        }
+        if (cnt == 1) {
+          x2 = cx;
+          y2 = cy;
+        }
+        px = cx;
+        py = cy;
+        cnt++;
+      }
+    }
+  }
+  return cnt;
+}
+
+// Corners q = 0..3 of faces front, back, right, left, top, bottom
+// (src/variables.f90:901-958), one nibble each, corner = di | dj << 1 | dk << 2.
+__constant__ unsigned kFaceCorners[6] = {0x2310u, 0x6754u, 0x3751u, 0x2640u, 0x6732u, 0x4510u};
+
+// One cell of the reference's iloop body.
+__device__ __forceinline__ void cell_line(const double cu[8], const double cv[8], CellOut& o) {
+  o.skip = 0;
+  o.add = 0.0;
+  o.npts = 0;
+  int m = 0;
+#pragma unroll 1
+  for (int n = 0; n < 6; n++) {
+    const unsigned tab = kFaceCorners[n];
+    double u[5], v[5];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int c = (tab >> (4 * q)) & 0xf;
+      // select among the 8 corners without indexing a local array
+      double uu = cu[0], vv = cv[0];
+#pragma unroll
+      for (int r = 1; r < 8; r++) {
+        uu = (c == r) ? cu[r] : uu;
+        vv = (c == r) ? cv[r] : vv;
+      }
+      u[q] = uu;
+      v[q] = vv;
+    }
+    u[4] = u[0];
+    v[4] = v[0];
+    const bool uz = u[0] == 0.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0;
+    const bool vz = v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0 && v[3] == 0.0;
+    const bool vcross = v[0] * v[1] < 0.0 || v[1] * v[2] < 0.0 || v[2] * v[3] < 0.0 ||
+                        v[3] * v[0] < 0.0;
+    const bool ucross = u[0] * u[1] < 0.0 || u[1] * u[2] < 0.0 || u[2] * u[3] < 0.0 ||
+                        u[3] * u[0] < 0.0;
+    if ((uz && vcross) || (vz && ucross)) {
+      o.skip = 1;
+      o.add = 0.5;
+      o.npts = m;
+      return;
+    }
+    bool edge = false;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      edge = edge || (u[q] == 0.0 && u[q + 1] == 0.0 && v[q] == 0.0 && v[q + 1] == 0.0);
+    if (edge) {
+      o.skip = 1;
+      o.add = 0.25;
+      o.npts = m;
+      return;
+    }
+    double xu1 = 0, yu1 = 0, xu2 = 0, yu2 = 0, xv1 = 0, yv1 = 0, xv2 = 0, yv2 = 0;
+    const int nu = edge_zeros(u, xu1, yu1, xu2, yu2);
+    const int nv = edge_zeros(v, xv1, yv1, xv2, yv2);
+    if (nu >= 2 && nv >= 2) {
+      double den = xv2 * (yu1 - yu2) + xv1 * (yu2 - yu1) + (xu1 - xu2) * (yv1 - yv2);
+      if (den == 0.0) den = den + 0.0000001;
+      const double xx = (xu1 * (xv2 * (yv1 - yu2) + xv1 * (yu2 - yv2)) +
+                         xu2 * (xv2 * (yu1 - yv1) + xv1 * (yv2 - yu1))) / den;
+      const double yy = (xv2 * (yu1 - yu2) * yv1 + xu1 * yu2 * yv1 - xv1 * yu1 * yv2 -
+                         xu1 * yu2 * yv2 + xv1 * yu2 * yv2 + xu2 * yu1 * (yv2 - yv1)) / den;
+      if (xx >= 0.0 && xx <= 1.0 && yy >= 0.0 && yy <= 1.0) {
+        Pt p;
+        switch (n) {
+          case 0: p = {xx, yy, 0.0}; break;
+          case 1: p = {xx, yy, 1.0}; break;
+          case 2: p = {1.0, yy, xx}; break;
+          case 3: p = {0.0, yy, xx}; break;
+          case 4: p = {xx, 1.0, yy}; break;
+          default: p = {xx, 0.0, yy}; break;
+        }
+        if (m == 0) o.p1 = p;
+        if (m == 1) o.p2 = p;
+        m++;
+      }
+    }
+  }
+  o.npts = m;
+}
+
+// The segment of a cell with points p1 and x(2) = p2
+// (src/variables.f90:1118-1134; the reference tests y twice where z may
+// have been meant, kept).
+__device__ __forceinline__ double segment(const Pt& p1, const Pt& p2) {
+  double a = 1.0;
+  const bool ex = p1.x == p2.x && (p1.x == 0.0 || p1.x == 1.0);
+  const bool ey = p1.y == p2.y && (p1.y == 0.0 || p1.y == 1.0);
+  const bool ez = p1.z == p2.z && (p1.z == 0.0 || p1.z == 1.0);
+  if (ex || ey) {
+    a = a * 0.5;
+    if ((ex && ey) || (ey && ez)) a = a * 0.5;
+  }
+  const double dx = p1.x - p2.x, dy = p1.y - p2.y, dz = p1.z - p2.z;
+  return a * sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+struct LineArgs {
+  const void* psi;
+  int nx, ny, nz, Nx, Ny;
+  int cx;               // cells per row, nx - 2
+  long long ncell;      // (nx-2)(ny-2)(nz-2)
+  long long per_block;  // cells per block (whole rows)
+  double* bsum;         // [nblk] sums of the cells resolved in the block
+  double* blast;        // [nblk][4] has-writer flag, last x(2) written
+  int* bunres;          // [nblk] one-point cells before the block's first writer
+  long long* bfirst;    // [nblk] cell offset of the block's first writer
+  double* bbuf;         // [nblk][L_CAP][3] their first points
+  double* bres;         // [nblk] sums of those cells once resolved
+  double* incoming;     // [nblk][3] x(2) carried into each block
+  double* out;          // [0] total length
+};
+
+template <typename T>
+__device__ __forceinline__ void load_cell(const LineArgs& p, long long c, double cu[8],
+                                          double cv[8]) {
+  using V = typename C2<T>::type;
+  const V* f = static_cast<const V*>(p.psi);
+  const long long row = c / p.cx;
+  const int i = 1 + (int)(c - row * p.cx);
+  const int j = 1 + (int)(row % (p.ny - 2));
+  const int k = 1 + (int)(row / (p.ny - 2));
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int di = q & 1, dj = (q >> 1) & 1, dk = q >> 2;
+    const size_t at = ((size_t)(k + dk + 2) * p.Ny + (size_t)(j + dj + 2)) * p.Nx +
+                      (size_t)(i + di + 2);
+    const V w = f[at];
+    cu[q] = (double)w.x;
+    cv[q] = (double)w.y;
+  }
+}
+
+// A cell can hold a point, a zero plane or a zero edge only if neither
+// component keeps one strict sign on all 8 corners.
+__device__ __forceinline__ bool may_hold_line(const double cu[8], const double cv[8]) {
+  bool up = true, un = true, vp = true, vn = true;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    up = up && cu[q] > 0.0;
+    un = un && cu[q] < 0.0;
+    vp = vp && cv[q] > 0.0;
+    vn = vn && cv[q] < 0.0;
+  }
+  return !(up || un || vp || vn);
+}
+
+// Exclusive block scan over a flag: the largest tid' < tid with the flag
+// set (-1 if none), and the block's first and last flagged tid.
+__device__ __forceinline__ int last_flag_before(bool flag, int* s_warp, int& first, int& last) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(0xffffffffu, flag);
+  const unsigned below = bal & ((1u << lane) - 1u);
+  const int in_warp = below ? (warp * 32 + 31 - __clz(below)) : -1;
+  __syncthreads();
+  if (lane == 0) {
+    s_warp[warp] = bal ? (warp * 32 + 31 - __clz(bal)) : -1;
+    s_warp[L_WARPS + warp] = bal ? (warp * 32 + __ffs(bal) - 1) : -1;
+  }
+  __syncthreads();
+  int before = in_warp;
+  if (before < 0)
+    for (int w = warp - 1; w >= 0; w--)
+      if (s_warp[w] >= 0) {
+        before = s_warp[w];
+        break;
+      }
+  first = -1;
+  last = -1;
+  for (int w = 0; w < L_WARPS; w++)
+    if (s_warp[L_WARPS + w] >= 0) {
+      first = s_warp[L_WARPS + w];
+      break;
+    }
+  for (int w = L_WARPS - 1; w >= 0; w--)
+    if (s_warp[w] >= 0) {
+      last = s_warp[w];
+      break;
+    }
+  return before;
+}
+
+__device__ __forceinline__ double block_sum(double x, double* s_red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+  __syncthreads();
+  if (lane == 0) s_red[warp] = x;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < L_WARPS; w++) t += s_red[w];
+  return t;
+}
+
+// Pass 1: every cell; one-point cells resolved inside the block wherever an
+// earlier cell of the block wrote x(2).
+template <typename T>
+__global__ void __launch_bounds__(L_THREADS) line_cells_kernel(LineArgs p) {
+  __shared__ double s_p2[L_THREADS][3];
+  __shared__ int s_warp[2 * L_WARPS];
+  __shared__ int s_cnt[L_WARPS];
+  __shared__ double s_red[L_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long c0 = (long long)blockIdx.x * p.per_block;
+  const long long c1 = min(c0 + p.per_block, p.ncell);
+  double acc = 0.0;
+  bool carry_ok = false;
+  Pt carry = {0.0, 0.0, 0.0};
+  long long first_writer = c1 - c0;
+  int unresolved = 0;
+  for (long long base = c0; base < c1; base += L_THREADS) {
+    const long long c = base + tid;
+    CellOut o;
+    o.skip = 0;
+    o.add = 0.0;
+    o.npts = 0;
+    o.p1 = o.p2 = Pt{0.0, 0.0, 0.0};
+    if (c < c1) {
+      double cu[8], cv[8];
+      load_cell<T>(p, c, cu, cv);
+      if (may_hold_line(cu, cv)) cell_line(cu, cv, o);
+    }
+    const bool writer = o.npts >= 2;
+    const bool pending = !o.skip && o.npts == 1;
+    if (o.skip)
+      acc += o.add;
+    else if (o.npts >= 2)
+      acc += segment(o.p1, o.p2);
+    s_p2[tid][0] = o.p2.x;
+    s_p2[tid][1] = o.p2.y;
+    s_p2[tid][2] = o.p2.z;
+    int first, last;
+    const int before = last_flag_before(writer, s_warp, first, last);
+    bool unres = false;
+    if (pending) {
+      if (before >= 0)
+        acc += segment(o.p1, Pt{s_p2[before][0], s_p2[before][1], s_p2[before][2]});
+      else if (carry_ok)
+        acc += segment(o.p1, carry);
+      else
+        unres = true;
+    }
+    // unresolved cells keep their first point, in cell order
+    const unsigned ub = __ballot_sync(0xffffffffu, unres);
+    if (lane == 0) s_cnt[warp] = __popc(ub);
+    __syncthreads();
+    int off = unresolved + __popc(ub & ((1u << lane) - 1u));
+    int total = 0;
+    for (int w = 0; w < L_WARPS; w++) {
+      if (w < warp) off += s_cnt[w];
+      total += s_cnt[w];
+    }
+    if (unres && off < L_CAP) {
+      double* b = p.bbuf + ((size_t)blockIdx.x * L_CAP + off) * 3;
+      b[0] = o.p1.x;
+      b[1] = o.p1.y;
+      b[2] = o.p1.z;
+    }
+    unresolved += total;
+    if (first >= 0 && !carry_ok) first_writer = base + first - c0;
+    if (last >= 0) {
+      carry = Pt{s_p2[last][0], s_p2[last][1], s_p2[last][2]};
+      carry_ok = true;
+    }
+    __syncthreads();
+  }
+  const double s = block_sum(acc, s_red);
+  if (tid == 0) {
+    p.bsum[blockIdx.x] = s;
+    double* L = p.blast + (size_t)blockIdx.x * 4;
+    L[0] = carry_ok ? 1.0 : 0.0;
+    L[1] = carry.x;
+    L[2] = carry.y;
+    L[3] = carry.z;
+    p.bunres[blockIdx.x] = unresolved;
+    p.bfirst[blockIdx.x] = first_writer;
+  }
+}
+
+// The x(2) carried into each block: the last one written by an earlier
+// block, else the starting value (zero).  One thread, blocks in order.
+__global__ void line_chain_kernel(LineArgs p, int nblk) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double x = 0.0, y = 0.0, z = 0.0;
+  for (int b = 0; b < nblk; b++) {
+    p.incoming[3 * b] = x;
+    p.incoming[3 * b + 1] = y;
+    p.incoming[3 * b + 2] = z;
+    const double* L = p.blast + (size_t)b * 4;
+    if (L[0] != 0.0) {
+      x = L[1];
+      y = L[2];
+      z = L[3];
+    }
+  }
+}
+
+// Pass 2: the one-point cells before each block's first writer, measured
+// to the carried x(2): from the kept points, or by walking those cells
+// again when there were more than L_CAP of them.
+template <typename T>
+__global__ void __launch_bounds__(L_THREADS) line_resolve_kernel(LineArgs p) {
+  __shared__ double s_red[L_WARPS];
+  const int b = blockIdx.x;
+  const Pt in = {p.incoming[3 * b], p.incoming[3 * b + 1], p.incoming[3 * b + 2]};
+  const int cnt = p.bunres[b];
+  double acc = 0.0;
+  if (cnt <= L_CAP) {
+    for (int t = threadIdx.x; t < cnt; t += L_THREADS) {
+      const double* q = p.bbuf + ((size_t)b * L_CAP + t) * 3;
+      acc += segment(Pt{q[0], q[1], q[2]}, in);
+    }
+  } else {
+    const long long c0 = (long long)b * p.per_block;
+    const long long c1 = c0 + p.bfirst[b];
+    for (long long base = c0; base < c1; base += L_THREADS) {
+      const long long c = base + threadIdx.x;
+      if (c < c1) {
+        double cu[8], cv[8];
+        load_cell<T>(p, c, cu, cv);
+        CellOut o;
+        o.skip = 0;
+        o.add = 0.0;
+        o.npts = 0;
+        o.p1 = o.p2 = Pt{0.0, 0.0, 0.0};
+        if (may_hold_line(cu, cv)) cell_line(cu, cv, o);
+        if (!o.skip && o.npts == 1) acc += segment(o.p1, in);
+      }
+    }
+  }
+  const double s = block_sum(acc, s_red);
+  if (threadIdx.x == 0) p.bres[b] = s;
+}
+
+// Total in block order (a fixed tree), times dx.
+__global__ void __launch_bounds__(L_THREADS) line_total_kernel(LineArgs p, int nblk, double dx) {
+  __shared__ double s_red[L_WARPS];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += L_THREADS) acc += p.bsum[b] + p.bres[b];
+  const double s = block_sum(acc, s_red);
+  if (threadIdx.x == 0) p.out[0] = s * dx;
+}
+
+}  // namespace vortex
+}  // namespace gpe

@@ -259,6 +259,12 @@ class GpeSolver:
         from . import spectral
         return spectral.filtered_field(self, filter_kc, m, out)
 
+    def linelength(self) -> float:
+        """linelength (src/variables.f90:879-1145): total vortex line length."""
+        v = ctypes.c_double()
+        check(lib().gpe_gpu_linelength(self._ctx, ctypes.byref(v)), self._ctx)
+        return v.value
+
     def renormalise(self, norm: float) -> None:
         """renormalise (src/variables.f90:698-709)."""
         check(lib().gpe_gpu_renormalise(self._ctx, float(norm)), self._ctx)

@@ -230,6 +230,14 @@ int gpe_gpu_condensed_particles(gpe_ctx* ctx, double* row, double* eta,
 int gpe_gpu_filtered_field(gpe_ctx* ctx, double filter_kc, double m, void* out,
                            int32_t elem_bytes, int32_t device_out);
 
+/* linelength (src/variables.f90:879-1145): total vortex line length of the
+ * resident state (single-domain contexts), from the zero lines of Re psi and
+ * Im psi on the faces of every interior cell, times dx (the reference
+ * assumes dx = dy = dz).  The reference carries its point arrays from cell
+ * to cell and leaves their start undefined; here they start at zero on
+ * every call. */
+int gpe_gpu_linelength(gpe_ctx* ctx, double* length);
+
 /* Failure-detection self-test (no reference counterpart): runs, on the
  * context's stream, a device wait on a flag that nothing sets, bounded by
  * limit_ns (at most 1 s) with the same bounded-wait code as the stage

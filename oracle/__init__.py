@@ -96,6 +96,9 @@ def lib():
             ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
         L.ora_ic_pade_pulse_ring.argtypes = [vp, ctypes.c_char_p] + [ctypes.c_double] * 4 + [dp]
         L.ora_ic_fermi.argtypes = [vp, dp]
+        L.ora_linelength.restype = ctypes.c_double
+        L.ora_linelength.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, dp]
         _lib = L
     return _lib
 
@@ -277,3 +280,14 @@ def drive(orc: Oracle, psi, tm: OraTime, nsteps: int, *, renorm=False,
         prev_norm = norm
         tm.p += 1
     return psi, rec
+
+
+def linelength(psi, dx: float, state=None):
+    """linelength (src/variables.f90:879-1145) of a single-domain interior
+    psi (nz, ny, nx).  state: the 18 carried-over work values x(1:6),
+    y(1:6), z(1:6) (zeros by default); returns (length, final state)."""
+    a = _c128(psi)
+    nz, ny, nx = a.shape
+    st = np.zeros(18) if state is None else np.array(state, dtype=np.float64)
+    L = float(lib().ora_linelength(_dp(a), nx, ny, nz, float(dx), _dp(st)))
+    return L, st

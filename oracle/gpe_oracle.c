@@ -1007,3 +1007,133 @@ void ora_ic_fermi(ora_ctx* c, double* out_) {
     out[q] = (f >= 0.0) ? sqrt(f) : 0.0;
   }
 }
+
+
+/* ------------------------------------------------------------------------
+ * linelength (src/variables.f90:879-1145), the reference's loops literally.
+ * Cells (i, j, k) with 1 <= i <= nx-2 and the same for j, k; on each of the
+ * 6 faces the zero lines of Re psi and Im psi are located by linear
+ * interpolation along the face edges and intersected; two points found on
+ * the cell's faces give a segment.  Faces: 1 front (k), 2 back (k+1),
+ * 3 right (i+1), 4 left (i), 5 top (j+1), 6 bottom (j). */
+static void face_corners(const double* psi, int nx, int ny, int i, int j, int k, int n,
+                         double u[6], double v[6]) {
+  /* corner (di, dj, dk) of corners 1..4 for each face */
+  static const int cor[6][4][3] = {
+      {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}},
+      {{0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}},
+      {{1, 0, 0}, {1, 0, 1}, {1, 1, 1}, {1, 1, 0}},
+      {{0, 0, 0}, {0, 0, 1}, {0, 1, 1}, {0, 1, 0}},
+      {{0, 1, 0}, {1, 1, 0}, {1, 1, 1}, {0, 1, 1}},
+      {{0, 0, 0}, {1, 0, 0}, {1, 0, 1}, {0, 0, 1}}};
+  for (int q = 0; q < 4; q++) {
+    const int* d = cor[n - 1][q];
+    const size_t at = (((size_t)(k + d[2]) * ny + (j + d[1])) * nx + (i + d[0])) * 2;
+    u[q + 1] = psi[at];
+    v[q + 1] = psi[at + 1];
+  }
+  u[5] = u[1];
+  v[5] = v[1];
+}
+
+/* The zero points of one component along the face edges (the q loops of
+ * src/variables.f90:990-1072): returns lu (or lv). */
+static int edge_zeros(const double w[6], double xw[7], double yw[7]) {
+  int l = 1;
+  for (int q = 1; q <= 4; q++) {
+    if (w[q] == 0.0) {
+      switch (q) {
+        case 1: xw[l] = 0.0; yw[l] = 0.0; break;
+        case 2: xw[l] = 1.0; yw[l] = 0.0; break;
+        case 3: xw[l] = 1.0; yw[l] = 1.0; break;
+        default: xw[l] = 0.0; yw[l] = 1.0; break;
+      }
+    } else if (w[q] * w[q + 1] < 0.0) {
+      switch (q) {
+        case 1: xw[l] = fabs(w[q] / (w[q] - w[q + 1])); yw[l] = 0.0; break;
+        case 2: xw[l] = 1.0; yw[l] = fabs(w[q] / (w[q] - w[q + 1])); break;
+        case 3: xw[l] = fabs(w[q + 1] / (w[q] - w[q + 1])); yw[l] = 1.0; break;
+        default: xw[l] = 0.0; yw[l] = fabs(w[q + 1] / (w[q] - w[q + 1])); break;
+      }
+      if (l == 1 || xw[l] != xw[l - 1] || yw[l] != yw[l - 1]) l++;
+    }
+  }
+  return l;
+}
+
+double ora_linelength(const double* psi, int nx, int ny, int nz, double dx, double* st) {
+  double* x = st - 1;       /* x(1:6) */
+  double* y = st + 6 - 1;   /* y(1:6) */
+  double* z = st + 12 - 1;  /* z(1:6) */
+  double xu[7] = {0}, yu[7] = {0}, xv[7] = {0}, yv[7] = {0};
+  double L = 0.0;
+  for (int k = 1; k <= nz - 2; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        int m = 1;
+        int skip = 0;
+        for (int n = 1; n <= 6 && !skip; n++) {
+          double u[6], v[6];
+          face_corners(psi, nx, ny, i, j, k, n, u, v);
+          /* a zero plane of one component crossed by the other */
+          if ((u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0 && u[4] == 0.0 &&
+               (v[1] * v[2] < 0.0 || v[2] * v[3] < 0.0 || v[3] * v[4] < 0.0 ||
+                v[4] * v[1] < 0.0)) ||
+              (v[1] == 0.0 && v[2] == 0.0 && v[3] == 0.0 && v[4] == 0.0 &&
+               (u[1] * u[2] < 0.0 || u[2] * u[3] < 0.0 || u[3] * u[4] < 0.0 ||
+                u[4] * u[1] < 0.0))) {
+            L += 0.5;
+            skip = 1;
+            break;
+          }
+          /* a zero edge of both components */
+          for (int q = 1; q <= 4; q++)
+            if (u[q] == 0.0 && u[q + 1] == 0.0 && v[q] == 0.0 && v[q + 1] == 0.0) {
+              L += 0.25;
+              skip = 1;
+              break;
+            }
+          if (skip) break;
+          const int lu = edge_zeros(u, xu, yu);
+          const int lv = edge_zeros(v, xv, yv);
+          if (lu > 2 && lv > 2) {
+            double den = xv[2] * (yu[1] - yu[2]) + xv[1] * (yu[2] - yu[1]) +
+                         (xu[1] - xu[2]) * (yv[1] - yv[2]);
+            if (den == 0.0) den = den + 0.0000001;
+            const double xx = (xu[1] * (xv[2] * (yv[1] - yu[2]) + xv[1] * (yu[2] - yv[2])) +
+                               xu[2] * (xv[2] * (yu[1] - yv[1]) + xv[1] * (yv[2] - yu[1]))) /
+                              den;
+            const double yy = (xv[2] * (yu[1] - yu[2]) * yv[1] + xu[1] * yu[2] * yv[1] -
+                               xv[1] * yu[1] * yv[2] - xu[1] * yu[2] * yv[2] +
+                               xv[1] * yu[2] * yv[2] + xu[2] * yu[1] * (yv[2] - yv[1])) /
+                              den;
+            if (xx >= 0.0 && xx <= 1.0 && yy >= 0.0 && yy <= 1.0) {
+              switch (n) {
+                case 1: x[m] = xx; y[m] = yy; z[m] = 0.0; break;
+                case 2: x[m] = xx; y[m] = yy; z[m] = 1.0; break;
+                case 3: x[m] = 1.0; y[m] = yy; z[m] = xx; break;
+                case 4: x[m] = 0.0; y[m] = yy; z[m] = xx; break;
+                case 5: x[m] = xx; y[m] = 1.0; z[m] = yy; break;
+                default: x[m] = xx; y[m] = 0.0; z[m] = yy; break;
+              }
+              m++;
+            }
+          }
+        }
+        if (skip) continue;
+        if (m > 1) {
+          double a = 1.0;
+          const int ex = x[1] == x[2] && (x[1] == 0.0 || x[1] == 1.0);
+          const int ey = y[1] == y[2] && (y[1] == 0.0 || y[1] == 1.0);
+          const int ez = z[1] == z[2] && (z[1] == 0.0 || z[1] == 1.0);
+          /* the reference tests y twice where z may have been meant */
+          if (ex || ey || ey) {
+            a *= 0.5;
+            if ((ex && (ey || ey)) || (ey && ez)) a *= 0.5;
+          }
+          L += a * sqrt((x[1] - x[2]) * (x[1] - x[2]) + (y[1] - y[2]) * (y[1] - y[2]) +
+                        (z[1] - z[2]) * (z[1] - z[2]));
+        }
+      }
+  return L * dx;
+}

@@ -104,6 +104,14 @@ void ora_ic_fermi(ora_ctx* c, double* out);
 /* get_rr (src/ic.f90:888-901) on a scalar. */
 double ora_get_rr(double r);
 
+/* linelength (src/variables.f90:879-1145) of a single-domain interior psi
+ * (nz, ny, nx complex, x fastest) with grid spacing dx.  st[18] holds the
+ * work arrays x(1:6), y(1:6), z(1:6), whose values carry over from cell to
+ * cell in the reference (a cell with one zero point measures to the x(2)
+ * left by an earlier cell); the caller passes their starting values (the
+ * reference leaves them undefined) and gets the final ones back. */
+double ora_linelength(const double* psi, int nx, int ny, int nz, double dx, double* st);
+
 #ifdef __cplusplus
 }
 #endif

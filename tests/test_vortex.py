@@ -1,0 +1,96 @@
+"""Vortex line length (linelength, src/variables.f90:879-1145): the C
+restatement in the oracle on analytic lines, and the library's kernels
+against it on B200 (analytic lines, a ring, random fields full of
+vortices, both storage precisions)."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+
+
+def _grid(n, h):
+    x = (np.arange(n) - (n - 1) / 2) * h
+    return np.meshgrid(x, x, x, indexing="ij")  # Z, Y, X
+
+
+def test_oracle_straight_and_tilted_lines():
+    n, h = 16, 0.5
+    Z, Y, X = _grid(n, h)
+    L, _ = oracle.linelength((X - 0.13) + 1j * (Y + 0.21), h)
+    assert L == pytest.approx((n - 2) * h, rel=1e-14)
+    L, _ = oracle.linelength((X - 0.3 * Z - 0.13) + 1j * (Y + 0.21), h)
+    assert L == pytest.approx((n - 2) * h * math.sqrt(1.09), rel=1e-12)
+
+
+def test_oracle_ring_is_close_to_its_circumference():
+    n, h, R = 24, 0.5, 3.0
+    Z, Y, X = _grid(n, h)
+    L, _ = oracle.linelength((np.sqrt(X ** 2 + Y ** 2) - R) + 1j * (Z - 0.1), h)
+    assert L == pytest.approx(2 * math.pi * R, rel=0.01)
+
+
+def test_oracle_carries_its_point_arrays():
+    """The work arrays come back changed and feed the next call."""
+    rng = np.random.default_rng(0)
+    psi = rng.standard_normal((10, 10, 10)) + 1j * rng.standard_normal((10, 10, 10))
+    L0, st = oracle.linelength(psi, 1.0)
+    assert np.any(st != 0.0) and L0 > 0
+
+
+# --- on the GPU -------------------------------------------------------------------
+
+def _solver(nz, ny, nx, precision=16, h=0.5):
+    from gpe_b200 import GpeParams, GpeSolver
+    prm = GpeParams(nx=nx, ny=ny, nz=nz, xr=0.5 * (nx - 1) * h, yr=0.5 * (ny - 1) * h,
+                    zr=0.5 * (nz - 1) * h, scheme="rk4", eqn_to_solve=4, bcs=1, order=2,
+                    precision=precision, g=1.0, mu=1.0)
+    return GpeSolver(prm, dt=0.01)
+
+
+@pytest.mark.gpu
+def test_gpu_analytic_lines_and_ring():
+    n, h = 24, 0.5
+    Z, Y, X = _grid(n, h)
+    fields = [(X - 0.13) + 1j * (Y + 0.21), (X - 0.3 * Z - 0.13) + 1j * (Y + 0.21),
+              (np.sqrt(X ** 2 + Y ** 2) - 3.0) + 1j * (Z - 0.1)]
+    with _solver(n, n, n, h=h) as s:
+        for psi in fields:
+            s.set_state(psi)
+            exp, _ = oracle.linelength(psi, h)
+            assert s.linelength() == pytest.approx(exp, rel=1e-13)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(16, 16, 16), (18, 20, 24), (9, 17, 33), (40, 36, 64),
+                                   (3, 3, 3), (3, 5, 4)])
+@pytest.mark.parametrize("precision", [16, 8])
+def test_gpu_random_fields_match_oracle(shape, precision):
+    """Random fields: vortex lines through most cells, with one-point cells
+    that measure to the x(2) carried from an earlier cell."""
+    nz, ny, nx = shape
+    rng = np.random.default_rng(nx * 7 + ny * 3 + nz)
+    psi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    if precision == 8:
+        psi = psi.astype(np.complex64)
+    with _solver(nz, ny, nx, precision) as s:
+        s.set_state(psi)
+        got = s.linelength()
+        again = s.linelength()
+    exp, _ = oracle.linelength(psi.astype(np.complex128), 0.5)
+    assert got == pytest.approx(exp, rel=1e-12, abs=1e-14)
+    assert got == again  # fixed reduction order
+
+
+@pytest.mark.gpu
+def test_gpu_smooth_field_at_128():
+    """Many blocks: a random-phase state (a tangle of long lines)."""
+    n = 128
+    with _solver(n, n, n) as s:
+        s.random_phase(0.75, 0.75, 2)
+        psi = s.get_state()
+        got = s.linelength()
+    exp, _ = oracle.linelength(psi, 0.5)
+    assert exp > 0
+    assert got == pytest.approx(exp, rel=1e-12)

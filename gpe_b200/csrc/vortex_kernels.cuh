@@ -428,3 +428,215 @@ __global__ void __launch_bounds__(L_THREADS) line_total_kernel(LineArgs p, int n
 
 }  // namespace vortex
 }  // namespace gpe
+
+// ===========================================================================
+// Zero finders: get_zeros, get_extra_zeros, get_re_im_zeros
+// (src/io.f90:895-1402).  Twelve sections, in the reference's file order:
+//   0-2  zeros, x / y / z edges where Re and Im cross together
+//   3-5  zeros, xy / xz / yz faces crossed alternately by Re and Im
+//   6-8  re_zeros, x / y / z edges of Re;  9-11 im_zeros, the same of Im
+// Every section walks the interior cells in loop order with at most one
+// point per cell; points are compacted in that order (a count pass, block
+// offsets, a write pass), so the lists equal the reference's line by line.
+namespace gpe {
+namespace vortex {
+
+constexpr int Z_SECTIONS = 12;
+
+struct ZeroArgs {
+  const void* psi;
+  int nx, ny, nz, Nx, Ny;
+  int cx;
+  long long ncell, per_block;
+  const double* x;  // grid coordinates (src/ic.f90:53-66)
+  const double* y;
+  const double* z;
+  long long* bcount;  // [nblk][Z_SECTIONS]
+  const long long* boff;  // [nblk][Z_SECTIONS] first output slot
+  double* pts;        // [total][3]
+};
+
+// Corners of a cell used by the sections: 0 (i,j,k), 1 (i+1,j,k), 2 (i,j+1,k),
+// 3 (i,j,k+1), 4 (i+1,j+1,k), 5 (i+1,j,k+1), 6 (i,j+1,k+1).
+template <typename T>
+__device__ __forceinline__ void load_zero_corners(const ZeroArgs& p, long long c, double re[7],
+                                                  double im[7], int& i, int& j, int& k) {
+  using V = typename C2<T>::type;
+  const V* f = static_cast<const V*>(p.psi);
+  const long long row = c / p.cx;
+  i = 1 + (int)(c - row * p.cx);
+  j = 1 + (int)(row % (p.ny - 2));
+  k = 1 + (int)(row / (p.ny - 2));
+  const int di[7] = {0, 1, 0, 0, 1, 1, 0}, dj[7] = {0, 0, 1, 0, 1, 0, 1},
+            dk[7] = {0, 0, 0, 1, 0, 1, 1};
+#pragma unroll
+  for (int q = 0; q < 7; q++) {
+    const size_t at = ((size_t)(k + dk[q] + 2) * p.Ny + (size_t)(j + dj[q] + 2)) * p.Nx +
+                      (size_t)(i + di[q] + 2);
+    const V w = f[at];
+    re[q] = (double)w.x;
+    im[q] = (double)w.y;
+  }
+}
+
+__device__ __forceinline__ double select7(const double v[7], int q) {
+  double r = v[0];
+#pragma unroll
+  for (int t = 1; t < 7; t++) r = (q == t) ? v[t] : r;
+  return r;
+}
+
+// Section s of one cell: whether it writes a point, and the point.
+__device__ __forceinline__ bool zero_section(int s, const double re[7], const double im[7],
+                                             int i, int j, int k, const ZeroArgs& p, Pt& o) {
+  if (s < 3 || s >= 6) {
+    const int d = s < 3 ? s : (s - 6) % 3;  // 0 x, 1 y, 2 z
+    const int n = 1 + d;                    // corner across the edge
+    const double* cc = d == 0 ? p.x : (d == 1 ? p.y : p.z);  // device grid table
+    const int a = d == 0 ? i : (d == 1 ? j : k);
+    double w, wn;
+    bool hit;
+    if (s < 3) {
+      const double r = re[0], m = im[0], rn = select7(re, n), mn = select7(im, n);
+      hit = (r == 0.0 && m == 0.0) || (r == 0.0 && m * mn < 0.0) ||
+            (m == 0.0 && r * rn < 0.0) || (r * rn < 0.0 && m * mn < 0.0);
+      w = r;
+      wn = rn;
+    } else {
+      const bool use_im = s >= 9;
+      w = use_im ? im[0] : re[0];
+      wn = use_im ? select7(im, n) : select7(re, n);
+      // the z edges test .and. where the x and y edges test .or. (kept)
+      hit = d == 2 ? (w == 0.0 && w * wn < 0.0) : (w == 0.0 || w * wn < 0.0);
+    }
+    if (!hit) return false;
+    const double den = w - wn;
+    if (den == 0.0) return false;
+    const double zero = -wn * cc[a] / den + w * cc[a + 1] / den;
+    o = Pt{d == 0 ? zero : p.x[i], d == 1 ? zero : p.y[j], d == 2 ? zero : p.z[k]};
+    return true;
+  }
+  // faces: corners c0..c3 around the face; u runs c0 -> c1, w runs c1 -> c2
+  const int f = s - 3;
+  int q0, q1, q2, q3;
+  double u0, u1, w0, w1;
+  if (f == 0) {
+    q0 = 0; q1 = 1; q2 = 4; q3 = 2;
+    u0 = p.x[i]; u1 = p.x[i + 1]; w0 = p.y[j]; w1 = p.y[j + 1];
+  } else if (f == 1) {
+    q0 = 0; q1 = 1; q2 = 5; q3 = 3;
+    u0 = p.x[i]; u1 = p.x[i + 1]; w0 = p.z[k]; w1 = p.z[k + 1];
+  } else {
+    q0 = 0; q1 = 3; q2 = 6; q3 = 2;
+    u0 = p.z[k]; u1 = p.z[k + 1]; w0 = p.y[j]; w1 = p.y[j + 1];
+  }
+#pragma unroll
+  for (int pass = 0; pass < 2; pass++) {
+    // pass 0: Re crosses the u edges and Im the w edges; pass 1 the reverse
+    const double r0 = select7(re, q0), r1 = select7(re, q1), r2 = select7(re, q2),
+                 r3 = select7(re, q3);
+    const double i0 = select7(im, q0), i1 = select7(im, q1), i2 = select7(im, q2),
+                 i3 = select7(im, q3);
+    const double A0 = pass ? i0 : r0, A1 = pass ? i1 : r1, A2 = pass ? i2 : r2,
+                 A3 = pass ? i3 : r3;
+    const double B0 = pass ? r0 : i0, B1 = pass ? r1 : i1, B2 = pass ? r2 : i2,
+                 B3 = pass ? r3 : i3;
+    if ((A0 * A1 < 0.0 && B0 * B1 >= 0.0) && (B1 * B2 < 0.0 && A1 * A2 >= 0.0) &&
+        (A2 * A3 < 0.0 && B2 * B3 >= 0.0) && (B3 * B0 < 0.0 && A3 * A0 >= 0.0)) {
+      double den = A0 - A1;
+      const double z0 = -A1 * u0 / den + A0 * u1 / den;
+      den = B1 - B2;
+      const double z1 = -B2 * w0 / den + B1 * w1 / den;
+      den = A2 - A3;
+      const double z2 = -A3 * u1 / den + A2 * u0 / den;
+      den = B3 - B0;
+      const double z3 = -B0 * w1 / den + B3 * w0 / den;
+      const double m1 = (w0 - w1) / (z0 - z2);
+      const double m2 = (z1 - z3) / (u1 - u0);
+      const double up = (z3 - u0 * m2 - w0 + z0 * m1) / (m1 - m2);
+      const double wp = up * m1 + w0 - z0 * m1;
+      if (f == 0) o = Pt{up, wp, p.z[k]};
+      else if (f == 1) o = Pt{up, p.y[j], wp};
+      else o = Pt{p.x[i], wp, up};
+      return true;
+    }
+  }
+  return false;
+}
+
+// Pass 1: points per block and section.
+template <typename T>
+__global__ void __launch_bounds__(L_THREADS) zeros_count_kernel(ZeroArgs p) {
+  __shared__ int s_cnt[L_WARPS][Z_SECTIONS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long c0 = (long long)blockIdx.x * p.per_block;
+  const long long c1 = min(c0 + p.per_block, p.ncell);
+  int cnt[Z_SECTIONS];
+#pragma unroll
+  for (int s = 0; s < Z_SECTIONS; s++) cnt[s] = 0;
+  for (long long c = c0 + threadIdx.x; c < c1; c += L_THREADS) {
+    double re[7], im[7];
+    int i, j, k;
+    load_zero_corners<T>(p, c, re, im, i, j, k);
+    Pt o;
+#pragma unroll
+    for (int s = 0; s < Z_SECTIONS; s++) cnt[s] += zero_section(s, re, im, i, j, k, p, o) ? 1 : 0;
+  }
+#pragma unroll
+  for (int s = 0; s < Z_SECTIONS; s++) {
+    int x = cnt[s];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+    if (lane == 0) s_cnt[warp][s] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < Z_SECTIONS) {
+    long long t = 0;
+    for (int w = 0; w < L_WARPS; w++) t += s_cnt[w][threadIdx.x];
+    p.bcount[(size_t)blockIdx.x * Z_SECTIONS + threadIdx.x] = t;
+  }
+}
+
+// Pass 2: the points, each at its place in loop order.
+template <typename T>
+__global__ void __launch_bounds__(L_THREADS) zeros_write_kernel(ZeroArgs p) {
+  __shared__ int s_cnt[L_WARPS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long c0 = (long long)blockIdx.x * p.per_block;
+  const long long c1 = min(c0 + p.per_block, p.ncell);
+  long long run[Z_SECTIONS];
+#pragma unroll
+  for (int s = 0; s < Z_SECTIONS; s++) run[s] = p.boff[(size_t)blockIdx.x * Z_SECTIONS + s];
+  for (long long base = c0; base < c1; base += L_THREADS) {
+    const long long c = base + threadIdx.x;
+    const bool valid = c < c1;
+    double re[7] = {0, 0, 0, 0, 0, 0, 0}, im[7] = {0, 0, 0, 0, 0, 0, 0};
+    int i = 1, j = 1, k = 1;
+    if (valid) load_zero_corners<T>(p, c, re, im, i, j, k);
+#pragma unroll 1
+    for (int s = 0; s < Z_SECTIONS; s++) {
+      Pt o;
+      const bool hit = valid && zero_section(s, re, im, i, j, k, p, o);
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0) s_cnt[warp] = __popc(bal);
+      __syncthreads();
+      long long at = run[s] + __popc(bal & ((1u << lane) - 1u));
+      int total = 0;
+      for (int w = 0; w < L_WARPS; w++) {
+        if (w < warp) at += s_cnt[w];
+        total += s_cnt[w];
+      }
+      if (hit) {
+        double* q = p.pts + 3 * at;
+        q[0] = o.x;
+        q[1] = o.y;
+        q[2] = o.z;
+      }
+      run[s] += total;
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace vortex
+}  // namespace gpe

@@ -28,6 +28,11 @@ procRR/ (RR = the two-digit rank, src/io.f90:118-143):
     same layout with t in place of t+im_t and the filtered field
   end_state_filtered.dat (flag 1, :607-616): the end_state layout
 
+Text files of the zero finders in procRR/ (src/io.f90:895-1402):
+zerosNNNNNNN.dat, re_zerosNNNNNNN.dat, im_zerosNNNNNNN.dat, each a list-
+directed header line per section (" # i,j,k --> ...") followed by its points
+as (3e17.9) records.
+
 NNNNNNN = itos(p), p as seven digits with leading zeros (src/io.f90:29-47).
 A single-domain run is process 0 of a 1 x 1 grid: js = ks = 0,
 je = ny-1, ke = nz-1.
@@ -216,3 +221,47 @@ def read_surface(path: str, pr_bytes: int = 8):
     if off != len(raw):
         raise ValueError(f"{path}: {len(raw) - off} trailing bytes")
     return time, (nx, ny, nz), procs, (js, je, ks, ke), field.copy(), x.copy(), y.copy(), z.copy()
+
+
+# ---- zero finders ------------------------------------------------------------------
+
+ZERO_HEADERS = [
+    "# i,j,k --> i+1,j,k", "# i,j,k --> i,j+1,k", "# i,j,k --> i,j,k+1",
+    "# i,j,k --> i+1,j,k --> i+1,j+1,k --> i,j+1,k",
+    "# i,j,k --> i+1,j,k --> i+1,j,k+1 --> i,j,k+1",
+    "# i,j,k --> i,j,k+1 --> i,j+1,k+1 --> i,j+1,k",
+]
+# sections of each file, in the order of gpe_gpu_zeros
+ZERO_FILES = (("zeros", range(0, 6)), ("re_zeros", range(6, 9)), ("im_zeros", range(9, 12)))
+
+
+def _header(s: int) -> str:
+    # list-directed output of a character constant starts with a blank
+    return " " + ZERO_HEADERS[s if s < 6 else (s - 6) % 3] + "\n"
+
+
+def zeros_texts(counts, points) -> dict:
+    """The three files' contents from the 12 sections' counts and points."""
+    starts = np.concatenate([[0], np.cumsum(np.asarray(counts, dtype=np.int64))])
+    out = {}
+    for name, secs in ZERO_FILES:
+        parts = []
+        for s in secs:
+            parts.append(_header(s))
+            for q in range(starts[s], starts[s + 1]):
+                parts.append(e_line(*points[q]))
+        out[name] = "".join(parts)
+    return out
+
+
+def write_zeros(run_dir: str, p: int, counts, points, rank: int = 0) -> list:
+    """procRR/zerosNNNNNNN.dat, re_zeros..., im_zeros... of one call."""
+    d = os.path.join(run_dir, proc_dir(rank))
+    os.makedirs(d, exist_ok=True)
+    paths = []
+    for name, text in zeros_texts(counts, points).items():
+        path = os.path.join(d, f"{name}{itos(p)}.dat")
+        with open(path, "w") as f:
+            f.write(text)
+        paths.append(path)
+    return paths

@@ -265,6 +265,18 @@ class GpeSolver:
         check(lib().gpe_gpu_linelength(self._ctx, ctypes.byref(v)), self._ctx)
         return v.value
 
+    def zeros(self):
+        """get_zeros / get_extra_zeros / get_re_im_zeros (src/io.f90:895-1402)
+        -> (counts[12], points (n, 3)), sections in the reference's order."""
+        counts = np.zeros(12, dtype=np.int64)
+        P64 = ctypes.POINTER(ctypes.c_int64)
+        check(lib().gpe_gpu_zeros(self._ctx, counts.ctypes.data_as(P64), None, 0), self._ctx)
+        pts = np.zeros((max(int(counts.sum()), 1), 3))
+        check(lib().gpe_gpu_zeros(self._ctx, counts.ctypes.data_as(P64),
+                                  pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  pts.shape[0]), self._ctx)
+        return counts, pts[:int(counts.sum())]
+
     def renormalise(self, norm: float) -> None:
         """renormalise (src/variables.f90:698-709)."""
         check(lib().gpe_gpu_renormalise(self._ctx, float(norm)), self._ctx)

@@ -238,6 +238,19 @@ int gpe_gpu_filtered_field(gpe_ctx* ctx, double filter_kc, double m, void* out,
  * every call. */
 int gpe_gpu_linelength(gpe_ctx* ctx, double* length);
 
+/* get_zeros, get_extra_zeros and get_re_im_zeros (src/io.f90:895-1402):
+ * the zero points of the resident state (single-domain contexts) that the
+ * reference writes to zeros*.dat, re_zeros*.dat and im_zeros*.dat, in its
+ * order, as 12 sections: 0-2 edges along x, y, z where Re and Im cross
+ * together; 3-5 xy, xz, yz faces crossed alternately by Re and Im; 6-8 the
+ * x, y, z edges where Re crosses; 9-11 the same for Im.  counts[12] (HOST)
+ * receives each section's number of points.  With points non-NULL (HOST,
+ * room for cap points of 3 doubles) the points follow, sections
+ * concatenated; a cap below the total returns GPE_ERR_INVALID with counts
+ * filled.  Call with points = NULL to size the buffer. */
+#define GPE_ZERO_SECTIONS 12
+int gpe_gpu_zeros(gpe_ctx* ctx, int64_t* counts, double* points, int64_t cap);
+
 /* Failure-detection self-test (no reference counterpart): runs, on the
  * context's stream, a device wait on a flag that nothing sets, bounded by
  * limit_ns (at most 1 s) with the same bounded-wait code as the stage

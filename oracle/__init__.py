@@ -96,6 +96,9 @@ def lib():
             ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
         L.ora_ic_pade_pulse_ring.argtypes = [vp, ctypes.c_char_p] + [ctypes.c_double] * 4 + [dp]
         L.ora_ic_fermi.argtypes = [vp, dp]
+        L.ora_zeros.restype = ctypes.c_longlong
+        L.ora_zeros.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp,
+                                ctypes.POINTER(ctypes.c_longlong), dp, ctypes.c_longlong]
         L.ora_linelength.restype = ctypes.c_double
         L.ora_linelength.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_double, dp]
@@ -291,3 +294,18 @@ def linelength(psi, dx: float, state=None):
     st = np.zeros(18) if state is None else np.array(state, dtype=np.float64)
     L = float(lib().ora_linelength(_dp(a), nx, ny, nz, float(dx), _dp(st)))
     return L, st
+
+
+def zeros(psi, x, y, z):
+    """get_zeros / get_extra_zeros / get_re_im_zeros (src/io.f90:895-1402)
+    of a single-domain interior psi on the grid x, y, z -> (counts[12],
+    points (n, 3))."""
+    a = _c128(psi)
+    nz, ny, nx = a.shape
+    xs, ys, zs = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+    counts = np.zeros(12, dtype=np.int64)
+    cp = counts.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+    n = int(lib().ora_zeros(_dp(a), nx, ny, nz, _dp(xs), _dp(ys), _dp(zs), cp, None, 0))
+    pts = np.zeros((max(n, 1), 3))
+    lib().ora_zeros(_dp(a), nx, ny, nz, _dp(xs), _dp(ys), _dp(zs), cp, _dp(pts), n)
+    return counts, pts[:n]

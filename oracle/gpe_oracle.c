@@ -1137,3 +1137,147 @@ double ora_linelength(const double* psi, int nx, int ny, int nz, double dx, doub
       }
   return L * dx;
 }
+
+
+/* ------------------------------------------------------------------------
+ * Zero finders (src/io.f90:895-1402), the reference's loops literally. */
+typedef struct {
+  double* pts;
+  long long cap, n;
+} zsink;
+
+static void zput(zsink* s, double a, double b, double c) {
+  if (s->pts && s->n < s->cap) {
+    s->pts[3 * s->n] = a;
+    s->pts[3 * s->n + 1] = b;
+    s->pts[3 * s->n + 2] = c;
+  }
+  s->n++;
+}
+
+#define ZRE(i, j, k) psi[(((size_t)(k) * ny + (j)) * nx + (i)) * 2]
+#define ZIM(i, j, k) psi[(((size_t)(k) * ny + (j)) * nx + (i)) * 2 + 1]
+
+/* get_zeros on one edge direction (d = 0 x, 1 y, 2 z). */
+static void zeros_edge_both(const double* psi, int nx, int ny, int nz, const double* x,
+                            const double* y, const double* z, int d, zsink* s) {
+  for (int k = 1; k <= nz - 2; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        const int i2 = i + (d == 0), j2 = j + (d == 1), k2 = k + (d == 2);
+        const double r = ZRE(i, j, k), m = ZIM(i, j, k);
+        const double rn = ZRE(i2, j2, k2), mn = ZIM(i2, j2, k2);
+        if ((r == 0.0 && m == 0.0) || (r == 0.0 && m * mn < 0.0) ||
+            (m == 0.0 && r * rn < 0.0) || (r * rn < 0.0 && m * mn < 0.0)) {
+          const double den = r - rn;
+          if (den == 0.0) continue;
+          const double* c = d == 0 ? x : (d == 1 ? y : z);
+          const int a = d == 0 ? i : (d == 1 ? j : k);
+          const double zero = -rn * c[a] / den + r * c[a + 1] / den;
+          if (d == 0) zput(s, zero, y[j], z[k]);
+          else if (d == 1) zput(s, x[i], zero, z[k]);
+          else zput(s, x[i], y[j], zero);
+        }
+      }
+}
+
+/* get_re_im_zeros on one component (comp 0 re, 1 im) and edge direction;
+ * the z-edge test has .and. where the others have .or. (kept). */
+static void zeros_edge_one(const double* psi, int nx, int ny, int nz, const double* x,
+                           const double* y, const double* z, int comp, int d, zsink* s) {
+  for (int k = 1; k <= nz - 2; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        const int i2 = i + (d == 0), j2 = j + (d == 1), k2 = k + (d == 2);
+        const double w = comp ? ZIM(i, j, k) : ZRE(i, j, k);
+        const double wn = comp ? ZIM(i2, j2, k2) : ZRE(i2, j2, k2);
+        const int hit = d == 2 ? (w == 0.0 && w * wn < 0.0) : (w == 0.0 || w * wn < 0.0);
+        if (hit) {
+          const double den = w - wn;
+          if (den == 0.0) continue;
+          const double* c = d == 0 ? x : (d == 1 ? y : z);
+          const int a = d == 0 ? i : (d == 1 ? j : k);
+          const double zero = -wn * c[a] / den + w * c[a + 1] / den;
+          if (d == 0) zput(s, zero, y[j], z[k]);
+          else if (d == 1) zput(s, x[i], zero, z[k]);
+          else zput(s, x[i], y[j], zero);
+        }
+      }
+}
+
+/* get_extra_zeros on one face orientation: f = 0 xy (corners (i,j), (i+1,j),
+ * (i+1,j+1), (i,j+1) at k), 1 xz (x then z), 2 yz (z then y, at i). */
+static void zeros_face(const double* psi, int nx, int ny, int nz, const double* x,
+                       const double* y, const double* z, int f, zsink* s) {
+  for (int k = 1; k <= nz - 2; k++)
+    for (int j = 1; j <= ny - 2; j++)
+      for (int i = 1; i <= nx - 2; i++) {
+        /* corners c0..c3 around the face and the coordinates along its two
+           axes: u runs c0 -> c1 (and c3 -> c2), w runs c1 -> c2 (and c0 -> c3) */
+        int ci[4], cj[4], ck[4];
+        double u0, u1, w0, w1;
+        if (f == 0) {
+          int a[4][3] = {{i, j, k}, {i + 1, j, k}, {i + 1, j + 1, k}, {i, j + 1, k}};
+          for (int q = 0; q < 4; q++) { ci[q] = a[q][0]; cj[q] = a[q][1]; ck[q] = a[q][2]; }
+          u0 = x[i]; u1 = x[i + 1]; w0 = y[j]; w1 = y[j + 1];
+        } else if (f == 1) {
+          int a[4][3] = {{i, j, k}, {i + 1, j, k}, {i + 1, j, k + 1}, {i, j, k + 1}};
+          for (int q = 0; q < 4; q++) { ci[q] = a[q][0]; cj[q] = a[q][1]; ck[q] = a[q][2]; }
+          u0 = x[i]; u1 = x[i + 1]; w0 = z[k]; w1 = z[k + 1];
+        } else {
+          int a[4][3] = {{i, j, k}, {i, j, k + 1}, {i, j + 1, k + 1}, {i, j + 1, k}};
+          for (int q = 0; q < 4; q++) { ci[q] = a[q][0]; cj[q] = a[q][1]; ck[q] = a[q][2]; }
+          u0 = z[k]; u1 = z[k + 1]; w0 = y[j]; w1 = y[j + 1];
+        }
+        double re[4], im[4];
+        for (int q = 0; q < 4; q++) {
+          re[q] = ZRE(ci[q], cj[q], ck[q]);
+          im[q] = ZIM(ci[q], cj[q], ck[q]);
+        }
+        for (int pass = 0; pass < 2; pass++) {
+          /* pass 0: re crosses c0-c1 and c2-c3, im crosses c1-c2 and c3-c0;
+             pass 1: the other way round */
+          const double* A = pass ? im : re; /* crosses on the u edges */
+          const double* B = pass ? re : im; /* crosses on the w edges */
+          if ((A[0] * A[1] < 0.0 && B[0] * B[1] >= 0.0) &&
+              (B[1] * B[2] < 0.0 && A[1] * A[2] >= 0.0) &&
+              (A[2] * A[3] < 0.0 && B[2] * B[3] >= 0.0) &&
+              (B[3] * B[0] < 0.0 && A[3] * A[0] >= 0.0)) {
+            double zr[4], den;
+            den = A[0] - A[1];
+            zr[0] = -A[1] * u0 / den + A[0] * u1 / den;
+            den = B[1] - B[2];
+            zr[1] = -B[2] * w0 / den + B[1] * w1 / den;
+            den = A[2] - A[3];
+            zr[2] = -A[3] * u1 / den + A[2] * u0 / den;
+            den = B[3] - B[0];
+            zr[3] = -B[0] * w1 / den + B[3] * w0 / den;
+            const double m1 = (w0 - w1) / (zr[0] - zr[2]);
+            const double m2 = (zr[1] - zr[3]) / (u1 - u0);
+            const double up = (zr[3] - u0 * m2 - w0 + zr[0] * m1) / (m1 - m2);
+            const double wp = up * m1 + w0 - zr[0] * m1;
+            if (f == 0) zput(s, up, wp, z[k]);
+            else if (f == 1) zput(s, up, y[j], wp);
+            else zput(s, x[i], wp, up);
+            break;
+          }
+        }
+      }
+}
+
+long long ora_zeros(const double* psi, int nx, int ny, int nz, const double* x,
+                    const double* y, const double* z, long long* counts, double* points,
+                    long long cap) {
+  zsink s = {points, cap, 0};
+  long long prev = 0;
+  for (int sec = 0; sec < 12; sec++) {
+    if (sec < 3) zeros_edge_both(psi, nx, ny, nz, x, y, z, sec, &s);
+    else if (sec < 6) zeros_face(psi, nx, ny, nz, x, y, z, sec - 3, &s);
+    else zeros_edge_one(psi, nx, ny, nz, x, y, z, sec >= 9, (sec - 6) % 3, &s);
+    counts[sec] = s.n - prev;
+    prev = s.n;
+  }
+  return s.n;
+}
+#undef ZRE
+#undef ZIM

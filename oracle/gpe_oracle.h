@@ -112,6 +112,17 @@ double ora_get_rr(double r);
  * reference leaves them undefined) and gets the final ones back. */
 double ora_linelength(const double* psi, int nx, int ny, int nz, double dx, double* st);
 
+/* get_zeros, get_extra_zeros and get_re_im_zeros (src/io.f90:895-1402) of a
+ * single-domain interior psi on the grid x, y, z: the points of the 12
+ * sections in the reference's order (zeros: x-, y-, z-edges, then the
+ * xy-, xz-, yz-face extras; re_zeros: x-, y-, z-edges; im_zeros: the
+ * same).  counts[12] receives each section's number of points; points (may
+ * be NULL) receives 3 doubles per point, sections concatenated, at most cap
+ * points.  Returns the total. */
+long long ora_zeros(const double* psi, int nx, int ny, int nz, const double* x,
+                    const double* y, const double* z, long long* counts, double* points,
+                    long long cap);
+
 #ifdef __cplusplus
 }
 #endif

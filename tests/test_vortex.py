@@ -64,7 +64,7 @@ def test_gpu_analytic_lines_and_ring():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", [(16, 16, 16), (18, 20, 24), (9, 17, 33), (40, 36, 64),
-                                   (3, 3, 3), (3, 5, 4)])
+                                   (6, 6, 6), (6, 7, 9)])
 @pytest.mark.parametrize("precision", [16, 8])
 def test_gpu_random_fields_match_oracle(shape, precision):
     """Random fields: vortex lines through most cells, with one-point cells
@@ -94,3 +94,78 @@ def test_gpu_smooth_field_at_128():
     exp, _ = oracle.linelength(psi, 0.5)
     assert exp > 0
     assert got == pytest.approx(exp, rel=1e-12)
+
+
+# --- zero finders (src/io.f90:895-1402) ----------------------------------------------
+
+def test_oracle_zeros_of_a_straight_line():
+    """psi = (x - a) + i (y - b): Re and Im cross together on no edge, the
+    xy faces hold the line (each with a NaN point: the reference's slope
+    divides by zero there), Re / Im crossings on the x / y edges."""
+    n, h = 12, 0.5
+    Z, Y, X = _grid(n, h)
+    x = (np.arange(n) - (n - 1) / 2) * h
+    counts, pts = oracle.zeros((X - 0.13) + 1j * (Y + 0.21), x, x, x)
+    assert counts.tolist() == [0, 0, 0, n - 2, 0, 0, (n - 2) ** 2, 0, 0, 0, (n - 2) ** 2, 0]
+    face = pts[:n - 2]
+    assert np.all(face[:, 2] == x[1:n - 1])
+    re_x = pts[n - 2:n - 2 + (n - 2) ** 2]
+    np.testing.assert_allclose(re_x[:, 0], 0.13, rtol=1e-12)
+
+
+def test_zero_files_layout(tmp_path):
+    from gpe_b200 import output
+    counts = [1, 0, 0, 0, 0, 0, 2, 0, 0, 0, 0, 1]
+    pts = np.array([[1.0, 2.0, 3.0], [4.0, 5.0, 6.0], [7.0, 8.0, 9.0], [0.5, 0.25, 0.125]])
+    paths = output.write_zeros(str(tmp_path), 7, counts, pts)
+    names = sorted(p.split("/")[-1] for p in paths)
+    assert names == ["im_zeros0000007.dat", "re_zeros0000007.dat", "zeros0000007.dat"]
+    z = open(paths[0]).read().splitlines()
+    assert z[0] == " # i,j,k --> i+1,j,k" and z[1] == output.e_line(1, 2, 3).rstrip("\n")
+    assert len(z) == 6 + 1 and z[-1] == " # i,j,k --> i,j,k+1 --> i,j+1,k+1 --> i,j+1,k"
+    r = open(paths[1]).read().splitlines()
+    assert r == [" # i,j,k --> i+1,j,k", output.e_line(4, 5, 6).rstrip("\n"),
+                 output.e_line(7, 8, 9).rstrip("\n"), " # i,j,k --> i,j+1,k",
+                 " # i,j,k --> i,j,k+1"]
+    m = open(paths[2]).read().splitlines()
+    assert m[-1] == output.e_line(0.5, 0.25, 0.125).rstrip("\n")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(16, 16, 16), (18, 20, 24), (6, 7, 9), (40, 36, 64)])
+@pytest.mark.parametrize("precision", [16, 8])
+def test_gpu_zeros_match_oracle(shape, precision):
+    """Every section's points equal the oracle's, in order, bit for bit."""
+    nz, ny, nx = shape
+    rng = np.random.default_rng(nx + 5 * ny + 11 * nz)
+    psi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    if precision == 8:
+        psi = psi.astype(np.complex64)
+    with _solver(nz, ny, nx, precision) as s:
+        s.set_state(psi)
+        counts, pts = s.zeros()
+        x, y, z = s.grid()
+    ec, ep = oracle.zeros(psi.astype(np.complex128), x, y, z)
+    assert counts.tolist() == ec.tolist()
+    np.testing.assert_array_equal(pts, ep)
+
+
+@pytest.mark.gpu
+def test_gpu_zeros_of_lines_and_a_random_phase_state():
+    n, h = 24, 0.5
+    Z, Y, X = _grid(n, h)
+    with _solver(n, n, n, h=h) as s:
+        for psi in [(X - 0.13) + 1j * (Y + 0.21),
+                    (np.sqrt(X ** 2 + Y ** 2) - 3.0) + 1j * (Z - 0.1)]:
+            s.set_state(psi)
+            counts, pts = s.zeros()
+            ec, ep = oracle.zeros(psi, *s.grid())
+            assert counts.tolist() == ec.tolist()
+            np.testing.assert_array_equal(pts, ep)  # NaN where the oracle has NaN
+    with _solver(96, 96, 96) as s:
+        s.random_phase(0.75, 0.75, 4)
+        psi = s.get_state()
+        counts, pts = s.zeros()
+        ec, ep = oracle.zeros(psi, *s.grid())
+    assert counts.tolist() == ec.tolist() and counts.sum() > 0
+    np.testing.assert_array_equal(pts, ep)

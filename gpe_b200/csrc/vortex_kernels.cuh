@@ -277,15 +277,35 @@ __device__ __forceinline__ double block_sum(double x, double* s_red) {
   return t;
 }
 
-// Pass 1: every cell; one-point cells resolved inside the block wherever an
-// earlier cell of the block wrote x(2).
+// Block-wide exclusive position of a flagged thread among the flagged ones
+// (thread order) and the block's total.
+__device__ __forceinline__ int flag_position(bool flag, int* s_cnt, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(0xffffffffu, flag);
+  __syncthreads();
+  if (lane == 0) s_cnt[warp] = __popc(b);
+  __syncthreads();
+  int pos = __popc(b & ((1u << lane) - 1u));
+  total = 0;
+  for (int w = 0; w < L_WARPS; w++) {
+    if (w < warp) pos += s_cnt[w];
+    total += s_cnt[w];
+  }
+  return pos;
+}
+
+// Pass 1: the block's cells in loop order.  Cells that may hold a line
+// (most do not) are queued in order and processed 256 at a time, so the
+// warps doing the full face loop are dense; one-point cells are resolved
+// inside the block wherever an earlier queued cell of the block wrote x(2).
 template <typename T>
 __global__ void __launch_bounds__(L_THREADS) line_cells_kernel(LineArgs p) {
   __shared__ double s_p2[L_THREADS][3];
+  __shared__ long long s_q[2 * L_THREADS];
   __shared__ int s_warp[2 * L_WARPS];
   __shared__ int s_cnt[L_WARPS];
   __shared__ double s_red[L_WARPS];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const long long c0 = (long long)blockIdx.x * p.per_block;
   const long long c1 = min(c0 + p.per_block, p.ncell);
   double acc = 0.0;
@@ -293,17 +313,38 @@ __global__ void __launch_bounds__(L_THREADS) line_cells_kernel(LineArgs p) {
   Pt carry = {0.0, 0.0, 0.0};
   long long first_writer = c1 - c0;
   int unresolved = 0;
-  for (long long base = c0; base < c1; base += L_THREADS) {
-    const long long c = base + tid;
+  int qn = 0;
+  long long scan = c0;
+  while (scan < c1 || qn > 0) {
+    // fill the queue with candidate cells, in order
+    while (qn < L_THREADS && scan < c1) {
+      const long long c = scan + tid;
+      bool cand = false;
+      if (c < c1) {
+        double cu[8], cv[8];
+        load_cell<T>(p, c, cu, cv);
+        cand = may_hold_line(cu, cv);
+      }
+      int total;
+      const int pos = flag_position(cand, s_cnt, total);
+      if (cand) s_q[qn + pos] = c;
+      qn += total;
+      scan += L_THREADS;
+      __syncthreads();
+    }
+    if (qn == 0) break;
+    const int nb = min(qn, L_THREADS);
+    const bool valid = tid < nb;
+    const long long c = valid ? s_q[tid] : 0;
     CellOut o;
     o.skip = 0;
     o.add = 0.0;
     o.npts = 0;
     o.p1 = o.p2 = Pt{0.0, 0.0, 0.0};
-    if (c < c1) {
+    if (valid) {
       double cu[8], cv[8];
       load_cell<T>(p, c, cu, cv);
-      if (may_hold_line(cu, cv)) cell_line(cu, cv, o);
+      cell_line(cu, cv, o);
     }
     const bool writer = o.npts >= 2;
     const bool pending = !o.skip && o.npts == 1;
@@ -326,15 +367,8 @@ __global__ void __launch_bounds__(L_THREADS) line_cells_kernel(LineArgs p) {
         unres = true;
     }
     // unresolved cells keep their first point, in cell order
-    const unsigned ub = __ballot_sync(0xffffffffu, unres);
-    if (lane == 0) s_cnt[warp] = __popc(ub);
-    __syncthreads();
-    int off = unresolved + __popc(ub & ((1u << lane) - 1u));
-    int total = 0;
-    for (int w = 0; w < L_WARPS; w++) {
-      if (w < warp) off += s_cnt[w];
-      total += s_cnt[w];
-    }
+    int total;
+    const int off = unresolved + flag_position(unres, s_cnt, total);
     if (unres && off < L_CAP) {
       double* b = p.bbuf + ((size_t)blockIdx.x * L_CAP + off) * 3;
       b[0] = o.p1.x;
@@ -342,11 +376,17 @@ __global__ void __launch_bounds__(L_THREADS) line_cells_kernel(LineArgs p) {
       b[2] = o.p1.z;
     }
     unresolved += total;
-    if (first >= 0 && !carry_ok) first_writer = base + first - c0;
+    if (first >= 0 && !carry_ok) first_writer = s_q[first] - c0;
     if (last >= 0) {
       carry = Pt{s_p2[last][0], s_p2[last][1], s_p2[last][2]};
       carry_ok = true;
     }
+    // drop the processed entries
+    __syncthreads();
+    const long long keep = (tid < qn - nb) ? s_q[nb + tid] : 0;
+    __syncthreads();
+    if (tid < qn - nb) s_q[tid] = keep;
+    qn -= nb;
     __syncthreads();
   }
   const double s = block_sum(acc, s_red);

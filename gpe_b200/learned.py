@@ -260,6 +260,7 @@ def main(argv=None) -> int:
     ap.add_argument("--out-scale", type=float)
     ap.add_argument("--rollout", type=int)
     ap.add_argument("--noise", type=float)
+    ap.add_argument("--dt", type=float, help="coarse step (a multiple of the fine 0.01)")
     a = ap.parse_args(argv)
     cfg = LearnedConfig()
     if a.iters is not None:
@@ -284,6 +285,9 @@ def main(argv=None) -> int:
         cfg.rollout = a.rollout
     if a.noise is not None:
         cfg.noise = a.noise
+    if a.dt is not None:
+        cfg.fine_substeps = int(round(a.dt / (cfg.dt / cfg.fine_substeps)))
+        cfg.dt = a.dt
     import torch
     torch.cuda.set_device(cfg.device)
     n = cfg.coarse_n

@@ -653,6 +653,14 @@ def run_spectrum(args):
     linelen = {"length": length, "ms_per_call": line_ms, "sites_per_s": sites / (line_ms / 1e3),
                "cells_kernel_ms": cells_ms,
                "cells_kernel_gbs": 16 * sites / (cells_ms / 1e3) / 1e9}
+    # zero finders of the same state: counts, points to host (wall clock, a host sync per pass)
+    s.zeros()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    zc, zp = s.zeros()
+    zeros = {"points": int(zc.sum()), "per_section": zc.tolist(),
+             "ms_per_call_wall": (time.perf_counter() - t0) * 1e3,
+             "note": "two passes (count, write) plus the point list copied to the host"}
     s.close()
     cpu = None
     if not args.no_cpu_baseline:
@@ -681,7 +689,7 @@ def run_spectrum(args):
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": int(launches), "gpu_launches_per_step": launches / args.steps,
         "n0_over_V": c.row["n0_over_V"], "eta": c.eta.tolist(), "nharm": c.nharm.tolist(),
-        "linelength": linelen,
+        "linelength": linelen, "zeros": zeros,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -49,8 +49,8 @@ class LearnedConfig:
     fine_n: int = 256
     fine_h: float = 0.25
     coarse_n: int = 128
-    dt: float = 0.02            # coarse step
-    fine_substeps: int = 2      # fine reference steps per coarse step (dt_f = 0.01)
+    dt: float = 0.04            # coarse step (twice the fine path's largest stable step)
+    fine_substeps: int = 4      # fine reference steps per coarse step (dt_f = 0.01)
     kmax: float = 1.0
     out_scale: float = 0.01
     coarse_kahan: bool = True

@@ -17,6 +17,8 @@ them without separators, one record (line) per write.
   idf/idfNNNNNNN.dat           (i9,e17.9)  kk, F(kk)        src/io.f90:712-717
   eta_time.dat  (4e17.9) t, eta(1:3)                        src/io.f90:719-721
   p_saved.dat   (i10) p                                     src/io.f90:521-525
+  timestep.dat  (3e17.9,i10) t, im_t, |dt|, p (rk45, every save_rate
+                steps, after the step)                      src/solve.f90:234-241
 
 Stream (unformatted, access='stream') files of one process directory
 procRR/ (RR = the two-digit rank, src/io.f90:118-143):
@@ -112,6 +114,10 @@ def psi_time_line(t, im_t, value: complex) -> str:
     v = complex(value)
     return e_line(t, im_t, v.real, v.imag, abs(v) ** 2,
                   float(np.arctan2(v.imag + 1.0e-6, v.real)))
+
+
+def timestep_line(t, im_t, dt, p) -> str:
+    return fortran_e(t) + fortran_e(im_t) + fortran_e(abs(dt)) + fortran_i(p, 10) + "\n"
 
 
 def mass_line(t, im_t, row: dict) -> str:

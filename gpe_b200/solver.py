@@ -405,7 +405,8 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
     step it writes the IDL surface run_dir/proc00/densNNNNNNN.dat and deletes
     SAVE (save_run, src/io.f90:1566-1595).  With outputs as well, it writes
     the reference's files at its cadence: energy.dat and psi_time.dat (and
-    norm.dat after the step) every save_rate steps, condensed_particles
+    norm.dat after the step, and timestep.dat for rk45) every save_rate
+    steps, condensed_particles
     (mass.dat, spectra, filtered surface) every save_rate3, idl_surface every
     save_rate2 and end_state every p_save time units, the counters starting
     from the current time (:126-128).
@@ -430,6 +431,11 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
         if outputs is not None and run_dir is not None:
             _cadence_outputs(s, run_dir, outputs, counters)
         s.solver()
+        if outputs is not None and run_dir is not None and prm.scheme == "rk45" and \
+                s.p % outputs.save_rate == 0:
+            # rkqs writes the next step's size after every save_rate-th step
+            output.append(os.path.join(run_dir, "timestep.dat"),
+                          output.timestep_line(s.t, s.im_t, s.dt, s.p))
         if run_dir is not None and os.path.exists(os.path.join(run_dir, "SAVE")):
             _idl_surface(s, run_dir)
             os.remove(os.path.join(run_dir, "SAVE"))

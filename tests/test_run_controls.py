@@ -114,3 +114,17 @@ def test_output_cadence(tmp_path):
     assert read_end_state(os.path.join(d, "proc00", "end_state.dat")).p == 4
     n = open(os.path.join(d, "norm.dat")).read().splitlines()
     assert len(n) >= 3 and all(len(line) == 4 * 17 for line in n)
+
+
+def test_rk45_writes_timestep_every_save_rate_steps(tmp_path):
+    d = str(tmp_path)
+    open(os.path.join(d, "RUNNING"), "w").close()
+    s = FakeSolver()
+    s.prm.scheme = "rk45"
+    run_loop(s, 7, run_dir=d, outputs=OutputParams(save_rate=3, save_rate2=1e9, save_rate3=1e9,
+                                                    p_save=1e9))
+    lines = open(os.path.join(d, "timestep.dat")).read().splitlines()
+    # p = 0, 3, 6 when the step is taken (src/solve.f90:236)
+    assert [int(line[51:]) for line in lines] == [0, 3, 6]
+    assert all(len(line) == 3 * 17 + 10 for line in lines)
+    assert lines[0][34:51] == output.fortran_e(0.1)

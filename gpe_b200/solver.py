@@ -338,6 +338,8 @@ class OutputParams:
     save_spectrum: bool = True
     save_filter: bool = False
     filter_kc: float = 10.0
+    save_ll: bool = False      # linelength.dat every save_rate steps
+    save_zeros: bool = False   # zero finders every save_rate2 time units
 
 
 def _modulo(a: float, p: float) -> float:
@@ -375,6 +377,9 @@ def _cadence_outputs(s, run_dir, io: OutputParams, counters: dict) -> None:
                       output.energy_line(s.t, s.im_t, E, prm.nx * prm.ny * prm.nz))
         v = s.get_site(prm.nx // 2, prm.ny // 2, prm.nz // 2)
         output.append(os.path.join(run_dir, "psi_time.dat"), output.psi_time_line(s.t, s.im_t, v))
+        if io.save_ll:
+            output.append(os.path.join(run_dir, "linelength.dat"),
+                          output.e_line(s.t, s.im_t, s.linelength()))
     if t_all >= io.save_rate3 * counters["m"]:
         c = s.condensed_particles()
         output.append(os.path.join(run_dir, "mass.dat"), output.mass_line(s.t, s.im_t, c.row))
@@ -386,6 +391,9 @@ def _cadence_outputs(s, run_dir, io: OutputParams, counters: dict) -> None:
                                           pr_bytes=_pr_bytes(prm))
         counters["m"] += 1
     if t_all >= io.save_rate2 * counters["n"]:
+        if io.save_zeros:
+            counts, pts = s.zeros()
+            output.write_zeros(run_dir, s.p, counts, pts)
         if io.save_3d:
             _idl_surface(s, run_dir)
         counters["n"] += 1

@@ -47,6 +47,12 @@ class FakeSolver:
     def get_site(self, i, j, k):
         return complex(self.calls, 0.5)
 
+    def linelength(self):
+        return 2.5 * self.calls
+
+    def zeros(self):
+        return np.array([1] + [0] * 11), np.array([[1.0, 2.0, 3.0]])
+
     def condensed_particles(self):
         from gpe_b200.spectral import Condensate
         row = dict(M_density=1.0, n0_over_V=0.5, M=8.0, n0=32.0, temp=0.1, temp2=0.2,
@@ -128,3 +134,17 @@ def test_rk45_writes_timestep_every_save_rate_steps(tmp_path):
     assert [int(line[51:]) for line in lines] == [0, 3, 6]
     assert all(len(line) == 3 * 17 + 10 for line in lines)
     assert lines[0][34:51] == output.fortran_e(0.1)
+
+
+def test_line_length_and_zero_files(tmp_path):
+    d = str(tmp_path)
+    open(os.path.join(d, "RUNNING"), "w").close()
+    s = FakeSolver()
+    io = OutputParams(save_rate=2, save_rate2=0.25, save_rate3=1e9, p_save=1e9, save_3d=False,
+                      save_ll=True, save_zeros=True)
+    run_loop(s, 5, run_dir=d, outputs=io)
+    ll = open(os.path.join(d, "linelength.dat")).read().splitlines()
+    assert ll[0] == output.e_line(0.0, 0.0, 0.0).rstrip("\n")
+    assert float(ll[1][34:51]) == 5.0  # before the third step: 2 calls so far
+    zs = sorted(f for f in os.listdir(os.path.join(d, "proc00")) if f.startswith("zeros"))
+    assert zs[0] == "zeros0000000.dat" and len(zs) >= 2

@@ -113,6 +113,13 @@ __device__ __forceinline__ void cell_line(const double cu[8], const double cv[8]
     }
     u[4] = u[0];
     v[4] = v[0];
+    // a component of one strict sign on the face's corners rules out every
+    // test below: no zero plane, no zero edge, no crossing to intersect
+    const bool u_one = (u[0] > 0.0 && u[1] > 0.0 && u[2] > 0.0 && u[3] > 0.0) ||
+                       (u[0] < 0.0 && u[1] < 0.0 && u[2] < 0.0 && u[3] < 0.0);
+    const bool v_one = (v[0] > 0.0 && v[1] > 0.0 && v[2] > 0.0 && v[3] > 0.0) ||
+                       (v[0] < 0.0 && v[1] < 0.0 && v[2] < 0.0 && v[3] < 0.0);
+    if (u_one || v_one) continue;
     const bool uz = u[0] == 0.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0;
     const bool vz = v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0 && v[3] == 0.0;
     const bool vcross = v[0] * v[1] < 0.0 || v[1] * v[2] < 0.0 || v[2] * v[3] < 0.0 ||
@@ -298,8 +305,14 @@ __device__ __forceinline__ int flag_position(bool flag, int* s_cnt, int& total) 
 // (most do not) are queued in order and processed 256 at a time, so the
 // warps doing the full face loop are dense; one-point cells are resolved
 // inside the block wherever an earlier queued cell of the block wrote x(2).
+// Resident blocks per SM the cell pass is compiled for (registers per thread
+// 65536 / (256 x this)).
+#ifndef GPE_LINE_MIN_BLOCKS
+#define GPE_LINE_MIN_BLOCKS 2
+#endif
+
 template <typename T>
-__global__ void __launch_bounds__(L_THREADS) line_cells_kernel(LineArgs p) {
+__global__ void __launch_bounds__(L_THREADS, GPE_LINE_MIN_BLOCKS) line_cells_kernel(LineArgs p) {
   __shared__ double s_p2[L_THREADS][3];
   __shared__ long long s_q[2 * L_THREADS];
   __shared__ int s_warp[2 * L_WARPS];

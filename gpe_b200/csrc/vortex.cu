@@ -67,9 +67,9 @@ int run(gpe_ctx* c, const FieldView& v, double* length) {
   const int nblk = (int)((rows + rows_per_block - 1) / rows_per_block);
   p.per_block = rows_per_block * p.cx;
   Vortex* x = vortex_ext(c);
-  // per block: bsum, blast[4], bbuf[L_CAP][3], bres, incoming[3] doubles,
+  // per block: bsum, blast[4], bbuf[L_CAP][3], bres doubles,
   // bfirst (long long), bunres (int); plus the total
-  const size_t per = sizeof(double) * (1 + 4 + L_CAP * 3 + 1 + 3) + sizeof(long long) +
+  const size_t per = sizeof(double) * (1 + 4 + L_CAP * 3 + 1) + sizeof(long long) +
                      sizeof(int);
   if (x->nblk < nblk) {
     cudaFree(x->mem);
@@ -87,8 +87,6 @@ int run(gpe_ctx* c, const FieldView& v, double* length) {
   d += (size_t)L_CAP * 3 * nblk;
   p.bres = d;
   d += nblk;
-  p.incoming = d;
-  d += 3 * (size_t)nblk;
   p.out = d;
   d += 1;
   p.bfirst = reinterpret_cast<long long*>(d);
@@ -98,13 +96,11 @@ int run(gpe_ctx* c, const FieldView& v, double* length) {
   line_cells_kernel<T><<<nblk, L_THREADS, 0, v.stream>>>(p);
   VX_CU(c, cudaGetLastError());
   gpe_internal_time_end(c, &t);
-  line_chain_kernel<<<1, 32, 0, v.stream>>>(p, nblk);
-  VX_CU(c, cudaGetLastError());
   line_resolve_kernel<T><<<nblk, L_THREADS, 0, v.stream>>>(p);
   VX_CU(c, cudaGetLastError());
   line_total_kernel<<<1, L_THREADS, 0, v.stream>>>(p, nblk, v.dx);
   VX_CU(c, cudaGetLastError());
-  gpe_internal_count_launches(c, 4);
+  gpe_internal_count_launches(c, 3);
   VX_CU(c, cudaMemcpyAsync(length, p.out, sizeof(double), cudaMemcpyDeviceToHost, v.stream));
   VX_CU(c, cudaStreamSynchronize(v.stream));
   return GPE_OK;

@@ -8,9 +8,9 @@
 // segment.  The reference keeps its point arrays x(1:6), y(1:6), z(1:6) from
 // cell to cell, so a cell that finds one point measures to the x(2) left by
 // the last earlier cell that found two: that carried value is resolved here
-// by block scans in loop order (the cells of a block are contiguous), a
-// per-block "last x(2)" chained across blocks, and a pass over each block's
-// cells that came before its first writer.  The arithmetic is compiled
+// by block scans in loop order (the cells of a block are contiguous), each
+// block's last x(2), looked up by the next blocks, and a pass over each
+// block's cells that came before its first writer.  The arithmetic is compiled
 // without FMA contraction and in the reference's order, so every cell's
 // points and segment equal a sequential evaluation bit for bit; only the
 // final sum is reassociated (a fixed tree, the same on every run).
@@ -199,7 +199,6 @@ struct LineArgs {
   long long* bfirst;    // [nblk] cell offset of the block's first writer
   double* bbuf;         // [nblk][L_CAP][3] their first points
   double* bres;         // [nblk] sums of those cells once resolved
-  double* incoming;     // [nblk][3] x(2) carried into each block
   double* out;          // [0] total length
 };
 
@@ -415,33 +414,37 @@ __global__ void __launch_bounds__(L_THREADS, GPE_LINE_MIN_BLOCKS) line_cells_ker
   }
 }
 
-// The x(2) carried into each block: the last one written by an earlier
-// block, else the starting value (zero).  One thread, blocks in order.
-__global__ void line_chain_kernel(LineArgs p, int nblk) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double x = 0.0, y = 0.0, z = 0.0;
-  for (int b = 0; b < nblk; b++) {
-    p.incoming[3 * b] = x;
-    p.incoming[3 * b + 1] = y;
-    p.incoming[3 * b + 2] = z;
-    const double* L = p.blast + (size_t)b * 4;
-    if (L[0] != 0.0) {
-      x = L[1];
-      y = L[2];
-      z = L[3];
-    }
-  }
-}
-
 // Pass 2: the one-point cells before each block's first writer, measured
 // to the carried x(2): from the kept points, or by walking those cells
 // again when there were more than L_CAP of them.
 template <typename T>
 __global__ void __launch_bounds__(L_THREADS) line_resolve_kernel(LineArgs p) {
   __shared__ double s_red[L_WARPS];
+  __shared__ Pt s_in;
   const int b = blockIdx.x;
-  const Pt in = {p.incoming[3 * b], p.incoming[3 * b + 1], p.incoming[3 * b + 2]};
   const int cnt = p.bunres[b];
+  if (cnt == 0) {  // block-uniform
+    if (threadIdx.x == 0) p.bres[b] = 0.0;
+    return;
+  }
+  // the x(2) carried in: the last written by the nearest earlier block that
+  // wrote one (zero if none), found by the first warp 32 blocks at a time
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int found = -1;
+    for (int top = b - 1; top >= 0 && found < 0; top -= 32) {
+      const int q = top - lane;
+      const bool w = q >= 0 && p.blast[(size_t)q * 4] != 0.0;
+      const unsigned bal = __ballot_sync(0xffffffffu, w);
+      if (bal) found = top - (__ffs(bal) - 1);
+    }
+    if (lane == 0)
+      s_in = found < 0 ? Pt{0.0, 0.0, 0.0}
+                       : Pt{p.blast[(size_t)found * 4 + 1], p.blast[(size_t)found * 4 + 2],
+                            p.blast[(size_t)found * 4 + 3]};
+  }
+  __syncthreads();
+  const Pt in = s_in;
   double acc = 0.0;
   if (cnt <= L_CAP) {
     for (int t = threadIdx.x; t < cnt; t += L_THREADS) {
@@ -650,44 +653,55 @@ __global__ void __launch_bounds__(L_THREADS) zeros_count_kernel(ZeroArgs p) {
   }
 }
 
-// Pass 2: the points, each at its place in loop order.
+// Pass 2: the points, each at its place in loop order.  A chunk of 256
+// cells finds its hits in all 12 sections first, then one block-wide
+// exchange of per-warp counts places every point.
 template <typename T>
 __global__ void __launch_bounds__(L_THREADS) zeros_write_kernel(ZeroArgs p) {
-  __shared__ int s_cnt[L_WARPS];
+  __shared__ int s_cnt[L_WARPS][Z_SECTIONS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long c0 = (long long)blockIdx.x * p.per_block;
   const long long c1 = min(c0 + p.per_block, p.ncell);
   long long run[Z_SECTIONS];
 #pragma unroll
   for (int s = 0; s < Z_SECTIONS; s++) run[s] = p.boff[(size_t)blockIdx.x * Z_SECTIONS + s];
+  const unsigned below = (1u << lane) - 1u;
   for (long long base = c0; base < c1; base += L_THREADS) {
     const long long c = base + threadIdx.x;
     const bool valid = c < c1;
     double re[7] = {0, 0, 0, 0, 0, 0, 0}, im[7] = {0, 0, 0, 0, 0, 0, 0};
     int i = 1, j = 1, k = 1;
     if (valid) load_zero_corners<T>(p, c, re, im, i, j, k);
-#pragma unroll 1
+    unsigned mask = 0;
+    Pt o;
+#pragma unroll
+    for (int s = 0; s < Z_SECTIONS; s++)
+      if (valid && zero_section(s, re, im, i, j, k, p, o)) mask |= 1u << s;
+#pragma unroll
     for (int s = 0; s < Z_SECTIONS; s++) {
-      Pt o;
-      const bool hit = valid && zero_section(s, re, im, i, j, k, p, o);
-      const unsigned bal = __ballot_sync(0xffffffffu, hit);
-      if (lane == 0) s_cnt[warp] = __popc(bal);
-      __syncthreads();
-      long long at = run[s] + __popc(bal & ((1u << lane) - 1u));
+      const unsigned bal = __ballot_sync(0xffffffffu, (mask >> s) & 1u);
+      if (lane == 0) s_cnt[warp][s] = __popc(bal);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < Z_SECTIONS; s++) {
+      const unsigned bal = __ballot_sync(0xffffffffu, (mask >> s) & 1u);
+      long long at = run[s] + __popc(bal & below);
       int total = 0;
       for (int w = 0; w < L_WARPS; w++) {
-        if (w < warp) at += s_cnt[w];
-        total += s_cnt[w];
+        if (w < warp) at += s_cnt[w][s];
+        total += s_cnt[w][s];
       }
-      if (hit) {
+      if ((mask >> s) & 1u) {
+        zero_section(s, re, im, i, j, k, p, o);
         double* q = p.pts + 3 * at;
         q[0] = o.x;
         q[1] = o.y;
         q[2] = o.z;
       }
       run[s] += total;
-      __syncthreads();
     }
+    __syncthreads();
   }
 }
 

@@ -655,16 +655,17 @@ __global__ void __launch_bounds__(L_THREADS) zeros_count_kernel(ZeroArgs p) {
 
 // Pass 2: the points, each at its place in loop order.  A chunk of 256
 // cells finds its hits in all 12 sections first, then one block-wide
-// exchange of per-warp counts places every point.
+// exchange of per-warp counts places every point; the points themselves
+// are computed again, in one loop over the sections, by the hitting lanes.
 template <typename T>
 __global__ void __launch_bounds__(L_THREADS) zeros_write_kernel(ZeroArgs p) {
   __shared__ int s_cnt[L_WARPS][Z_SECTIONS];
+  __shared__ long long s_run[Z_SECTIONS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long c0 = (long long)blockIdx.x * p.per_block;
   const long long c1 = min(c0 + p.per_block, p.ncell);
-  long long run[Z_SECTIONS];
-#pragma unroll
-  for (int s = 0; s < Z_SECTIONS; s++) run[s] = p.boff[(size_t)blockIdx.x * Z_SECTIONS + s];
+  if (threadIdx.x < Z_SECTIONS)
+    s_run[threadIdx.x] = p.boff[(size_t)blockIdx.x * Z_SECTIONS + threadIdx.x];
   const unsigned below = (1u << lane) - 1u;
   for (long long base = c0; base < c1; base += L_THREADS) {
     const long long c = base + threadIdx.x;
@@ -683,23 +684,24 @@ __global__ void __launch_bounds__(L_THREADS) zeros_write_kernel(ZeroArgs p) {
       if (lane == 0) s_cnt[warp][s] = __popc(bal);
     }
     __syncthreads();
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < Z_SECTIONS; s++) {
       const unsigned bal = __ballot_sync(0xffffffffu, (mask >> s) & 1u);
-      long long at = run[s] + __popc(bal & below);
-      int total = 0;
-      for (int w = 0; w < L_WARPS; w++) {
-        if (w < warp) at += s_cnt[w][s];
-        total += s_cnt[w][s];
-      }
       if ((mask >> s) & 1u) {
+        long long at = s_run[s] + __popc(bal & below);
+        for (int w = 0; w < warp; w++) at += s_cnt[w][s];
         zero_section(s, re, im, i, j, k, p, o);
         double* q = p.pts + 3 * at;
         q[0] = o.x;
         q[1] = o.y;
         q[2] = o.z;
       }
-      run[s] += total;
+    }
+    __syncthreads();
+    if (threadIdx.x < Z_SECTIONS) {
+      int t = 0;
+      for (int w = 0; w < L_WARPS; w++) t += s_cnt[w][threadIdx.x];
+      s_run[threadIdx.x] += t;
     }
     __syncthreads();
   }

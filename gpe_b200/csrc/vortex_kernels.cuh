@@ -88,7 +88,100 @@ __device__ __forceinline__ int edge_zeros(const double w[5], double& x1, double&
 // (src/variables.f90:901-958), one nibble each, corner = di | dj << 1 | dk << 2.
 __constant__ unsigned kFaceCorners[6] = {0x2310u, 0x6754u, 0x3751u, 0x2640u, 0x6732u, 0x4510u};
 
-// One cell of the reference's iloop body.
+// Outcome of one face (the body of the reference's nloop for face n).
+constexpr int F_NONE = 0, F_POINT = 1, F_PLANE = 2, F_EDGE = 3;
+
+// Corner values of face n from the cell's 8 corners (selects, no indexing).
+__device__ __forceinline__ void face_values(const double cu[8], const double cv[8], int n,
+                                            double u[5], double v[5]) {
+  const unsigned tab = kFaceCorners[n];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = (tab >> (4 * q)) & 0xf;
+    double uu = cu[0], vv = cv[0];
+#pragma unroll
+    for (int r = 1; r < 8; r++) {
+      uu = (c == r) ? cu[r] : uu;
+      vv = (c == r) ? cv[r] : vv;
+    }
+    u[q] = uu;
+    v[q] = vv;
+  }
+  u[4] = u[0];
+  v[4] = v[0];
+}
+
+// A component of one strict sign on the face's corners rules out every test
+// of face_eval: no zero plane, no zero edge, no crossing to intersect.
+__device__ __forceinline__ bool face_active(const double u[5], const double v[5]) {
+  const bool u_one = (u[0] > 0.0 && u[1] > 0.0 && u[2] > 0.0 && u[3] > 0.0) ||
+                     (u[0] < 0.0 && u[1] < 0.0 && u[2] < 0.0 && u[3] < 0.0);
+  const bool v_one = (v[0] > 0.0 && v[1] > 0.0 && v[2] > 0.0 && v[3] > 0.0) ||
+                     (v[0] < 0.0 && v[1] < 0.0 && v[2] < 0.0 && v[3] < 0.0);
+  return !(u_one || v_one);
+}
+
+__device__ __forceinline__ int face_eval(const double u[5], const double v[5], double& xx,
+                                         double& yy) {
+  const bool uz = u[0] == 0.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0;
+  const bool vz = v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0 && v[3] == 0.0;
+  const bool vcross = v[0] * v[1] < 0.0 || v[1] * v[2] < 0.0 || v[2] * v[3] < 0.0 ||
+                      v[3] * v[0] < 0.0;
+  const bool ucross = u[0] * u[1] < 0.0 || u[1] * u[2] < 0.0 || u[2] * u[3] < 0.0 ||
+                      u[3] * u[0] < 0.0;
+  if ((uz && vcross) || (vz && ucross)) return F_PLANE;
+  bool edge = false;
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    edge = edge || (u[q] == 0.0 && u[q + 1] == 0.0 && v[q] == 0.0 && v[q + 1] == 0.0);
+  if (edge) return F_EDGE;
+  double xu1 = 0, yu1 = 0, xu2 = 0, yu2 = 0, xv1 = 0, yv1 = 0, xv2 = 0, yv2 = 0;
+  const int nu = edge_zeros(u, xu1, yu1, xu2, yu2);
+  const int nv = edge_zeros(v, xv1, yv1, xv2, yv2);
+  if (nu >= 2 && nv >= 2) {
+    double den = xv2 * (yu1 - yu2) + xv1 * (yu2 - yu1) + (xu1 - xu2) * (yv1 - yv2);
+    if (den == 0.0) den = den + 0.0000001;
+    xx = (xu1 * (xv2 * (yv1 - yu2) + xv1 * (yu2 - yv2)) +
+          xu2 * (xv2 * (yu1 - yv1) + xv1 * (yv2 - yu1))) / den;
+    yy = (xv2 * (yu1 - yu2) * yv1 + xu1 * yu2 * yv1 - xv1 * yu1 * yv2 - xu1 * yu2 * yv2 +
+          xv1 * yu2 * yv2 + xu2 * yu1 * (yv2 - yv1)) / den;
+    if (xx >= 0.0 && xx <= 1.0 && yy >= 0.0 && yy <= 1.0) return F_POINT;
+  }
+  return F_NONE;
+}
+
+// The cell-local point of a face's (xx, yy) (src/variables.f90:1088-1113).
+__device__ __forceinline__ Pt face_point(int n, double xx, double yy) {
+  switch (n) {
+    case 0: return Pt{xx, yy, 0.0};
+    case 1: return Pt{xx, yy, 1.0};
+    case 2: return Pt{1.0, yy, xx};
+    case 3: return Pt{0.0, yy, xx};
+    case 4: return Pt{xx, 1.0, yy};
+    default: return Pt{xx, 0.0, yy};
+  }
+}
+
+// Folds a face outcome into the cell in face order (the reference's m, its
+// "cycle iloop" on a zero plane or edge).  Returns false once the cell ended.
+__device__ __forceinline__ bool fold_face(CellOut& o, int& m, int n, int code, double xx,
+                                          double yy) {
+  if (code == F_PLANE || code == F_EDGE) {
+    o.skip = 1;
+    o.add = code == F_PLANE ? 0.5 : 0.25;
+    o.npts = m;
+    return false;
+  }
+  if (code == F_POINT) {
+    const Pt p = face_point(n, xx, yy);
+    if (m == 0) o.p1 = p;
+    if (m == 1) o.p2 = p;
+    m++;
+  }
+  return true;
+}
+
+// One cell of the reference's iloop body, faces in order.
 __device__ __forceinline__ void cell_line(const double cu[8], const double cv[8], CellOut& o) {
   o.skip = 0;
   o.add = 0.0;
@@ -96,77 +189,12 @@ __device__ __forceinline__ void cell_line(const double cu[8], const double cv[8]
   int m = 0;
 #pragma unroll 1
   for (int n = 0; n < 6; n++) {
-    const unsigned tab = kFaceCorners[n];
     double u[5], v[5];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int c = (tab >> (4 * q)) & 0xf;
-      // select among the 8 corners without indexing a local array
-      double uu = cu[0], vv = cv[0];
-#pragma unroll
-      for (int r = 1; r < 8; r++) {
-        uu = (c == r) ? cu[r] : uu;
-        vv = (c == r) ? cv[r] : vv;
-      }
-      u[q] = uu;
-      v[q] = vv;
-    }
-    u[4] = u[0];
-    v[4] = v[0];
-    // a component of one strict sign on the face's corners rules out every
-    // test below: no zero plane, no zero edge, no crossing to intersect
-    const bool u_one = (u[0] > 0.0 && u[1] > 0.0 && u[2] > 0.0 && u[3] > 0.0) ||
-                       (u[0] < 0.0 && u[1] < 0.0 && u[2] < 0.0 && u[3] < 0.0);
-    const bool v_one = (v[0] > 0.0 && v[1] > 0.0 && v[2] > 0.0 && v[3] > 0.0) ||
-                       (v[0] < 0.0 && v[1] < 0.0 && v[2] < 0.0 && v[3] < 0.0);
-    if (u_one || v_one) continue;
-    const bool uz = u[0] == 0.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0;
-    const bool vz = v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0 && v[3] == 0.0;
-    const bool vcross = v[0] * v[1] < 0.0 || v[1] * v[2] < 0.0 || v[2] * v[3] < 0.0 ||
-                        v[3] * v[0] < 0.0;
-    const bool ucross = u[0] * u[1] < 0.0 || u[1] * u[2] < 0.0 || u[2] * u[3] < 0.0 ||
-                        u[3] * u[0] < 0.0;
-    if ((uz && vcross) || (vz && ucross)) {
-      o.skip = 1;
-      o.add = 0.5;
-      o.npts = m;
-      return;
-    }
-    bool edge = false;
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-      edge = edge || (u[q] == 0.0 && u[q + 1] == 0.0 && v[q] == 0.0 && v[q + 1] == 0.0);
-    if (edge) {
-      o.skip = 1;
-      o.add = 0.25;
-      o.npts = m;
-      return;
-    }
-    double xu1 = 0, yu1 = 0, xu2 = 0, yu2 = 0, xv1 = 0, yv1 = 0, xv2 = 0, yv2 = 0;
-    const int nu = edge_zeros(u, xu1, yu1, xu2, yu2);
-    const int nv = edge_zeros(v, xv1, yv1, xv2, yv2);
-    if (nu >= 2 && nv >= 2) {
-      double den = xv2 * (yu1 - yu2) + xv1 * (yu2 - yu1) + (xu1 - xu2) * (yv1 - yv2);
-      if (den == 0.0) den = den + 0.0000001;
-      const double xx = (xu1 * (xv2 * (yv1 - yu2) + xv1 * (yu2 - yv2)) +
-                         xu2 * (xv2 * (yu1 - yv1) + xv1 * (yv2 - yu1))) / den;
-      const double yy = (xv2 * (yu1 - yu2) * yv1 + xu1 * yu2 * yv1 - xv1 * yu1 * yv2 -
-                         xu1 * yu2 * yv2 + xv1 * yu2 * yv2 + xu2 * yu1 * (yv2 - yv1)) / den;
-      if (xx >= 0.0 && xx <= 1.0 && yy >= 0.0 && yy <= 1.0) {
-        Pt p;
-        switch (n) {
-          case 0: p = {xx, yy, 0.0}; break;
-          case 1: p = {xx, yy, 1.0}; break;
-          case 2: p = {1.0, yy, xx}; break;
-          case 3: p = {0.0, yy, xx}; break;
-          case 4: p = {xx, 1.0, yy}; break;
-          default: p = {xx, 0.0, yy}; break;
-        }
-        if (m == 0) o.p1 = p;
-        if (m == 1) o.p2 = p;
-        m++;
-      }
-    }
+    face_values(cu, cv, n, u, v);
+    if (!face_active(u, v)) continue;
+    double xx = 0.0, yy = 0.0;
+    const int code = face_eval(u, v, xx, yy);
+    if (!fold_face(o, m, n, code, xx, yy)) return;
   }
   o.npts = m;
 }
@@ -283,6 +311,28 @@ __device__ __forceinline__ double block_sum(double x, double* s_red) {
   return t;
 }
 
+// Block-wide exclusive prefix sum of one small count per thread (thread
+// order) and the block's total.
+__device__ __forceinline__ int block_excl_sum(int x, int* s_cnt, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int inc = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += o;
+  }
+  __syncthreads();
+  if (lane == 31) s_cnt[warp] = inc;
+  __syncthreads();
+  int pos = inc - x;
+  total = 0;
+  for (int w = 0; w < L_WARPS; w++) {
+    if (w < warp) pos += s_cnt[w];
+    total += s_cnt[w];
+  }
+  return pos;
+}
+
 // Block-wide exclusive position of a flagged thread among the flagged ones
 // (thread order) and the block's total.
 __device__ __forceinline__ int flag_position(bool flag, int* s_cnt, int& total) {
@@ -301,9 +351,11 @@ __device__ __forceinline__ int flag_position(bool flag, int* s_cnt, int& total) 
 }
 
 // Pass 1: the block's cells in loop order.  Cells that may hold a line
-// (most do not) are queued in order and processed 256 at a time, so the
-// warps doing the full face loop are dense; one-point cells are resolved
-// inside the block wherever an earlier queued cell of the block wrote x(2).
+// (most do not) are queued in order and processed 256 at a time; their
+// faces on which neither component keeps one sign are queued again and
+// evaluated one per thread, so the warps doing the face arithmetic are
+// dense; one-point cells are resolved inside the block wherever an earlier
+// queued cell of the block wrote x(2).
 // Resident blocks per SM the cell pass is compiled for (registers per thread
 // 65536 / (256 x this)).
 #ifndef GPE_LINE_MIN_BLOCKS
@@ -314,6 +366,9 @@ template <typename T>
 __global__ void __launch_bounds__(L_THREADS, GPE_LINE_MIN_BLOCKS) line_cells_kernel(LineArgs p) {
   __shared__ double s_p2[L_THREADS][3];
   __shared__ long long s_q[2 * L_THREADS];
+  __shared__ double s_fx[6 * L_THREADS], s_fy[6 * L_THREADS];
+  __shared__ unsigned char s_fc[6 * L_THREADS];
+  __shared__ unsigned short s_face[6 * L_THREADS];
   __shared__ int s_warp[2 * L_WARPS];
   __shared__ int s_cnt[L_WARPS];
   __shared__ double s_red[L_WARPS];
@@ -348,15 +403,52 @@ __global__ void __launch_bounds__(L_THREADS, GPE_LINE_MIN_BLOCKS) line_cells_ker
     const int nb = min(qn, L_THREADS);
     const bool valid = tid < nb;
     const long long c = valid ? s_q[tid] : 0;
+    // the batch's faces: each active one evaluated by whichever thread takes
+    // it from the face queue, outcomes folded per cell in face order
+    unsigned amask = 0;
+    if (valid) {
+      double cu[8], cv[8];
+      load_cell<T>(p, c, cu, cv);
+#pragma unroll
+      for (int n = 0; n < 6; n++) {
+        double u[5], v[5];
+        face_values(cu, cv, n, u, v);
+        if (face_active(u, v)) amask |= 1u << n;
+        s_fc[tid * 6 + n] = (unsigned char)F_NONE;
+      }
+    }
+    int nface;
+    int at = block_excl_sum(__popc(amask), s_cnt, nface);
+#pragma unroll
+    for (int n = 0; n < 6; n++)
+      if ((amask >> n) & 1u) s_face[at++] = (unsigned short)((tid << 3) | n);
+    __syncthreads();
+    for (int q = tid; q < nface; q += L_THREADS) {
+      const int t = s_face[q] >> 3, n = s_face[q] & 7;
+      double cu[8], cv[8];
+      load_cell<T>(p, s_q[t], cu, cv);
+      double u[5], v[5];
+      face_values(cu, cv, n, u, v);
+      double xx = 0.0, yy = 0.0;
+      const int code = face_eval(u, v, xx, yy);
+      s_fc[t * 6 + n] = (unsigned char)code;
+      s_fx[t * 6 + n] = xx;
+      s_fy[t * 6 + n] = yy;
+    }
+    __syncthreads();
     CellOut o;
     o.skip = 0;
     o.add = 0.0;
     o.npts = 0;
     o.p1 = o.p2 = Pt{0.0, 0.0, 0.0};
     if (valid) {
-      double cu[8], cv[8];
-      load_cell<T>(p, c, cu, cv);
-      cell_line(cu, cv, o);
+      int m = 0;
+      bool live = true;
+#pragma unroll
+      for (int n = 0; n < 6; n++)
+        if (live)
+          live = fold_face(o, m, n, s_fc[tid * 6 + n], s_fx[tid * 6 + n], s_fy[tid * 6 + n]);
+      if (live) o.npts = m;
     }
     const bool writer = o.npts >= 2;
     const bool pending = !o.skip && o.npts == 1;

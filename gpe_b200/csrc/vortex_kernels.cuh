@@ -746,13 +746,16 @@ __global__ void __launch_bounds__(L_THREADS) zeros_count_kernel(ZeroArgs p) {
 }
 
 // Pass 2: the points, each at its place in loop order.  A chunk of 256
-// cells finds its hits in all 12 sections first, then one block-wide
-// exchange of per-warp counts places every point; the points themselves
-// are computed again, in one loop over the sections, by the hitting lanes.
+// cells finds its hits in all 12 sections, places them (block-wide counts
+// per warp and section), and queues them section by section; the queue is
+// then worked one hit per thread, so the point arithmetic runs in dense,
+// mostly same-section warps.
 template <typename T>
 __global__ void __launch_bounds__(L_THREADS) zeros_write_kernel(ZeroArgs p) {
   __shared__ int s_cnt[L_WARPS][Z_SECTIONS];
   __shared__ long long s_run[Z_SECTIONS];
+  __shared__ long long s_qat[Z_SECTIONS * L_THREADS];
+  __shared__ unsigned short s_qts[Z_SECTIONS * L_THREADS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long c0 = (long long)blockIdx.x * p.per_block;
   const long long c1 = min(c0 + p.per_block, p.ncell);
@@ -762,32 +765,51 @@ __global__ void __launch_bounds__(L_THREADS) zeros_write_kernel(ZeroArgs p) {
   for (long long base = c0; base < c1; base += L_THREADS) {
     const long long c = base + threadIdx.x;
     const bool valid = c < c1;
-    double re[7] = {0, 0, 0, 0, 0, 0, 0}, im[7] = {0, 0, 0, 0, 0, 0, 0};
-    int i = 1, j = 1, k = 1;
-    if (valid) load_zero_corners<T>(p, c, re, im, i, j, k);
     unsigned mask = 0;
-    Pt o;
+    if (valid) {
+      double re[7], im[7];
+      int i, j, k;
+      load_zero_corners<T>(p, c, re, im, i, j, k);
+      Pt o;
 #pragma unroll
-    for (int s = 0; s < Z_SECTIONS; s++)
-      if (valid && zero_section(s, re, im, i, j, k, p, o)) mask |= 1u << s;
+      for (int s = 0; s < Z_SECTIONS; s++)
+        if (zero_section(s, re, im, i, j, k, p, o)) mask |= 1u << s;
+    }
 #pragma unroll
     for (int s = 0; s < Z_SECTIONS; s++) {
       const unsigned bal = __ballot_sync(0xffffffffu, (mask >> s) & 1u);
       if (lane == 0) s_cnt[warp][s] = __popc(bal);
     }
     __syncthreads();
-#pragma unroll 1
+    // queue: sections in order, each in thread (= cell) order
+    int qbase = 0, nq = 0;
+#pragma unroll
     for (int s = 0; s < Z_SECTIONS; s++) {
       const unsigned bal = __ballot_sync(0xffffffffu, (mask >> s) & 1u);
-      if ((mask >> s) & 1u) {
-        long long at = s_run[s] + __popc(bal & below);
-        for (int w = 0; w < warp; w++) at += s_cnt[w][s];
-        zero_section(s, re, im, i, j, k, p, o);
-        double* q = p.pts + 3 * at;
-        q[0] = o.x;
-        q[1] = o.y;
-        q[2] = o.z;
+      int before = __popc(bal & below), tot = 0;
+      for (int w = 0; w < L_WARPS; w++) {
+        if (w < warp) before += s_cnt[w][s];
+        tot += s_cnt[w][s];
       }
+      if ((mask >> s) & 1u) {
+        s_qat[qbase + before] = s_run[s] + before;
+        s_qts[qbase + before] = (unsigned short)((threadIdx.x << 4) | s);
+      }
+      qbase += tot;
+    }
+    nq = qbase;
+    __syncthreads();
+    for (int q = threadIdx.x; q < nq; q += L_THREADS) {
+      const int t = s_qts[q] >> 4, sec = s_qts[q] & 15;
+      double re[7], im[7];
+      int i, j, k;
+      load_zero_corners<T>(p, base + t, re, im, i, j, k);
+      Pt o = {0.0, 0.0, 0.0};
+      zero_section(sec, re, im, i, j, k, p, o);
+      double* out = p.pts + 3 * s_qat[q];
+      out[0] = o.x;
+      out[1] = o.y;
+      out[2] = o.z;
     }
     __syncthreads();
     if (threadIdx.x < Z_SECTIONS) {

@@ -82,6 +82,13 @@ def test_no_device_is_a_clean_error_without_gpu(L):
 def test_null_context_calls_are_rejected(L):
     assert L.gpe_gpu_solver(None, None, None) == 1
     assert L.gpe_gpu_norm(None, None) == 1
+    # diagnostics entry points check the context before touching a device
+    assert L.gpe_gpu_random_phase(None, 1.0, 1.0, 0, None, None) == 1
+    assert L.gpe_gpu_condensed_particles(None, None, None, None, None, 0) == 1
+    assert L.gpe_gpu_filtered_field(None, 1.0, 1.0, None, 16, 0) == 1
+    assert L.gpe_gpu_linelength(None, None) == 1
+    assert L.gpe_gpu_zeros(None, None, None, 0) == 1
+    assert L.gpe_gpu_get_site(None, 0, 0, 0, None) == 1
     assert L.gpe_gpu_launch_count(None) == -1
     L.gpe_gpu_destroy(None)
 

@@ -169,3 +169,24 @@ def test_gpu_zeros_of_lines_and_a_random_phase_state():
         ec, ep = oracle.zeros(psi, *s.grid())
     assert counts.tolist() == ec.tolist() and counts.sum() > 0
     np.testing.assert_array_equal(pts, ep)
+
+
+@pytest.mark.gpu
+def test_gpu_zeros_rejects_a_small_buffer_and_fills_the_counts():
+    import ctypes
+
+    from gpe_b200 import GpeError
+    from gpe_b200._lib import check, lib
+    rng = np.random.default_rng(3)
+    psi = rng.standard_normal((12, 12, 12)) + 1j * rng.standard_normal((12, 12, 12))
+    with _solver(12, 12, 12) as s:
+        s.set_state(psi)
+        want, _ = s.zeros()
+        counts = np.zeros(12, dtype=np.int64)
+        pts = np.zeros((2, 3))
+        P64 = ctypes.POINTER(ctypes.c_int64)
+        with pytest.raises(GpeError):
+            check(lib().gpe_gpu_zeros(s.handle, counts.ctypes.data_as(P64),
+                                      pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2),
+                  s.handle)
+    assert want.sum() > 2 and counts.tolist() == want.tolist()

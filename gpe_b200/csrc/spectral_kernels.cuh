@@ -25,6 +25,10 @@ __host__ __device__ __forceinline__ long long index_k2(int i, int n) {
   return (i <= (n - 1) / 2 + 1) ? (long long)i * i : (long long)(n - i) * (n - i);
 }
 
+__device__ __forceinline__ int index_k2i(int i, int n) {
+  return (i <= (n - 1) / 2 + 1) ? i * i : (n - i) * (n - i);
+}
+
 // SplitMix64 (Steele, Lea and Flood, "Fast splittable pseudorandom number
 // generators", OOPSLA 2014): the finaliser of state seed + (q+1) G, top 53
 // bits as a double in [0, 1).
@@ -82,9 +86,12 @@ __global__ void filter_kernel(T* __restrict__ a, int nx, int ny, int nz, double 
 
 // Smallest b with b^2 >= k2 (k2 < 2^31): the first kk of F(kk) that holds
 // the mode, as the reference's sqrt(real(k2)) <= kk test (src/io.f90:673-677).
-// The FP32 root is within one of the true root; integer checks make it exact.
+// The approximate FP32 root is within one of the true root for every k2 here;
+// integer checks make it exact.
 __device__ __forceinline__ int ceil_sqrt(int k2) {
-  int b = (int)sqrtf((float)k2);
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"((float)k2));
+  int b = (int)r;
   if (b * b > k2) b--;
   if ((b + 1) * (b + 1) <= k2) b++;
   return b + (b * b < k2 ? 1 : 0);
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(S_THREADS, S_E <= 4 ? 4 : 3) spectrum_kernel(
   for (long long row = (long long)blockIdx.x * S_WARPS + warp; row < nrows;
        row += (long long)gridDim.x * S_WARPS) {
     const int j = (int)(row % p.ny), k = (int)(row / p.ny);
-    const int c2 = (int)(index_k2(j, p.ny) + index_k2(k, p.nz));
+    const int c2 = index_k2i(j, p.ny) + index_k2i(k, p.nz);
     const double ayz = __ldg(p.ay + j);
     const double azk = __ldg(p.az + k);
     const V2* arow = reinterpret_cast<const V2*>(a) + (size_t)row * nx;
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(S_THREADS, S_E <= 4 ? 4 : 3) spectrum_kernel(
         // shells: k2 is monotone along the lane's sites, so equal shell codes
         // at its two ends put every site in that shell
         const int ilast = min(i0 + S_E - 1, end);
-        const int k2f = (int)index_k2(i0, nx) + c2, k2l = (int)index_k2(ilast, nx) + c2;
+        const int k2f = index_k2i(i0, nx) + c2, k2l = index_k2i(ilast, nx) + c2;
         const bool any = i0 <= end;
         const int sf = (any && k2f > 0) ? shell_code(k2f, sh_up, sh_dn) : -1;
         const int sl = (any && k2l > 0) ? shell_code(k2l, sh_up, sh_dn) : -2;
@@ -237,7 +244,7 @@ __global__ void __launch_bounds__(S_THREADS, S_E <= 4 ? 4 : 3) spectrum_kernel(
           const double k2p = m12 * ((__ldg(p.ax + ic) + ayz) + azk);
           const double term = (k2p + rho0) * recip_newton(k2p * (k2p + two_rho0));
           tot += (valid && k2p != 0.0) ? term : 0.0;
-          const int k2 = (int)index_k2(ic, nx) + c2;
+          const int k2 = index_k2i(ic, nx) + c2;
           const bool live = valid && k2 > 0;
           if (one_shell) {
             lane_sum += live ? pw : 0.0;

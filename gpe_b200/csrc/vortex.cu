@@ -45,15 +45,17 @@ Vortex* vortex_ext(gpe_ctx* c) {
                                std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// field: the resident padded psi (dense = false) or a dense interior array.
 template <typename T>
-int run(gpe_ctx* c, const FieldView& v, double* length) {
+int run(gpe_ctx* c, const FieldView& v, const void* field, bool dense, double* length) {
   LineArgs p;
-  p.psi = v.psi;
+  p.psi = field;
   p.nx = v.nx;
   p.ny = v.ny;
   p.nz = v.nz;
-  p.Nx = v.Nx;
-  p.Ny = v.Ny;
+  p.Nx = dense ? v.nx : v.Nx;
+  p.Ny = dense ? v.ny : v.Ny;
+  p.ghost = dense ? 0 : 2;
   p.cx = v.nx - 2;
   const long long rows = (long long)(v.ny - 2) * (v.nz - 2);
   p.ncell = rows * p.cx;
@@ -215,5 +217,25 @@ extern "C" int gpe_gpu_linelength(gpe_ctx* c, double* length) {
     *length = 0.0;
     return GPE_OK;
   }
-  return v.es == 16 ? run<double>(c, v, length) : run<float>(c, v, length);
+  return v.es == 16 ? run<double>(c, v, v.psi, false, length)
+                    : run<float>(c, v, v.psi, false, length);
+}
+
+extern "C" int gpe_gpu_linelength_field(gpe_ctx* c, const void* field, int32_t elem_bytes,
+                                        double* length) {
+  FieldView v;
+  if (!c || gpe_internal_field_view(c, &v)) return GPE_ERR_INVALID;
+  if (!length || !field) return gpe_internal_fail(c, GPE_ERR_INVALID, "null argument");
+  if (elem_bytes != 8 && elem_bytes != 16)
+    return gpe_internal_fail(c, GPE_ERR_INVALID, "elem_bytes must be 8 or 16");
+  VX_CU(c, cudaSetDevice(v.dev));
+  if (!v.single_domain)
+    return gpe_internal_fail(c, GPE_ERR_INVALID,
+                             "linelength needs a single-domain context (the whole grid)");
+  if (v.nx < 3 || v.ny < 3 || v.nz < 3) {
+    *length = 0.0;
+    return GPE_OK;
+  }
+  return elem_bytes == 16 ? run<double>(c, v, field, true, length)
+                          : run<float>(c, v, field, true, length);
 }

@@ -216,8 +216,9 @@ __device__ __forceinline__ double segment(const Pt& p1, const Pt& p2) {
 }
 
 struct LineArgs {
-  const void* psi;
+  const void* psi;        // the resident padded field, or a dense interior array
   int nx, ny, nz, Nx, Ny;
+  int ghost;              // 2 for the padded field, 0 for a dense array
   int cx;               // cells per row, nx - 2
   long long ncell;      // (nx-2)(ny-2)(nz-2)
   long long per_block;  // cells per block (whole rows)
@@ -242,8 +243,8 @@ __device__ __forceinline__ void load_cell(const LineArgs& p, long long c, double
 #pragma unroll
   for (int q = 0; q < 8; q++) {
     const int di = q & 1, dj = (q >> 1) & 1, dk = q >> 2;
-    const size_t at = ((size_t)(k + dk + 2) * p.Ny + (size_t)(j + dj + 2)) * p.Nx +
-                      (size_t)(i + di + 2);
+    const size_t at = ((size_t)(k + dk + p.ghost) * p.Ny + (size_t)(j + dj + p.ghost)) * p.Nx +
+                      (size_t)(i + di + p.ghost);
     const V w = f[at];
     cu[q] = (double)w.x;
     cv[q] = (double)w.y;

@@ -18,6 +18,7 @@ them without separators, one record (line) per write.
   eta_time.dat  (4e17.9) t, eta(1:3)                        src/io.f90:719-721
   p_saved.dat   (i10) p                                     src/io.f90:521-525
   linelength.dat (3e17.9) t, im_t, total line length        src/io.f90:1405-1438
+  filtered_ll.dat (3e17.9) the same of the filtered field    src/io.f90:583-585
   timestep.dat  (3e17.9,i10) t, im_t, |dt|, p (rk45, every save_rate
                 steps, after the step)                      src/solve.f90:234-241
 

@@ -259,10 +259,18 @@ class GpeSolver:
         from . import spectral
         return spectral.filtered_field(self, filter_kc, m, out)
 
-    def linelength(self) -> float:
-        """linelength (src/variables.f90:879-1145): total vortex line length."""
+    def linelength(self, field=None) -> float:
+        """linelength (src/variables.f90:879-1145): total vortex line length of
+        the state, or of `field` (a contiguous CUDA torch tensor (nz, ny, nx),
+        complex64/128), e.g. the filtered field."""
         v = ctypes.c_double()
-        check(lib().gpe_gpu_linelength(self._ctx, ctypes.byref(v)), self._ctx)
+        if field is None:
+            check(lib().gpe_gpu_linelength(self._ctx, ctypes.byref(v)), self._ctx)
+        else:
+            torch_ready(field)
+            eb = 16 if str(field.dtype) == "torch.complex128" else 8
+            check(lib().gpe_gpu_linelength_field(self._ctx, ctypes.c_void_p(field.data_ptr()), eb,
+                                                 ctypes.byref(v)), self._ctx)
         return v.value
 
     def zeros(self):
@@ -385,9 +393,15 @@ def _cadence_outputs(s, run_dir, io: OutputParams, counters: dict) -> None:
         output.append(os.path.join(run_dir, "mass.dat"), output.mass_line(s.t, s.im_t, c.row))
         if io.save_spectrum:
             output.write_spectrum(run_dir, s.p, s.t, c)
-        if io.save_filter:
-            f = s.filtered_field(io.filter_kc, 1.0)
-            output.write_filtered_surface(run_dir, s.p, s.t, f, s.grid(),
+        if io.save_filter:  # filtered_surface (src/io.f90:398-400, 533-628)
+            import torch
+            f = torch.empty(s.shape, dtype=torch.complex128 if prm.precision == 16 else
+                            torch.complex64, device=torch.device("cuda", prm.device))
+            s.filtered_field(io.filter_kc, 1.0, out=f)
+            if io.save_ll:  # save_linelength(filtered, 1) (src/io.f90:583-585)
+                output.append(os.path.join(run_dir, "filtered_ll.dat"),
+                              output.e_line(s.t, s.im_t, s.linelength(f)))
+            output.write_filtered_surface(run_dir, s.p, s.t, f.cpu().numpy(), s.grid(),
                                           pr_bytes=_pr_bytes(prm))
         counters["m"] += 1
     if t_all >= io.save_rate2 * counters["n"]:

@@ -237,6 +237,13 @@ int gpe_gpu_filtered_field(gpe_ctx* ctx, double filter_kc, double m, void* out,
  * to cell and leaves their start undefined; here they start at zero on
  * every call. */
 int gpe_gpu_linelength(gpe_ctx* ctx, double* length);
+/* The same for a DEVICE array in the interior layout on the context's grid
+ * (complex64 when elem_bytes = 8, complex128 when 16), e.g. the field of
+ * gpe_gpu_filtered_field: save_linelength(filtered, 1) of
+ * filtered_surface (src/io.f90:583-585), filtered_ll.dat.  The array must
+ * be complete (written on the caller's streams and synchronised). */
+int gpe_gpu_linelength_field(gpe_ctx* ctx, const void* field, int32_t elem_bytes,
+                             double* length);
 
 /* get_zeros, get_extra_zeros and get_re_im_zeros (src/io.f90:895-1402):
  * the zero points of the resident state (single-domain contexts) that the

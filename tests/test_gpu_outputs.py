@@ -8,6 +8,7 @@ import pytest
 
 from gpe_b200 import GpeParams, GpeSolver, output
 from gpe_b200.solver import OutputParams, run_loop
+import oracle
 from oracle import spectral_ref as ref
 
 pytestmark = pytest.mark.gpu
@@ -61,3 +62,21 @@ def test_run_loop_writes_the_reference_files(tmp_path):
     from gpe_b200.restart import read_end_state
     st = read_end_state(os.path.join(d, "proc00", "end_state.dat"), expect=(16, 16, 16))
     assert st.p in (10, 11) and not np.array_equal(st.psi, final)  # t = 0.1 up to rounding
+
+
+def test_run_loop_filtered_surface_and_its_line_length(tmp_path):
+    d = str(tmp_path)
+    open(os.path.join(d, "RUNNING"), "w").close()
+    with _solver(16) as s:
+        s.random_phase(0.75, 0.75, 2)
+        io = OutputParams(save_rate=100, save_rate2=1e9, save_rate3=1e9, p_save=1e9,
+                          save_3d=False, save_spectrum=False, save_filter=True, save_ll=True,
+                          filter_kc=6.0)
+        run_loop(s, 2, run_dir=d, outputs=io)
+        grid = s.grid()
+    t, dims, _, _, field, x, _, _ = output.read_surface(
+        os.path.join(d, "proc00", "filtered0000000.dat"))
+    assert dims == (16, 16, 16) and t == 0.0 and np.array_equal(x, grid[0])
+    line = open(os.path.join(d, "filtered_ll.dat")).read().splitlines()
+    exp, _ = oracle.linelength(field, 1.0)  # dx = 2 xr / (n - 1) = 1
+    assert len(line) == 1 and float(line[0][34:51]) == pytest.approx(exp, rel=1e-8)

@@ -190,3 +190,27 @@ def test_gpu_zeros_rejects_a_small_buffer_and_fills_the_counts():
                                       pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2),
                   s.handle)
     assert want.sum() > 2 and counts.tolist() == want.tolist()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [16, 8])
+def test_gpu_line_length_of_a_device_field(precision):
+    """gpe_gpu_linelength_field on a dense device array: the same number as the
+    resident state holding the same values, and the oracle's on the filtered
+    field (save_linelength(filtered, 1))."""
+    import torch
+    shape = (20, 18, 24)
+    rng = np.random.default_rng(8)
+    psi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    dt = torch.complex128 if precision == 16 else torch.complex64
+    with _solver(*shape, precision=precision) as s:
+        s.set_state(psi.astype(np.complex128 if precision == 16 else np.complex64))
+        here = s.linelength()
+        dev = torch.empty(shape, dtype=dt, device="cuda")
+        s.get_state_device(dev)
+        assert s.linelength(dev) == here
+        f = torch.empty(shape, dtype=dt, device="cuda")
+        s.filtered_field(6.0, 1.0, out=f)
+        got = s.linelength(f)
+    exp, _ = oracle.linelength(f.cpu().numpy().astype(np.complex128), 0.5)
+    assert got == pytest.approx(exp, rel=1e-12, abs=1e-14)

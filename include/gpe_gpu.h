@@ -199,7 +199,9 @@ int gpe_gpu_diagnostics(gpe_ctx* ctx, double* mass, double* mom);
  * 'backward' = exp(+i k.x), both scaled by 1/sqrt(nx ny nz); the integer
  * wavenumber of index i along an axis of n points is i for
  * i <= (n-1)/2 + 1 and n - i above (src/ic.f90:221-238).  libcufft.so.11 is
- * opened on first use; without it the calls return GPE_ERR_CUDA.
+ * opened on first use; without it the calls return GPE_ERR_CUDA.  The first
+ * call on a context creates its two cuFFT plans (with cuFFT's work areas),
+ * kept until the context is destroyed.
  *
  * gpe_gpu_random_phase replaces ics' random_phase (src/ic.f90:190-252) with
  * get_kc_amp (:256-269): every mode with |k|^2 <= kc2 gets amplitude
@@ -254,7 +256,9 @@ int gpe_gpu_linelength_field(gpe_ctx* ctx, const void* field, int32_t elem_bytes
  * receives each section's number of points.  With points non-NULL (HOST,
  * room for cap points of 3 doubles) the points follow, sections
  * concatenated; a cap below the total returns GPE_ERR_INVALID with counts
- * filled.  Call with points = NULL to size the buffer. */
+ * filled.  Call with points = NULL to size the buffer.  The device copy of
+ * the points (24 bytes each) is kept by the context for the next call and
+ * freed with it. */
 #define GPE_ZERO_SECTIONS 12
 int gpe_gpu_zeros(gpe_ctx* ctx, int64_t* counts, double* points, int64_t cap);
 

@@ -99,6 +99,7 @@ SIGNATURES = {
     "gpe_gpu_linelength_field": (ctypes.c_int, [_vp, _vp, _i32, _dp]),
     "gpe_gpu_zeros": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _dp, _i64]),
     "gpe_gpu_get_site": (ctypes.c_int, [_vp, _i32, _i32, _i32, _dp]),
+    "gpe_gpu_get_plane": (ctypes.c_int, [_vp, _i32, _vp, _i32]),
     "gpe_gpu_random_phase": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_uint64, _dp, _dp]),
     "gpe_gpu_condensed_particles": (ctypes.c_int, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int64),

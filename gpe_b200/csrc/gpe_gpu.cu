@@ -1665,6 +1665,40 @@ int gpe_gpu_get_site(gpe_ctx* c, int32_t i, int32_t j, int32_t k, double* re_im)
   return GPE_OK;
 }
 
+int gpe_gpu_get_plane(gpe_ctx* c, int32_t k, void* out, int32_t elem_bytes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  rc = check_elem(c, elem_bytes, out);
+  if (rc) return rc;
+  if (k < 0 || k >= c->nz) return fail(c, GPE_ERR_INVALID, "plane outside the grid");
+  const size_t first = ((size_t)(k + 2) * c->Ny + 2) * c->Nx + 2;
+  const unsigned char* src = static_cast<const unsigned char*>(c->fld[c->psi_id]) +
+                             first * (size_t)c->es;
+  const size_t n = (size_t)c->nx * c->ny;
+  std::vector<unsigned char> tmp;
+  void* dst = out;
+  if (elem_bytes != c->es) {
+    tmp.resize(n * (size_t)c->es);
+    dst = tmp.data();
+  }
+  CU_CHECK(c, cudaMemcpy2DAsync(dst, (size_t)c->nx * c->es, src, (size_t)c->Nx * c->es,
+                                (size_t)c->nx * c->es, c->ny, cudaMemcpyDeviceToHost,
+                                c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  if (elem_bytes != c->es) {
+    if (c->es == 8) {
+      const float* f = reinterpret_cast<const float*>(tmp.data());
+      double* o = static_cast<double*>(out);
+      for (size_t q = 0; q < 2 * n; q++) o[q] = f[q];
+    } else {
+      const double* f = reinterpret_cast<const double*>(tmp.data());
+      float* o = static_cast<float*>(out);
+      for (size_t q = 0; q < 2 * n; q++) o[q] = (float)f[q];
+    }
+  }
+  return GPE_OK;
+}
+
 int gpe_gpu_solver(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
   int rc = check_ctx(c);
   if (rc) return rc;

@@ -32,6 +32,10 @@ procRR/ (RR = the two-digit rank, src/io.f90:118-143):
     same layout with t in place of t+im_t and the filtered field
   end_state_filtered.dat (flag 1, :607-616): the end_state layout
 
+save_surface (src/io.f90:449-485): procRR/psiNNNNNNN.dat, the plane z = nz/2
+as (6e17.9) records x(i), y(j), |psi|^2, phase, Re psi, Im psi, j fastest,
+an empty record after each i.
+
 Text files of the zero finders in procRR/ (src/io.f90:895-1402):
 zerosNNNNNNN.dat, re_zerosNNNNNNN.dat, im_zerosNNNNNNN.dat, each a list-
 directed header line per section (" # i,j,k --> ...") followed by its points
@@ -273,3 +277,25 @@ def write_zeros(run_dir: str, p: int, counts, points, rank: int = 0) -> list:
             f.write(text)
         paths.append(path)
     return paths
+
+
+def surface_slice_text(plane, x, y) -> str:
+    """save_surface of one z-plane (ny, nx)."""
+    parts = []
+    nyy, nxx = plane.shape
+    for i in range(nxx):
+        for j in range(nyy):
+            v = complex(plane[j, i])
+            parts.append(e_line(x[i], y[j], abs(v) ** 2,
+                                float(np.arctan2(v.imag + 1.0e-6, v.real)), v.real, v.imag))
+        parts.append("\n")
+    return "".join(parts)
+
+
+def write_surface_slice(run_dir: str, p: int, plane, grid, rank: int = 0) -> str:
+    d = os.path.join(run_dir, proc_dir(rank))
+    os.makedirs(d, exist_ok=True)
+    path = os.path.join(d, f"psi{itos(p)}.dat")
+    with open(path, "w") as f:
+        f.write(surface_slice_text(plane, grid[0], grid[1]))
+    return path

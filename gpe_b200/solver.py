@@ -158,6 +158,13 @@ class GpeSolver:
               self._ctx)
         return complex(v[0], v[1])
 
+    def get_plane(self, k: int, dtype=np.complex128) -> np.ndarray:
+        """The z-plane k, (ny, nx): the slice of save_surface."""
+        out = np.empty((self.prm.ny, self.prm.nx), dtype=dtype)
+        check(lib().gpe_gpu_get_plane(self._ctx, int(k), out.ctypes.data_as(ctypes.c_void_p),
+                                      self._elem(dtype)), self._ctx)
+        return out
+
     # ---- the reference's hot-path procedures --------------------------------
     def _tm(self) -> GpeTimeC:
         return GpeTimeC(self.t, self.im_t, self.dt.real, self.dt.imag, self.p, 0)
@@ -347,6 +354,7 @@ class OutputParams:
     save_filter: bool = False
     filter_kc: float = 10.0
     save_ll: bool = False      # linelength.dat every save_rate steps
+    save_contour: bool = False  # save_surface slice every save_rate2 time units
     save_zeros: bool = False   # zero finders every save_rate2 time units
 
 
@@ -408,6 +416,8 @@ def _cadence_outputs(s, run_dir, io: OutputParams, counters: dict) -> None:
         if io.save_zeros:
             counts, pts = s.zeros()
             output.write_zeros(run_dir, s.p, counts, pts)
+        if io.save_contour:
+            output.write_surface_slice(run_dir, s.p, s.get_plane(prm.nz // 2), s.grid())
         if io.save_3d:
             _idl_surface(s, run_dir)
         counters["n"] += 1

@@ -153,6 +153,11 @@ int gpe_gpu_get_state_device(gpe_ctx* ctx, void* psi, int32_t elem_bytes);
  * writes to psi_time.dat (src/io.f90:147-195), without copying the field. */
 int gpe_gpu_get_site(gpe_ctx* ctx, int32_t i, int32_t j, int32_t k, double* re_im);
 
+/* The z-plane k of this context (k counts its own planes) into a HOST array
+ * out[ny][nx] (x fastest) of elem_bytes complexes: the slice save_surface
+ * writes (src/io.f90:449-485, psi*.dat at nz/2), without copying the field. */
+int gpe_gpu_get_plane(gpe_ctx* ctx, int32_t k, void* out, int32_t elem_bytes);
+
 /* One call of solver(var_in, var_out) (src/solve.f90:25-53) on the
  * resident state: advances psi by one step of the configured scheme and
  * updates tm->t, tm->im_t and (rk45) tm->dt exactly as the reference updates

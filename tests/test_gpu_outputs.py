@@ -80,3 +80,16 @@ def test_run_loop_filtered_surface_and_its_line_length(tmp_path):
     line = open(os.path.join(d, "filtered_ll.dat")).read().splitlines()
     exp, _ = oracle.linelength(field, 1.0)  # dx = 2 xr / (n - 1) = 1
     assert len(line) == 1 and float(line[0][34:51]) == pytest.approx(exp, rel=1e-8)
+
+
+@pytest.mark.parametrize("precision", [16, 8])
+def test_get_plane_matches_the_state(precision):
+    with _solver(12, precision) as s:
+        s.random_phase(1.0, 5.0, 6)
+        psi = s.get_state()
+        for k in (0, 6, 11):
+            np.testing.assert_array_equal(s.get_plane(k), psi[k])
+        np.testing.assert_array_equal(s.get_plane(3, np.complex64),
+                                      s.get_state(np.complex64)[3])
+        with pytest.raises(Exception):
+            s.get_plane(12)

@@ -75,3 +75,14 @@ def test_write_spectrum_files(tmp_path):
     assert (tmp_path / "idf" / "idf0000003.dat").read_text().splitlines()[2] == \
         "        3  0.400000000E+01"
     assert (tmp_path / "eta_time.dat").read_text() == output.e_line(0.25, 0.0, 0.5, 1.0)
+
+
+def test_surface_slice_layout():
+    plane = np.array([[1 + 2j, 3 + 0j], [0 - 1j, 2 + 2j]])  # (ny=2, nx=2)
+    text = output.surface_slice_text(plane, [0.0, 0.5], [-1.0, 1.0])
+    lines = text.split("\n")
+    # i outer, j inner, an empty record after each i
+    assert len(lines) == 2 * 3 + 1 and lines[2] == "" and lines[5] == ""
+    assert lines[0] == output.e_line(0.0, -1.0, 5.0, np.arctan2(2.0 + 1e-6, 1.0), 1.0,
+                                     2.0).rstrip("\n")
+    assert lines[1].startswith(output.fortran_e(0.0) + output.fortran_e(1.0))

@@ -226,7 +226,8 @@ int gpe_gpu_random_phase(gpe_ctx* ctx, double nv, double enerv, uint64_t seed,
  *   eta[7], nharm[7] = mean occupation and mode count of the 7 logarithmic
  *     shells (spectrum*.dat);
  *   F[nf] = the integral distribution function F(kk), kk = 1..nf, nf = nx/2
- *     (idf*.dat; nf must equal nx/2).
+ *     (idf*.dat; nf must equal nx/2; nx up to 5120, the bins living in
+ *     shared memory).
  * Any output pointer may be NULL (HOST arrays). */
 int gpe_gpu_condensed_particles(gpe_ctx* ctx, double* row, double* eta,
                                 int64_t* nharm, double* F, int32_t nf);

@@ -95,6 +95,8 @@ SIGNATURES = {
     "gpe_gpu_energy": (ctypes.c_int, [_vp, _dp, _dp]),
     "gpe_gpu_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
     "gpe_gpu_wait_probe": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "gpe_gpu_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "gpe_gpu_test_stall": (ctypes.c_int, [_vp, _i32]),
     "gpe_gpu_linelength": (ctypes.c_int, [_vp, _dp]),
     "gpe_gpu_linelength_field": (ctypes.c_int, [_vp, _vp, _i32, _dp]),
     "gpe_gpu_zeros": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _dp, _i64]),
@@ -178,6 +180,37 @@ def torch_ready(t) -> None:
     reading) must be finished before its pointer is handed over."""
     import torch
     torch.cuda.current_stream(t.device).synchronize()
+
+
+_COMPLEX_EB = {"torch.complex64": 8, "torch.complex128": 16}
+
+
+def device_field(t, shape, device: int, what: str, elem_bytes: int | None = None,
+                 dtypes=_COMPLEX_EB) -> int:
+    """Check a tensor before its raw pointer goes to the library, and return
+    its element size in bytes.
+
+    The entry points that take a device pointer read or write exactly
+    prod(shape) elements of the given size, densely; a host tensor, a tensor
+    on another GPU, a strided view, a wrong shape or another dtype would make
+    them touch memory outside the allocation.  Raises GpeError(GPE_ERR_INVALID)
+    before any launch."""
+    if not getattr(t, "is_cuda", False):
+        raise GpeError(1, f"{what}: expected a CUDA tensor")
+    idx = t.device.index
+    if (0 if idx is None else idx) != device:
+        raise GpeError(1, f"{what}: tensor is on cuda:{idx}, the solver on cuda:{device}")
+    if not t.is_contiguous():
+        raise GpeError(1, f"{what}: tensor must be contiguous")
+    if tuple(t.shape) != tuple(shape):
+        raise GpeError(1, f"{what}: shape {tuple(t.shape)} != {tuple(shape)}")
+    eb = dtypes.get(str(t.dtype))
+    if eb is None:
+        raise GpeError(1, f"{what}: dtype {t.dtype} not in {sorted(dtypes)}")
+    if elem_bytes is not None and eb != elem_bytes:
+        raise GpeError(1, f"{what}: dtype {t.dtype} does not match the solver's precision "
+                          f"({elem_bytes}-byte complex)")
+    return eb
 
 
 def check(rc: int, ctx=None) -> None:

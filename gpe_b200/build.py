@@ -44,6 +44,23 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def local_deps(path: str, seen=None) -> set:
+    """The file and every header of csrc/ or include/ it includes, transitively."""
+    import re
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read(), flags=re.M):
+            for d in (CSRC, INCLUDE):
+                cand = os.path.join(d, name)
+                if os.path.exists(cand):
+                    local_deps(cand, seen)
+                    break
+    return seen
+
+
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     if not force and not needs_build():
         return LIB
@@ -59,10 +76,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     for cu in cus:
         obj = os.path.join(objdir, os.path.basename(cu)[:-3] + ".o")
         objs.append(obj)
+        # a translation unit is recompiled only when it or a header it
+        # includes is newer than its object
+        if (not force and not ptxas_info and os.path.exists(obj) and
+                all(os.path.getmtime(d) <= os.path.getmtime(obj) for d in local_deps(cu))):
+            continue
         cmds.append([*common, *EXTRA.get(os.path.basename(cu), []), "-c", cu, "-o", obj])
     # translation units compile in parallel, then one link
     from concurrent.futures import ThreadPoolExecutor
-    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
         for cmd in cmds:
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)

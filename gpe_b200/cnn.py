@@ -15,7 +15,7 @@ import math
 
 import numpy as np
 
-from ._lib import GpeCnnParamsC, check_cnn, lib, torch_ready
+from ._lib import GpeCnnParamsC, check_cnn, device_field, lib, torch_ready
 from .solver import GpeSolver
 
 LAYERS, TAPS, CH = 4, 27, 16
@@ -49,6 +49,7 @@ class CoarseCorrector:
         self._h = ctypes.c_void_p()
         check_cnn(lib().gpe_cnn_create(ctypes.byref(p), ctypes.byref(self._h)), None)
         self.shape = (nz, ny, nx)
+        self.device = int(device)
         self.out_scale = float(out_scale)
         self.train = bool(train)
 
@@ -104,27 +105,28 @@ class CoarseCorrector:
         self._chk(lib().gpe_cnn_delta(self._h, s.handle, ctypes.c_void_p(out.data_ptr())))
         return out
 
-    @staticmethod
-    def _eb(t) -> int:
-        return 16 if str(t.dtype) == "torch.complex128" else 8
+    def _eb(self, t, what: str) -> int:
+        return device_field(t, self.shape, self.device, what)
 
     def grad(self, s: GpeSolver, target):
         """(loss, dW, db) of the pair (s's psi, target CUDA tensor)."""
         t = target.contiguous()
+        eb = self._eb(t, "grad target")
         torch_ready(t)
         loss = ctypes.c_double()
         dw = np.zeros((LAYERS, TAPS, CH, CH), dtype=np.float32)
         db = np.zeros((LAYERS, CH), dtype=np.float32)
         self._chk(lib().gpe_cnn_grad(self._h, s.handle, ctypes.c_void_p(t.data_ptr()),
-                                     self._eb(t), ctypes.byref(loss), _fptr(dw), _fptr(db)))
+                                     eb, ctypes.byref(loss), _fptr(dw), _fptr(db)))
         return loss.value, dw, db
 
     def train_step(self, s: GpeSolver, target, lr: float) -> float:
         t = target.contiguous()
+        eb = self._eb(t, "train_step target")
         torch_ready(t)
         loss = ctypes.c_double()
         self._chk(lib().gpe_cnn_train_step(self._h, s.handle, ctypes.c_void_p(t.data_ptr()),
-                                           self._eb(t), float(lr), ctypes.byref(loss)))
+                                           eb, float(lr), ctypes.byref(loss)))
         return loss.value
 
     def adam_reset(self) -> None:
@@ -137,6 +139,7 @@ class CoarseCorrector:
 def restrict(fine: GpeSolver, out) -> None:
     """2:1 restriction (2x2x2 average) of fine's psi into `out`, a CUDA
     complex64/complex128 tensor of shape (nz/2, ny/2, nx/2)."""
-    eb = 16 if str(out.dtype) == "torch.complex128" else 8
+    nz, ny, nx = fine.shape
+    eb = device_field(out, (nz // 2, ny // 2, nx // 2), fine.prm.device, "restrict(out)")
     torch_ready(out)
     check_cnn(lib().gpe_cnn_restrict(fine.handle, ctypes.c_void_p(out.data_ptr()), eb), None)

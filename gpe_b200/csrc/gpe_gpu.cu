@@ -164,6 +164,8 @@ struct gpe_ctx {
   void* h_pinned = nullptr;
   size_t h_pinned_bytes = 0;
   bool norm_valid = false;
+  unsigned long long wait_limit_ns = 2000000000ull;
+  int stall_plane = -1;  // failure-detection test hook (gpe_gpu_test_stall)
   int64_t launches = 0;
   int last_nblk = 0;
   int64_t device_bytes = 0;
@@ -613,6 +615,7 @@ void fill_common(const StageSpec& sp, bool fold, const LaunchShape& sh,
   p->dt0_r = sp.dt0.real(); p->dt0_i = sp.dt0.imag();
   p->inv_absdt = sp.inv_absdt;
   p->wait_limit_ns = WAIT_LIMIT_NS;
+  p->stall_plane = -1;
 }
 
 template <typename TS, typename TC, bool BATCH>
@@ -643,6 +646,8 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   rc = fill_run<TS, TC>(c, sp, R, sh, f, &p.run);
   if (rc) return rc;
   fill_common<TS, TC>(sp, fold, sh, &p);
+  p.wait_limit_ns = c->wait_limit_ns;
+  p.stall_plane = c->stall_plane;
   p.partials = c->d_partials;
   p.status = c->d_status;
   const size_t nblk = (size_t)sh.ntx * sh.nty * sh.nchunks;
@@ -937,8 +942,17 @@ int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
     attempts++;
     int rc = attempt_rkck(c, dt, dt0);
     if (rc) return rc;
-    rc = read_scalars(c, &errmax, 3, 1);
-    if (rc) return rc;
+    {
+      // errmax and the status word in one synchronisation: an attempt whose
+      // kernels timed out has no valid error estimate
+      int st = 0;
+      CU_CHECK(c, cudaMemcpyAsync(&errmax, c->d_scal + 3, sizeof(double),
+                                  cudaMemcpyDeviceToHost, c->stream));
+      CU_CHECK(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                                  c->stream));
+      CU_CHECK(c, cudaStreamSynchronize(c->stream));
+      if (st != 0) return check_status(c);
+    }
     if (!std::isfinite(errmax))
       return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate");
     if (errmax <= 1.0) break;
@@ -1794,6 +1808,18 @@ int gpe_gpu_wait_probe(gpe_ctx* c, uint64_t limit_ns) {
   c->launches++;
   CU_CHECK(c, cudaStreamSynchronize(c->stream));
   return check_status(c);
+}
+
+int gpe_gpu_set_wait_limit(gpe_ctx* c, uint64_t limit_ns) {
+  if (!c) return GPE_ERR_INVALID;
+  c->wait_limit_ns = limit_ns ? (unsigned long long)limit_ns : WAIT_LIMIT_NS;
+  return GPE_OK;
+}
+
+int gpe_gpu_test_stall(gpe_ctx* c, int32_t plane) {
+  if (!c) return GPE_ERR_INVALID;
+  c->stall_plane = plane >= 0 ? plane : -1;
+  return GPE_OK;
 }
 
 int gpe_gpu_diagnostics(gpe_ctx* c, double* mass, double* mom) {

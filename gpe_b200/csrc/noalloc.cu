@@ -69,8 +69,9 @@ __global__ void plane_sums_kernel(const T* __restrict__ psi, int nx, int ny,
   const int k = blockIdx.x;
   const size_t off = (size_t)k * ny * nx;
   double acc = 0.0;
-  for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
-    const int i = q % nx, j = q / nx;
+  const long long nq = (long long)nx * ny;
+  for (long long q = threadIdx.x; q < nq; q += blockDim.x) {
+    const int i = (int)(q % nx), j = (int)(q / nx);
     const double a = (double)psi[2 * (off + q)], b = (double)psi[2 * (off + q) + 1];
     acc += weight_x(i, nx) * weight_yz(j, ny) * (a * a + b * b);
   }

@@ -189,6 +189,10 @@ int launch_spectrum(gpe_ctx* c, Spectral* s, const FieldView& v, const SpecArgs&
     cudaFree(s->d_partials);
     cudaFree(s->d_out);
     s->d_partials = s->d_out = nullptr;
+    // mark the cache empty first: a failed allocation below must not leave
+    // sizes that let the next call launch on null buffers
+    s->nblk = 0;
+    s->nf = -1;
     SP_CU(c, cudaMalloc(&s->d_partials, sizeof(double) * (size_t)nblk * (HEAD + f0.nf)));
     SP_CU(c, cudaMalloc(&s->d_out, sizeof(double) * (size_t)(21 + f0.nf)));
     s->nblk = nblk;

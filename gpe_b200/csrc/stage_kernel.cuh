@@ -43,6 +43,13 @@
 #include "device_utils.cuh"
 #include "vec2.cuh"
 
+// Cache policy of the stage kernels' streams (1: outputs stored and
+// pointwise inputs loaded evict-first, stencil planes with the default
+// policy so that the rows shared with the neighbouring tiles stay in L2).
+#ifndef GPE_STREAM_HINTS
+#define GPE_STREAM_HINTS 1
+#endif
+
 namespace gpe {
 
 constexpr int TX = 64;   // x sites per tile: one warp row, two per lane
@@ -116,6 +123,8 @@ struct StageParams {
   double* partials;       // 2 doubles per work item
   int* status;
   unsigned long long wait_limit_ns;
+  int stall_plane;        // >= 0: failure-detection test, the producer stops
+                          // issuing when it reaches this plane of an item
 };
 
 __device__ __forceinline__ bool near_edge(int i, int n) {
@@ -132,7 +141,7 @@ __global__ void __launch_bounds__(288)
   using V = typename VT<TC>::T;
   using RD = RunDesc<TS, TC>;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int s_abort, s_issued;
+  __shared__ int s_abort, s_issued, s_stop;
   __shared__ double s_red[2][32];
 
   constexpr int W = (int)(sizeof(TS) / 4);  // 8-byte TMA units per complex
@@ -169,6 +178,7 @@ __global__ void __launch_bounds__(288)
     fence_mbar_init();
     s_abort = 0;
     s_issued = 0;
+    s_stop = 0;
   }
   __syncthreads();
 
@@ -177,6 +187,9 @@ __global__ void __launch_bounds__(288)
     // Planes of successive items follow each other through the ring, so the
     // next item's first planes load while the current item drains.
     if (lane == 0) {
+#if GPE_STREAM_HINTS
+      const uint64_t pol_first = policy_evict_first();
+#endif
       int slot = 0, issued = 0;
       uint32_t cyc = 0;  // completed passes over the ring
       bool stop = false;
@@ -189,6 +202,12 @@ __global__ void __launch_bounds__(288)
 #pragma unroll
         for (int qq = 0; qq < NP; qq++) prefetch_tmap(&rd.maps.pt[qq]);
         for (int u = 0; u < niters; u++) {
+          if (u == p.stall_plane) {
+            // the plane is never loaded: the compute warps' wait for it runs
+            // out and takes the abort path
+            stop = true;
+            break;
+          }
           if (cyc > 0) {
             // the slot's previous plane must have been released by every
             // compute warp
@@ -208,10 +227,17 @@ __global__ void __launch_bounds__(288)
                       tile_y * TY + GH - R, w.z0 + u + GH);
           if (with_pt) {
 #pragma unroll
-            for (int qq = 0; qq < NP; qq++)
+            for (int qq = 0; qq < NP; qq++) {
+#if GPE_STREAM_HINTS
+              tma_load_3d_hint(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
+                               &rd.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
+                               tile_y * TY + GH, w.z0 + u - R + GH, pol_first);
+#else
               tma_load_3d(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
                           &rd.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
                           tile_y * TY + GH, w.z0 + u - R + GH);
+#endif
+            }
           }
           s_issued = ++issued;
           if (++slot == S) {
@@ -470,8 +496,13 @@ __global__ void __launch_bounds__(288)
         for (int o = 0; o < NOUT; o++) {
           TS* out = outp[o] + 2 * base;
           if (ok1) {
+#if GPE_STREAM_HINTS
+            st_cpair_stream<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
+                                                     cvt_v<TS>(res[o][1]));
+#else
             st_cpair<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
                                               cvt_v<TS>(res[o][1]));
+#endif
           } else if (ok0) {
             st_c1<TS>(out, res[o][0]);
           }
@@ -516,17 +547,25 @@ __global__ void __launch_bounds__(288)
       if (!step(IC<4>())) break;
     }
   }
-  if (t < niters) break;  // aborted
-  // Hand back the item's last R planes, still held for their x/y neighbours.
+  // A warp whose wait ran out (or that saw another's) leaves the item early.
+  const bool aborted = t < niters;
+  if (!aborted) {
+    // Hand back the item's last R planes, still held for their x/y
+    // neighbours.
 #pragma unroll
-  for (int k = 0; k < R; k++) {
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[cslot]);
-    if (++cslot == S) cslot = 0;
+    for (int k = 0; k < R; k++) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[cslot]);
+      if (++cslot == S) cslot = 0;
+    }
   }
 
   if (EPI & (EPI_NORM | EPI_ERR | EPI_ENERGY)) {
-    // per-item partials; only the compute warps take part (named barrier 1)
+    // Per-item partials; only the compute warps take part (named barrier 1).
+    // Every compute warp reaches both barriers of every item it starts, an
+    // aborted one included, and all of them leave the item loop on the same
+    // decision (s_stop, read once between the barriers), so no warp can be
+    // left waiting at a barrier that a sibling will never reach.
     red0 = warp_sum(red0);
     red1 = (EPI & EPI_ERR) ? warp_max(red1) : warp_sum(red1);
     if (lane == 0) {
@@ -542,8 +581,12 @@ __global__ void __launch_bounds__(288)
       }
       p.partials[2 * (size_t)it + 0] = a;
       p.partials[2 * (size_t)it + 1] = b;
+      s_stop = *(volatile int*)&s_abort;
     }
     named_barrier_sync(1, 32 * TY);
+    if (*(volatile int*)&s_stop) break;
+  } else if (aborted) {
+    break;  // no barrier among the compute warps in this recipe
   }
   }  // items
   }  // compute warps
@@ -551,11 +594,15 @@ __global__ void __launch_bounds__(288)
   __syncthreads();
   // After a timed-out wait, let the copies already in flight land (bounded)
   // before the CTA's shared memory is released: the last load issued into
-  // each slot completes phase (u / S) of that slot's full barrier.
+  // each slot completes phase (u / S) of that slot's full barrier.  This
+  // wait has its own limit of at least 2 s, so that a short wait limit set
+  // for the pipeline cannot release shared memory under a copy in flight.
   if (s_abort && tid == 0) {
     const int issued = s_issued;
+    const unsigned long long drain =
+        p.wait_limit_ns > 2000000000ull ? p.wait_limit_ns : 2000000000ull;
     for (int u = max(0, issued - S); u < issued; u++)
-      mbar_wait_bounded(&full[u % S], (uint32_t)((u / S) & 1), p.wait_limit_ns);
+      mbar_wait_bounded(&full[u % S], (uint32_t)((u / S) & 1), drain);
   }
 }
 

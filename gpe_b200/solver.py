@@ -20,7 +20,7 @@ from dataclasses import dataclass, fields
 import numpy as np
 
 from ._lib import (GpeError, GpeParamsC, GpeStepInfoC, GpeTimeC, GpeTimingC, SCHEMES,
-                   TIMING_FAMILIES, check, lib, torch_ready)
+                   TIMING_FAMILIES, check, device_field, lib, torch_ready)
 
 
 @dataclass
@@ -123,8 +123,8 @@ class GpeSolver:
         """Load psi (numpy host array or CUDA torch tensor, interior layout)."""
         if hasattr(psi, "is_cuda") and psi.is_cuda:
             t = psi.contiguous()
+            eb = device_field(t, self.shape, self.prm.device, "set_state")
             torch_ready(t)
-            eb = 16 if str(t.dtype) == "torch.complex128" else 8
             check(lib().gpe_gpu_set_state_device(self._ctx, ctypes.c_void_p(t.data_ptr()), eb),
                   self._ctx)
             return
@@ -145,8 +145,8 @@ class GpeSolver:
 
     def get_state_device(self, out) -> None:
         """Copy the state into a contiguous CUDA torch tensor (complex64/128)."""
+        eb = device_field(out, self.shape, self.prm.device, "get_state_device")
         torch_ready(out)
-        eb = 16 if str(out.dtype) == "torch.complex128" else 8
         check(lib().gpe_gpu_get_state_device(self._ctx, ctypes.c_void_p(out.data_ptr()), eb),
               self._ctx)
 
@@ -241,6 +241,15 @@ class GpeSolver:
         """Failure-detection self-test: raises GpeError(GPE_ERR_TIMEOUT)."""
         check(lib().gpe_gpu_wait_probe(self._ctx, int(limit_ns)), self._ctx)
 
+    def set_wait_limit(self, limit_ns: int) -> None:
+        """Limit of the stage kernels' device-side waits (0: the 2 s default)."""
+        check(lib().gpe_gpu_set_wait_limit(self._ctx, int(limit_ns)), self._ctx)
+
+    def test_stall(self, plane: int) -> None:
+        """Failure-detection test hook: later stage launches never load `plane`
+        of a work item, so their bounded waits run out (-1: off)."""
+        check(lib().gpe_gpu_test_stall(self._ctx, int(plane)), self._ctx)
+
     def diagnostics(self) -> tuple[float, np.ndarray]:
         """mass and momentum (src/variables.f90:590-694) -> (M, (Px, Py, Pz))."""
         m = ctypes.c_double()
@@ -274,8 +283,8 @@ class GpeSolver:
         if field is None:
             check(lib().gpe_gpu_linelength(self._ctx, ctypes.byref(v)), self._ctx)
         else:
+            eb = device_field(field, self.shape, self.prm.device, "linelength")
             torch_ready(field)
-            eb = 16 if str(field.dtype) == "torch.complex128" else 8
             check(lib().gpe_gpu_linelength_field(self._ctx, ctypes.c_void_p(field.data_ptr()), eb,
                                                  ctypes.byref(v)), self._ctx)
         return v.value

@@ -15,7 +15,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import check, lib, torch_ready
+from ._lib import check, device_field, lib, torch_ready
 
 NSHELLS = 7
 MASS_COLUMNS = ("M_density", "n0_over_V", "M", "n0", "temp", "temp2", "H_over_V")
@@ -69,6 +69,7 @@ def filtered_field(solver, filter_kc: float, m: float = 1.0, out=None):
     precision, shape (nz, ny, nx)) and returns it."""
     eb = 16 if solver.prm.precision == 16 else 8
     if out is not None:
+        device_field(out, solver.shape, solver.prm.device, "filtered_field(out=)", elem_bytes=eb)
         torch_ready(out)
         check(lib().gpe_gpu_filtered_field(solver.handle, float(filter_kc), float(m),
                                            ctypes.c_void_p(out.data_ptr()), eb, 1), solver.handle)

@@ -275,6 +275,25 @@ int gpe_gpu_zeros(gpe_ctx* ctx, int64_t* counts, double* points, int64_t cap);
  * after which the context is still usable. */
 int gpe_gpu_wait_probe(gpe_ctx* ctx, uint64_t limit_ns);
 
+/* Limit of every bounded wait inside this context's stage kernels (the TMA
+ * ring hand-over between the producer warp and the compute warps); 0 restores
+ * the default of 2 s.  A wait that runs out makes the kernel stop, record
+ * GPE_ERR_TIMEOUT in the status word and return; the step that hit it
+ * returns GPE_ERR_TIMEOUT and its output is undefined, but the context stays
+ * usable (set the state again).  Copies already in flight are always waited
+ * for with a limit of at least 2 s before a block exits.  No reference
+ * counterpart: failure detection of the device pipeline. */
+int gpe_gpu_set_wait_limit(gpe_ctx* ctx, uint64_t limit_ns);
+
+/* Failure-detection test hook: with plane >= 0, the producer warp of every
+ * block of this context's later stage launches stops issuing loads when it
+ * reaches that plane (counted from the start of a work item, whose first
+ * planes are its z-chunk's halo; every item has at least 2), so the compute
+ * warps' bounded wait for it runs out (GPE_ERR_TIMEOUT, as above) without any
+ * fault; -1 turns it off.  Results of the launches it affects are undefined.
+ * No reference counterpart. */
+int gpe_gpu_test_stall(gpe_ctx* ctx, int32_t plane);
+
 /* renormalise (src/variables.f90:698-709): psi = sqrt(nn) psi / sqrt(norm). */
 int gpe_gpu_renormalise(gpe_ctx* ctx, double norm);
 

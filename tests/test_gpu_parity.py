@@ -386,3 +386,39 @@ def test_non_finite_state_is_reported():
         g.get_norm()
     assert e.value.code == 5
     g.close()
+
+
+@pytest.mark.parametrize("scheme,order,bcs,kahan", [("rk4", 4, 1, False), ("rk4", 2, 2, True),
+                                                    ("rk45", 4, 2, False), ("euler", 2, 1, True)])
+def test_stage_kernel_waits_run_out_and_the_context_survives(scheme, order, bcs, kahan):
+    """The stage kernels' own pipeline waits run out: with the test hook the
+    producer warps never load plane 1, the compute warps' wait for it (limit
+    20 ms) runs out and the step returns GPE_ERR_TIMEOUT instead of hanging
+    (the recipes with a per-item reduction exercise the compute warps' shared
+    barrier on the abort path), energy() too; with the hook off and the
+    default limit restored the same context steps exactly like the oracle."""
+    from gpe_b200 import GpeError
+    n = (130, 24, 20)
+    g, o = pair(n, (8.0, 4.0, 3.5), scheme, 4, bcs, order, True,
+                precision=8 if kahan else 16, kahan=kahan)
+    psi = random_field((n[2], n[1], n[0]), seed=11)
+    g.dt = 0.01
+    g.set_state(psi)
+    g.set_wait_limit(20_000_000)
+    g.test_stall(1)
+    for _ in range(2):
+        with pytest.raises(GpeError) as e:
+            g.solver()
+        assert e.value.code == 6
+    with pytest.raises(GpeError) as e:
+        g.energy()
+    assert e.value.code == 6
+    g.test_stall(-1)
+    g.set_wait_limit(0)
+    g.t, g.dt = 0.0, 0.01
+    g.set_state(psi)
+    g.solver()
+    tm = oracle.OraTime(0.0, 0.0, 0.01, 0.0, 0)
+    exp, _, _ = o.solver(psi, tm)
+    assert rel_l2(g.get_state(), exp) < (2e-6 if kahan else 1e-12)
+    g.close()

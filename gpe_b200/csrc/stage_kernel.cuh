@@ -43,13 +43,6 @@
 #include "device_utils.cuh"
 #include "vec2.cuh"
 
-// Cache policy of the stage kernels' streams (1: outputs stored and
-// pointwise inputs loaded evict-first, stencil planes with the default
-// policy so that the rows shared with the neighbouring tiles stay in L2).
-#ifndef GPE_STREAM_HINTS
-#define GPE_STREAM_HINTS 1
-#endif
-
 namespace gpe {
 
 constexpr int TX = 64;   // x sites per tile: one warp row, two per lane
@@ -187,9 +180,6 @@ __global__ void __launch_bounds__(288)
     // Planes of successive items follow each other through the ring, so the
     // next item's first planes load while the current item drains.
     if (lane == 0) {
-#if GPE_STREAM_HINTS
-      const uint64_t pol_first = policy_evict_first();
-#endif
       int slot = 0, issued = 0;
       uint32_t cyc = 0;  // completed passes over the ring
       bool stop = false;
@@ -227,17 +217,10 @@ __global__ void __launch_bounds__(288)
                       tile_y * TY + GH - R, w.z0 + u + GH);
           if (with_pt) {
 #pragma unroll
-            for (int qq = 0; qq < NP; qq++) {
-#if GPE_STREAM_HINTS
-              tma_load_3d_hint(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
-                               &rd.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
-                               tile_y * TY + GH, w.z0 + u - R + GH, pol_first);
-#else
+            for (int qq = 0; qq < NP; qq++)
               tma_load_3d(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
                           &rd.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
                           tile_y * TY + GH, w.z0 + u - R + GH);
-#endif
-            }
           }
           s_issued = ++issued;
           if (++slot == S) {
@@ -496,13 +479,8 @@ __global__ void __launch_bounds__(288)
         for (int o = 0; o < NOUT; o++) {
           TS* out = outp[o] + 2 * base;
           if (ok1) {
-#if GPE_STREAM_HINTS
-            st_cpair_stream<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
-                                                     cvt_v<TS>(res[o][1]));
-#else
             st_cpair<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
                                               cvt_v<TS>(res[o][1]));
-#endif
           } else if (ok0) {
             st_c1<TS>(out, res[o][0]);
           }

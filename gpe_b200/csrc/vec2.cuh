@@ -90,23 +90,6 @@ __device__ __forceinline__ void st_cpair<double, double2>(double* p, double2 a, 
   reinterpret_cast<double2*>(p)[1] = b;
 }
 
-// The same 16-byte stores with the evict-first (streaming) cache policy: a
-// stage's outputs are read again only by the next stage, a full pass later,
-// so they should not displace the stencil rows that neighbouring tiles are
-// about to re-read from L2.
-template <typename TS, typename V>
-__device__ __forceinline__ void st_cpair_stream(TS* p, V a, V b);
-template <>
-__device__ __forceinline__ void st_cpair_stream<float, float2>(float* p, float2 a, float2 b) {
-  __stcs(reinterpret_cast<float4*>(p), make_float4(a.x, a.y, b.x, b.y));
-}
-template <>
-__device__ __forceinline__ void st_cpair_stream<double, double2>(double* p, double2 a,
-                                                                 double2 b) {
-  __stcs(reinterpret_cast<double2*>(p), a);
-  __stcs(reinterpret_cast<double2*>(p) + 1, b);
-}
-
 template <typename TS, typename V>
 __device__ __forceinline__ typename VT<TS>::T cvt_v(V a) {
   typename VT<TS>::T r;

@@ -4,16 +4,28 @@
 rkf45 (Cash-Karp stages + rkqs step control, src/solve.f90:158-378) with
 tolerance 1e-6 from dt = 0.005, equation 4 (g = mu = 1), from the vortex ring
 (r0 = 8) times the Pade rarefaction pulse at x0 = -10, stepped while
-t + im_t <= 20 as the reference loop does (src/gpe.f90:134).
+t + im_t <= 20 as the reference loop does (src/gpe.f90:134): about 516
+accepted steps in 529 attempts.
 
-complex128 on the GPU against the FP64 oracle, step by step: the same
-attempt count every step, accepted and next dt within 1e-8 (the embedded
-error estimate cancels about 8 digits, so two FP64 implementations agree on
-errmax to ~1e-9), and at the end psi within 1e-9 relative L2, norm and
-energy within 1e-9.  complex64 + Kahan with FP64 step control, on its own
-step sequence, against the same oracle state: density within 5e-3 relative
-L2 (its FP32 error estimates choose different steps, and its last step ends
-at a slightly different time).
+Two FP64 implementations that sum in a different order part by rounding,
+and this vortex state amplifies the difference over t = 20 (measured on
+B200: psi 1e-12 apart after a step, 5e-9 after the whole run).  rkqs then
+magnifies it: errmax is the maximum over sites of |err|/psi_scal, reached
+next to a vortex core where psi_scal is small and the embedded error has
+cancelled most of its digits, so errmax agrees to 2e-7 over the first 100
+steps and to 3e-5 by t = 20, and the next dt (errmax^-0.2) to 1e-8 and
+6e-6.  The checks, with about ten times the measured margins:
+
+* lockstep (the GPU takes the oracle's t and dt before every step, so each
+  step's step control is compared from the same input): the same attempt
+  count at every step; accepted dt and next dt within 1e-7 over the first 100
+  steps and 5e-5 over the run; psi at the end within 5e-8 relative L2, norm
+  and energy within 1e-10;
+* free run (the GPU on its own step sequence): the same numbers of steps and
+  attempts, end time within 1e-7, psi within 2e-7;
+* complex64 + Kahan with FP64 step control, on its own step sequence:
+  density within 5e-3 of the oracle (FP32 error estimates choose other steps
+  and its last step ends at a slightly different time).
 """
 import os
 
@@ -30,57 +42,69 @@ pytestmark = pytest.mark.gpu
 T_END = 20.0
 
 
-def _oracle(p):
-    return oracle.Oracle(oracle.OracleParams(nx=p.nx, ny=p.ny, nz=p.nz, xr=p.xr, yr=p.yr,
-                                             zr=p.zr, scheme="rk45", eqn_to_solve=4, bcs=2,
-                                             order=4, g=1.0, mu=1.0))
-
-
 @pytest.fixture(scope="module")
-def c2_run():
-    """The oracle's whole run with the GPU complex128 run beside it, compared
-    step by step."""
+def c2_runs():
     oracle.set_threads(os.cpu_count() or 1)
     psi0 = bench.c2_initial_state()
     p = bench.c2_params(16, False)
-    g = GpeSolver(p, dt=0.005)
-    g.set_state(psi0)
-    o = _oracle(p)
+    free = GpeSolver(p, dt=0.005)
+    free.set_state(psi0)
+    free_steps = free_attempts = 0
+    while free.t + free.im_t <= T_END:
+        free_attempts += free.solver().attempts
+        free_steps += 1
+    lock = GpeSolver(p, dt=0.005)
+    lock.set_state(psi0)
+    o = oracle.Oracle(oracle.OracleParams(nx=p.nx, ny=p.ny, nz=p.nz, xr=p.xr, yr=p.yr,
+                                          zr=p.zr, scheme="rk45", eqn_to_solve=4, bcs=2,
+                                          order=4, g=1.0, mu=1.0))
     tm = oracle.OraTime(0.0, 0.0, 0.005, 0.0, 0)
     q = psi0
-    steps = attempts = 0
-    worst_dt = 0.0
+    rows = []
     while tm.t + tm.im_t <= T_END:
+        lock.t, lock.dt = tm.t, complex(tm.dt_re, tm.dt_im)
         t_before = tm.t
-        info = g.solver()
+        info = lock.solver()
         q, em, att = o.solver(q, tm)
-        steps += 1
-        attempts += att
-        assert info.attempts == att, f"step {steps}: {info.attempts} attempts vs {att}"
-        dt_did = tm.t - t_before
-        assert info.dt_did_re == pytest.approx(dt_did, rel=1e-8), f"step {steps}"
-        assert g.dt == pytest.approx(complex(tm.dt_re, tm.dt_im), rel=1e-8), f"step {steps}"
-        worst_dt = max(worst_dt, abs(g.dt.real - tm.dt_re) / tm.dt_re)
-    out = {"steps": steps, "attempts": attempts, "t": tm.t, "psi": q, "gpu_psi": g.get_state(),
-           "gpu_t": g.t, "gpu_norm": g.get_norm(), "gpu_E": g.energy()[0],
-           "norm": o.get_norm(q), "E": o.energy(q), "worst_dt": worst_dt}
-    g.close()
+        rows.append((info.attempts, att, info.dt_did_re, tm.t - t_before, lock.dt.real,
+                     tm.dt_re))
+    out = {"rows": rows, "t": tm.t, "psi": q, "norm": o.get_norm(q), "E": o.energy(q),
+           "lock_psi": lock.get_state(), "lock_norm": lock.get_norm(),
+           "lock_E": lock.energy()[0], "free_psi": free.get_state(), "free_t": free.t,
+           "free_steps": free_steps, "free_attempts": free_attempts}
+    for s in (free, lock):
+        s.close()
     o.close()
     return out
 
 
-def test_c2_complex128_whole_run_matches_oracle(c2_run):
-    r = c2_run
-    # the reference run takes about 516 accepted steps in about 529 attempts
-    assert 400 < r["steps"] < 700 and r["attempts"] >= r["steps"]
-    assert r["gpu_t"] == pytest.approx(r["t"], rel=1e-9)
-    assert rel_l2(r["gpu_psi"], r["psi"]) < 1e-9
-    assert r["gpu_norm"] == pytest.approx(r["norm"], rel=1e-9)
-    assert r["gpu_E"] == pytest.approx(r["E"], rel=1e-9)
+def test_c2_step_control_matches_oracle_every_step(c2_runs):
+    rows = c2_runs["rows"]
+    assert 400 < len(rows) < 700
+    for k, (att_g, att_o, did_g, did_o, nxt_g, nxt_o) in enumerate(rows):
+        tol = 1e-7 if k < 100 else 5e-5
+        assert att_g == att_o, f"step {k + 1}: {att_g} attempts vs {att_o}"
+        assert did_g == pytest.approx(did_o, rel=tol), f"step {k + 1}"
+        assert nxt_g == pytest.approx(nxt_o, rel=tol), f"step {k + 1}"
 
 
-def test_c2_complex64_kahan_tracks_the_oracle(c2_run):
-    r = c2_run
+def test_c2_complex128_state_matches_oracle(c2_runs):
+    r = c2_runs
+    assert rel_l2(r["lock_psi"], r["psi"]) < 5e-8
+    assert r["lock_norm"] == pytest.approx(r["norm"], rel=1e-10)
+    assert r["lock_E"] == pytest.approx(r["E"], rel=1e-10)
+
+
+def test_c2_free_run_matches_oracle(c2_runs):
+    r = c2_runs
+    assert r["free_steps"] == len(r["rows"])
+    assert r["free_attempts"] == sum(row[1] for row in r["rows"])
+    assert r["free_t"] == pytest.approx(r["t"], rel=1e-7)
+    assert rel_l2(r["free_psi"], r["psi"]) < 2e-7
+
+
+def test_c2_complex64_kahan_tracks_the_oracle(c2_runs):
+    r = c2_runs
     psi0 = bench.c2_initial_state()
     s = GpeSolver(bench.c2_params(8, True), dt=0.005)
     s.set_state(psi0.astype(np.complex64))
@@ -91,4 +115,4 @@ def test_c2_complex64_kahan_tracks_the_oracle(c2_run):
     got = s.get_state(np.complex128)
     s.close()
     dens = rel_l2(np.abs(got) ** 2, np.abs(r["psi"]) ** 2)
-    assert dens < 5e-3, (dens, steps, r["steps"])
+    assert dens < 5e-3, (dens, steps, len(r["rows"]))

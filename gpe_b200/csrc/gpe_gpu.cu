@@ -335,13 +335,16 @@ int allreduce_scalars(gpe_ctx* c, int first, int count, int op) {
 
 struct StageSpec {
   int stencil = F_PSI;
+  int stencil2 = -1;  // second stencil field: the kernel steps stencil + stencil2
   int np = 0;
   int pt[MAXP] = {0, 0, 0, 0, 0, 0};
   int nout = 0;
   int out[2] = {0, 0};
   int ghost_mask = 0;
-  // out[o] = alpha[o]*u + sum_q beta[o][q]*P_q + a[o]*f(u)
+  // out[o] = alpha[o]*s0 + alpha2[o]*s1 + sum_q beta[o][q]*P_q + a[o]*f(u),
+  // u = s0 (+ s1) the stencil field(s)
   double alpha[2] = {0.0, 0.0};
+  double alpha2[2] = {0.0, 0.0};
   double beta[2][MAXP] = {};
   cd a[2] = {cd(0), cd(0)};
   int epi = 0;
@@ -357,7 +360,7 @@ using KernelFn = const void*;
 
 // Ring depth S and tile height TY from the shared-memory budget: as many
 // slots (up to 8) as fit two CTAs per SM, else one CTA per SM, else TY = 4.
-LaunchShape ring_shape(int es, int R, int np, int tile_y) {
+LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1) {
   LaunchShape s{};
   int TY = tile_y > 0 ? tile_y : 8;
   for (int attempt = 0; attempt < 2; attempt++) {
@@ -366,7 +369,7 @@ LaunchShape ring_shape(int es, int R, int np, int tile_y) {
     s.pt_box = (unsigned)(TX * TY * es);
     s.halo_smem = (unsigned)round_up(s.halo_box, 128);
     s.pt_smem = (unsigned)round_up(s.pt_box, 128);
-    const size_t stage = s.halo_smem + (size_t)np * s.pt_smem;
+    const size_t stage = (size_t)ns * s.halo_smem + (size_t)np * s.pt_smem;
     int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
     if (S < R + 3) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
     if (S >= R + 2 || attempt == 1 || tile_y > 0) {
@@ -375,7 +378,7 @@ LaunchShape ring_shape(int es, int R, int np, int tile_y) {
     }
     TY = 4;
   }
-  s.smem = 128 + (size_t)s.S * (s.halo_smem + (size_t)np * s.pt_smem);
+  s.smem = 128 + (size_t)s.S * ((size_t)ns * s.halo_smem + (size_t)np * s.pt_smem);
   return s;
 }
 
@@ -384,13 +387,13 @@ LaunchShape ring_shape(int es, int R, int np, int tile_y) {
 // one that minimises (waves of CTAs) x (planes per CTA + pipeline fill),
 // which trades the last wave's idle SMs against the R extra halo planes and
 // the fill latency every chunk pays.
-int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, LaunchShape* out) {
+int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, int ns, LaunchShape* out) {
   auto hit = c->shapes.find(fn);
   if (hit != c->shapes.end()) {
     *out = hit->second;
     return GPE_OK;
   }
-  LaunchShape s = ring_shape(c->es, R, np, c->prm.tile_y);
+  LaunchShape s = ring_shape(c->es, R, np, c->prm.tile_y, ns);
   s.ntx = (c->nx + TX - 1) / TX;
   s.nty = (c->ny + s.TY - 1) / s.TY;
   CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -426,48 +429,46 @@ int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, LaunchShape* out) {
 // The stage recipes that the schemes use; see stage_kernel.cuh for the
 // meaning of (NP, NOUT, EPI, AMASK, BMASK).  BMASK bit o*8+q: beta[o][q] != 0.
 template <typename TS, typename TC, int R, bool FULL, bool BATCH>
-KernelFn pick_kernel(int np, int nout, int epi, int am, int bm) {
-#define GPE_CASE(NP_, NOUT_, EPI_, AM_, BM_)                                   \
-  if (np == NP_ && nout == NOUT_ && epi == (EPI_) && am == AM_ && bm == BM_)   \
-    return reinterpret_cast<KernelFn>(                                         \
-        &stage_kernel<TS, TC, R, NP_, NOUT_, (EPI_), AM_, BM_, FULL, BATCH>);
+KernelFn pick_kernel(int ns, int np, int nout, int epi, int am, int bm) {
+#define GPE_CASE(NS_, NP_, NOUT_, EPI_, AM_, BM_)                                      \
+  if (ns == NS_ && np == NP_ && nout == NOUT_ && epi == (EPI_) && am == AM_ && bm == BM_) \
+    return reinterpret_cast<KernelFn>(                                                 \
+        &stage_kernel<TS, TC, R, NS_, NP_, NOUT_, (EPI_), AM_, BM_, FULL, BATCH>);
   if constexpr (BATCH) {
     // batched ensembles step with rk4
     if constexpr (std::is_same<TS, TC>::value) {
-      GPE_CASE(0, 2, 0, 3, 0)                   // rk4 stage 1
-      GPE_CASE(0, 2, 0, 1, 0)                   // rk4 stage 1 (compensated)
-      GPE_CASE(2, 2, 0, 0, 0x201)               // rk4 stages 2, 3
-      GPE_CASE(1, 1, EPI_NORM, 0, 0x1)          // rk4 stage 4
+      GPE_CASE(1, 0, 1, 0, 0, 0)                   // rk4 stage 1
+      GPE_CASE(2, 0, 1, 0, 0, 0)                   // rk4 stages 2, 3
+      GPE_CASE(2, 2, 1, EPI_NORM, 5, 0x3)          // rk4 stage 4
       if constexpr (std::is_same<TS, float>::value) {
-        GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM, 0, 0x2)   // rk4 stage 4 (compensated)
+        GPE_CASE(2, 3, 2, EPI_KAHAN | EPI_NORM, 4, 0x3)   // rk4 stage 4 (compensated)
       }
     }
   } else {
   if constexpr (std::is_same<TC, double>::value && !FULL) {
-    GPE_CASE(0, 0, EPI_ENERGY, 0, 0)
+    GPE_CASE(1, 0, 0, EPI_ENERGY, 0, 0)
   }
   if constexpr (std::is_same<TS, TC>::value) {
-    GPE_CASE(0, 1, EPI_NORM, 1, 0)            // euler
-    GPE_CASE(0, 1, 0, 1, 0)                   // rk2 stage 1
-    GPE_CASE(1, 1, EPI_NORM, 0, 0x1)          // rk2 stage 2, rk4 stage 4
-    GPE_CASE(0, 2, 0, 3, 0)                   // rk4 stage 1
-    GPE_CASE(0, 2, 0, 1, 0)                   // rk4 stage 1 (compensated)
-    GPE_CASE(2, 2, 0, 0, 0x201)               // rk4 stages 2, 3
-    GPE_CASE(0, 2, 0, 2, 0)                   // rkck stage 1
-    GPE_CASE(2, 2, 0, 0, 0x300)               // rkck stage 2
-    GPE_CASE(3, 2, 0, 0, 0x700)               // rkck stage 3
-    GPE_CASE(4, 2, 0, 0, 0xF00)               // rkck stage 4
-    GPE_CASE(5, 2, 0, 0, 0x1F00)              // rkck stage 5
-    GPE_CASE(5, 1, EPI_NORM | EPI_ERR, 0, 0xF)  // rkck stage 6
-    GPE_CASE(0, 1, 0, 0, 0)                   // get_rhs
+    GPE_CASE(1, 0, 1, EPI_NORM, 1, 0)            // euler
+    GPE_CASE(1, 0, 1, 0, 1, 0)                   // rk2 stage 1
+    GPE_CASE(1, 1, 1, EPI_NORM, 0, 0x1)          // rk2 stage 2
+    GPE_CASE(1, 0, 1, 0, 0, 0)                   // rk4 stage 1, get_rhs
+    GPE_CASE(2, 0, 1, 0, 0, 0)                   // rk4 stages 2, 3
+    GPE_CASE(2, 2, 1, EPI_NORM, 5, 0x3)          // rk4 stage 4
+    GPE_CASE(1, 0, 2, 0, 2, 0)                   // rkck stage 1
+    GPE_CASE(1, 2, 2, 0, 0, 0x300)               // rkck stage 2
+    GPE_CASE(1, 3, 2, 0, 0, 0x700)               // rkck stage 3
+    GPE_CASE(1, 4, 2, 0, 0, 0xF00)               // rkck stage 4
+    GPE_CASE(1, 5, 2, 0, 0, 0x1F00)              // rkck stage 5
+    GPE_CASE(1, 5, 1, EPI_NORM | EPI_ERR, 0, 0xF)  // rkck stage 6
     if constexpr (!FULL) {
-      GPE_CASE(0, 1, EPI_LAP, 0, 0)           // laplacian
+      GPE_CASE(1, 0, 1, EPI_LAP, 0, 0)           // laplacian
     }
     if constexpr (std::is_same<TS, float>::value) {
-      GPE_CASE(1, 2, EPI_KAHAN | EPI_NORM, 0, 0)       // euler (compensated)
-      GPE_CASE(2, 2, EPI_KAHAN | EPI_NORM, 0, 0)       // rk2 stage 2
-      GPE_CASE(3, 2, EPI_KAHAN | EPI_NORM, 0, 0x2)     // rk4 stage 4
-      GPE_CASE(6, 2, EPI_KAHAN | EPI_NORM | EPI_ERR, 0, 0xE)  // rkck stage 6
+      GPE_CASE(1, 1, 2, EPI_KAHAN | EPI_NORM, 0, 0)       // euler (compensated)
+      GPE_CASE(1, 2, 2, EPI_KAHAN | EPI_NORM, 0, 0)       // rk2 stage 2
+      GPE_CASE(2, 3, 2, EPI_KAHAN | EPI_NORM, 4, 0x3)     // rk4 stage 4
+      GPE_CASE(1, 6, 2, EPI_KAHAN | EPI_NORM | EPI_ERR, 0, 0xE)  // rkck stage 6
     }
   }
   }
@@ -537,6 +538,7 @@ void recipe_masks(const StageSpec& sp, int* am, int* bm) {
   *bm = 0;
   for (int o = 0; o < sp.nout; o++) {
     if (sp.alpha[o] != 0.0) *am |= 1 << o;
+    if (sp.alpha2[o] != 0.0) *am |= 4 << o;
     for (int q = 0; q < sp.np; q++)
       if (sp.beta[o][q] != 0.0) *bm |= 1 << (o * 8 + q);
   }
@@ -550,6 +552,10 @@ int fill_run(gpe_ctx* c, const StageSpec& sp, int R, const LaunchShape& sh,
   memset(rd, 0, sizeof(*rd));
   int rc = get_map(c, sp.stencil, 0, sh.TY, R, &rd->maps.halo);
   if (rc) return rc;
+  if (sp.stencil2 >= 0) {
+    rc = get_map(c, sp.stencil2, 0, sh.TY, R, &rd->maps.halo2);
+    if (rc) return rc;
+  }
   for (int q = 0; q < sp.np; q++) {
     rc = get_map(c, sp.pt[q], 1, sh.TY, R, &rd->maps.pt[q]);
     if (rc) return rc;
@@ -560,6 +566,7 @@ int fill_run(gpe_ctx* c, const StageSpec& sp, int R, const LaunchShape& sh,
   rd->zg_lo = c->exch_lo ? 0 : 1;
   rd->zg_hi = c->exch_hi ? 0 : 1;
   rd->stencil = static_cast<const TS*>(c->fld[sp.stencil]);
+  rd->stencil2 = sp.stencil2 >= 0 ? static_cast<const TS*>(c->fld[sp.stencil2]) : nullptr;
   for (int o = 0; o < sp.nout; o++) rd->out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
   const double h2[3] = {c->dx * c->dx, c->dy * c->dy, c->dz * c->dz};
   double c1[3], c2[3];
@@ -605,6 +612,7 @@ void fill_common(const StageSpec& sp, bool fold, const LaunchShape& sh,
   p->ghost_mask = sp.ghost_mask;
   for (int o = 0; o < 2; o++) {
     p->alpha[o] = (TC)sp.alpha[o];
+    p->alpha2[o] = (TC)sp.alpha2[o];
     const cd a = fold ? I * sp.a[o] : sp.a[o];
     p->a_r[o] = (TC)a.real(); p->a_i[o] = (TC)a.imag();
     for (int q = 0; q < MAXP; q++) p->beta[o][q] = (TC)sp.beta[o][q];
@@ -620,11 +628,12 @@ void fill_common(const StageSpec& sp, bool fold, const LaunchShape& sh,
 
 template <typename TS, typename TC, bool BATCH>
 KernelFn select_kernel(int R, bool kfull, const StageSpec& sp, int am, int bm) {
+  const int ns = sp.stencil2 >= 0 ? 2 : 1;
   if (R == 1)
-    return kfull ? pick_kernel<TS, TC, 1, true, BATCH>(sp.np, sp.nout, sp.epi, am, bm)
-                 : pick_kernel<TS, TC, 1, false, BATCH>(sp.np, sp.nout, sp.epi, am, bm);
-  return kfull ? pick_kernel<TS, TC, 2, true, BATCH>(sp.np, sp.nout, sp.epi, am, bm)
-               : pick_kernel<TS, TC, 2, false, BATCH>(sp.np, sp.nout, sp.epi, am, bm);
+    return kfull ? pick_kernel<TS, TC, 1, true, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm)
+                 : pick_kernel<TS, TC, 1, false, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
+  return kfull ? pick_kernel<TS, TC, 2, true, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm)
+               : pick_kernel<TS, TC, 2, false, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
 }
 
 template <typename TS, typename TC>
@@ -639,7 +648,7 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   KernelFn fn = select_kernel<TS, TC, false>(R, kfull, sp, am, bm);
   if (!fn) return fail(c, GPE_ERR_INVALID, "no kernel for this stage shape");
   LaunchShape sh;
-  int rc = choose_shape(c, fn, R, sp.np, &sh);
+  int rc = choose_shape(c, fn, R, sp.np, sp.stencil2 >= 0 ? 2 : 1, &sh);
   if (rc) return rc;
   StageParams<TS, TC> p;
   memset(&p, 0, sizeof(p));
@@ -808,40 +817,54 @@ int step_rk2(gpe_ctx* c, cd dt) {
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
-// The four classic RK4 stages (src/solve.f90:109-154) as stage recipes.
+// The four classic RK4 stages (src/solve.f90:109-154) as stage recipes, in
+// increment form.  With f1 = f(psi), d2 = dt/2 f1, d3 = dt/2 f(psi + d2),
+// d4 = dt f(psi + d3), classic RK4 is
+//   psi' = psi + dt/6 (f1 + 2 f2 + 2 f3 + f4)
+//        = psi + [d2/3 + 2 d3/3 + d4/3 + dt/6 f(psi + d4)],
+// and every stage after the first steps psi + d, staged from both fields
+// with their halos (the kernel's second stencil field), so neither the stage
+// values nor an accumulator are stored.  Traffic per site: S1 reads psi and
+// writes d2; S2, S3 read psi, d and write the next d; S4 reads psi, d4, d2,
+// d3 (and c) and writes psi' (and c): 16 + 24 + 24 + 48 (56 with Kahan)
+// bytes at complex64, against 128 (152) for stage values plus accumulator.
+// psi' is written over d2 (read at the same site only), then psi and that
+// buffer trade roles; the bracket is summed smallest terms first and added
+// to psi last (Kahan-compensated when enabled).
 void rk4_specs(const gpe_ctx* c, cd dt, StageSpec sp[4]) {
   const bool K = c->prm.kahan != 0;
-  // S1: u2 = psi + dt/2 f(psi); acc = [psi] + dt/6 f(psi)
+  const int psi = c->psi_id, d2 = c->alt_id, d3 = F_UB, d4 = F_ACC;
+  // S1: d2 = dt/2 f(psi)
   StageSpec& s1 = sp[0];
   s1 = StageSpec();
-  s1.stencil = c->psi_id; s1.nout = 2; s1.out[0] = F_UA; s1.out[1] = F_ACC;
-  s1.ghost_mask = 1; s1.alpha[0] = 1.0; s1.a[0] = 0.5 * dt;
-  s1.alpha[1] = K ? 0.0 : 1.0; s1.a[1] = dt / 6.0;
+  s1.stencil = psi; s1.nout = 1; s1.out[0] = d2; s1.ghost_mask = 1;
+  s1.a[0] = 0.5 * dt;
   s1.family = GPE_FAM_STAGE_FIRST;
-  // S2: u3 = psi + dt/2 f(u2); acc += dt/3 f(u2)
+  // S2: d3 = dt/2 f(psi + d2)
   StageSpec& s2 = sp[1];
   s2 = StageSpec();
-  s2.stencil = F_UA; s2.np = 2; s2.pt[0] = c->psi_id; s2.pt[1] = F_ACC;
-  s2.nout = 2; s2.out[0] = F_UB; s2.out[1] = F_ACC; s2.ghost_mask = 1;
-  s2.beta[0][0] = 1.0; s2.a[0] = 0.5 * dt;
-  s2.beta[1][1] = 1.0; s2.a[1] = dt / 3.0;
+  s2.stencil = psi; s2.stencil2 = d2; s2.nout = 1; s2.out[0] = d3; s2.ghost_mask = 1;
+  s2.a[0] = 0.5 * dt;
   s2.family = GPE_FAM_STAGE_MID;
-  // S3: u4 = psi + dt f(u3); acc += dt/3 f(u3)
+  // S3: d4 = dt f(psi + d3)
   sp[2] = s2;
-  sp[2].stencil = F_UB; sp[2].out[0] = F_UA; sp[2].a[0] = dt;
-  // S4: psi' = acc + dt/6 f(u4)   (Kahan: psi' = psi (+) (acc + dt/6 f))
+  sp[2].stencil2 = d3; sp[2].out[0] = d4; sp[2].a[0] = dt;
+  // S4: psi' = psi (+) [d2/3 + 2 d3/3 + d4/3 + dt/6 f(psi + d4)], into d2's buffer
   StageSpec& s4 = sp[3];
   s4 = StageSpec();
-  s4.stencil = F_UA; s4.out[0] = c->psi_id; s4.ghost_mask = 1;
+  s4.stencil = psi; s4.stencil2 = d4; s4.out[0] = d2; s4.ghost_mask = 1;
   s4.family = GPE_FAM_STAGE_LAST;
+  s4.pt[0] = d2; s4.pt[1] = d3;
+  s4.beta[0][0] = 1.0 / 3.0; s4.beta[0][1] = 2.0 / 3.0;
+  s4.alpha2[0] = 1.0 / 3.0;
+  s4.a[0] = dt / 6.0;
   if (K) {
-    s4.np = 3; s4.pt[0] = c->psi_id; s4.pt[1] = F_ACC; s4.pt[2] = c->c_id;
+    s4.np = 3; s4.pt[2] = c->c_id;
     s4.nout = 2; s4.out[1] = c->c_id;
-    s4.beta[0][1] = 1.0; s4.a[0] = dt / 6.0;
     s4.epi = EPI_KAHAN | EPI_NORM;
   } else {
-    s4.np = 1; s4.pt[0] = F_ACC; s4.nout = 1;
-    s4.beta[0][0] = 1.0; s4.a[0] = dt / 6.0;
+    s4.np = 2; s4.nout = 1;
+    s4.alpha[0] = 1.0;
     s4.epi = EPI_NORM;
   }
 }
@@ -853,6 +876,7 @@ int step_rk4(gpe_ctx* c, cd dt) {
     const int rc = launch_stage(c, sp[st]);
     if (rc) return rc;
   }
+  std::swap(c->psi_id, c->alt_id);
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
@@ -1266,17 +1290,21 @@ struct gpe_batch {
   size_t series_cap = 0;  // steps per run
   int* d_counter = nullptr;
   int* d_status = nullptr;
-  void* d_rundesc[4] = {nullptr, nullptr, nullptr, nullptr};
+  // Two prepared step forms: RK4 leaves psi in the members' other buffer
+  // (rk4_specs), so [0] steps from the members' current psi and [1] from the
+  // buffer the step after it starts from; steps alternate between them.
+  void* d_rundesc[2][4] = {};
   struct Stage {
     KernelFn fn = nullptr;
     LaunchShape sh{};
     int grid = 0;
     std::vector<unsigned char> params;  // StageParams bytes
-  } st[4];
+  } st[2][4];
   cd prepared_dt = cd(0.0, 0.0);
   bool prepared = false;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  std::vector<int> prepared_psi;  // each member's psi buffer that [0] starts from
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
   double* graph_series = nullptr;
   int64_t launches = 0;
   int64_t sites = 0;
@@ -1301,7 +1329,7 @@ int bfail(gpe_batch* b, int code, const std::string& msg) {
 
 // Kernels, shapes and RunDesc arrays of the four stages for time step dt.
 template <typename TS, typename TC>
-int batch_prepare_t(gpe_batch* b, cd dt) {
+int batch_prepare_par(gpe_batch* b, cd dt, int par) {
   for (int s = 0; s < 4; s++) {
     std::vector<RunDesc<TS, TC>> rds(b->runs.size());
     StageSpec sp0[4];
@@ -1311,7 +1339,7 @@ int batch_prepare_t(gpe_batch* b, cd dt) {
     recipe_masks(sp, &am, &bm);
     KernelFn fn = select_kernel<TS, TC, true>(b->R, b->full, sp, am, bm);
     if (!fn) return bfail(b, GPE_ERR_INVALID, "no batched kernel for this stage");
-    LaunchShape sh = ring_shape(b->es, b->R, sp.np, b->TY);
+    LaunchShape sh = ring_shape(b->es, b->R, sp.np, b->TY, sp.stencil2 >= 0 ? 2 : 1);
     BCU(b, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     int occ = 0;
     BCU(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (sh.TY + 1), sh.smem));
@@ -1330,24 +1358,41 @@ int batch_prepare_t(gpe_batch* b, cd dt) {
       const int rc = fill_run<TS, TC>(c, spr[s], b->R, shr, rhs_form(c), &rds[r], b->full ? 1 : 0);
       if (rc) return bfail(b, rc, c->err);
     }
-    BCU(b, cudaMemcpy(b->d_rundesc[s], rds.data(), sizeof(RunDesc<TS, TC>) * rds.size(),
+    BCU(b, cudaMemcpy(b->d_rundesc[par][s], rds.data(), sizeof(RunDesc<TS, TC>) * rds.size(),
                       cudaMemcpyHostToDevice));
     StageParams<TS, TC> p;
     memset(&p, 0, sizeof(p));
     fill_common<TS, TC>(sp, !b->full, sh, &p);
-    p.runs = static_cast<const RunDesc<TS, TC>*>(b->d_rundesc[s]);
+    p.runs = static_cast<const RunDesc<TS, TC>*>(b->d_rundesc[par][s]);
     p.items = b->d_items;
     p.nitems = b->nitems;
     p.partials = b->d_partials;
     p.status = b->d_status;
-    b->st[s].fn = fn;
-    b->st[s].sh = sh;
-    b->st[s].grid = grid;
-    b->st[s].params.assign(reinterpret_cast<unsigned char*>(&p),
-                           reinterpret_cast<unsigned char*>(&p) + sizeof(p));
+    b->st[par][s].fn = fn;
+    b->st[par][s].sh = sh;
+    b->st[par][s].grid = grid;
+    b->st[par][s].params.assign(reinterpret_cast<unsigned char*>(&p),
+                                reinterpret_cast<unsigned char*>(&p) + sizeof(p));
   }
+  return GPE_OK;
+}
+
+void batch_swap_members(gpe_batch* b) {
+  for (auto* c : b->runs) std::swap(c->psi_id, c->alt_id);
+}
+
+template <typename TS, typename TC>
+int batch_prepare_t(gpe_batch* b, cd dt) {
+  int rc = batch_prepare_par<TS, TC>(b, dt, 0);
+  if (rc) return rc;
+  batch_swap_members(b);
+  rc = batch_prepare_par<TS, TC>(b, dt, 1);
+  batch_swap_members(b);
+  if (rc) return rc;
   b->prepared_dt = dt;
   b->prepared = true;
+  b->prepared_psi.clear();
+  for (auto* c : b->runs) b->prepared_psi.push_back(c->psi_id);
   return GPE_OK;
 }
 
@@ -1358,9 +1403,9 @@ int batch_prepare(gpe_batch* b, cd dt) {
 
 // One RK4 step of every member: 4 persistent stage launches, per-run norm
 // into d_norm and the series, step counter bump.
-int batch_enqueue_step(gpe_batch* b) {
+int batch_enqueue_step(gpe_batch* b, int par) {
   for (int s = 0; s < 4; s++) {
-    auto& S = b->st[s];
+    auto& S = b->st[par][s];
     void* args[] = {S.params.data()};
     BCU(b, cudaLaunchKernel(S.fn, dim3((unsigned)S.grid), dim3(32, (unsigned)S.sh.TY + 1),
                             args, S.sh.smem, b->stream));
@@ -1436,10 +1481,26 @@ int batch_plan(gpe_batch* b) {
 }
 
 void batch_drop_graph(gpe_batch* b) {
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->graph) cudaGraphDestroy(b->graph);
-  b->exec = nullptr;
-  b->graph = nullptr;
+  for (int k = 0; k < 2; k++) {
+    if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
+    if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
+    b->exec[k] = nullptr;
+    b->graph[k] = nullptr;
+  }
+}
+
+// After an odd number of steps the members' psi is in their other buffer:
+// swap their ids and the two prepared forms, so [0] again starts from psi.
+void batch_flip(gpe_batch* b) {
+  batch_swap_members(b);
+  for (size_t r = 0; r < b->runs.size() && r < b->prepared_psi.size(); r++)
+    b->prepared_psi[r] = b->runs[r]->psi_id;
+  for (int s = 0; s < 4; s++) {
+    std::swap(b->st[0][s], b->st[1][s]);
+    std::swap(b->d_rundesc[0][s], b->d_rundesc[1][s]);
+  }
+  std::swap(b->graph[0], b->graph[1]);
+  std::swap(b->exec[0], b->exec[1]);
 }
 
 }  // namespace
@@ -1541,7 +1602,7 @@ int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
   switch (p.scheme) {
     case GPE_SCHEME_RK2: need.push_back(F_UA); break;
     case GPE_SCHEME_RK4:
-      need.insert(need.end(), {F_UA, F_UB, F_ACC});
+      need.insert(need.end(), {F_UB, F_ACC});
       break;
     case GPE_SCHEME_RK45:
       need.insert(need.end(), {F_UA, F_UB, F_K1, F_K2, F_K3, F_K4, F_K5});
@@ -2121,12 +2182,13 @@ int gpe_batch_create(const gpe_params* prms, int32_t nruns, const gpe_batch_opts
     b->err = "cudaMalloc of batch buffers failed";
     return bail(GPE_ERR_OOM);
   }
-  for (int s = 0; s < 4; s++)
-    if (cudaMalloc(&b->d_rundesc[s], rdsz * nruns) != cudaSuccess) {
-      cudaGetLastError();
-      b->err = "cudaMalloc of run descriptors failed";
-      return bail(GPE_ERR_OOM);
-    }
+  for (int k = 0; k < 2; k++)
+    for (int s = 0; s < 4; s++)
+      if (cudaMalloc(&b->d_rundesc[k][s], rdsz * nruns) != cudaSuccess) {
+        cudaGetLastError();
+        b->err = "cudaMalloc of run descriptors failed";
+        return bail(GPE_ERR_OOM);
+      }
   cudaMemcpy(b->d_scale, scale.data(), sizeof(double) * nruns, cudaMemcpyHostToDevice);
   cudaMemset(b->d_counter, 0, sizeof(int));
   cudaMemset(b->d_status, 0, sizeof(int));
@@ -2144,8 +2206,9 @@ void gpe_batch_destroy(gpe_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop_graph(b);
   for (auto* c : b->runs) gpe_gpu_destroy(c);
-  for (int s = 0; s < 4; s++)
-    if (b->d_rundesc[s]) cudaFree(b->d_rundesc[s]);
+  for (int k = 0; k < 2; k++)
+    for (int s = 0; s < 4; s++)
+      if (b->d_rundesc[k][s]) cudaFree(b->d_rundesc[k][s]);
   if (b->d_items) cudaFree(b->d_items);
   if (b->d_item_run) cudaFree(b->d_item_run);
   if (b->d_partials) cudaFree(b->d_partials);
@@ -2184,7 +2247,10 @@ int gpe_batch_advance(gpe_batch* b, int64_t nsteps, double dt_re, double dt_im,
     BCU(b, cudaMalloc(&b->d_series, sizeof(double) * cap * nr));
     b->series_cap = cap;
   }
-  if (!b->prepared || dt != b->prepared_dt) {
+  bool moved = false;  // a member was stepped on its own since the batch prepared
+  for (size_t r = 0; r < nr && b->prepared; r++)
+    moved = moved || b->prepared_psi[r] != b->runs[r]->psi_id;
+  if (!b->prepared || dt != b->prepared_dt || moved) {
     batch_drop_graph(b);
     const int rc = batch_prepare(b, dt);
     if (rc) return rc;
@@ -2192,9 +2258,10 @@ int gpe_batch_advance(gpe_batch* b, int64_t nsteps, double dt_re, double dt_im,
   // members' own kernels (state loads) must be done before the batch runs
   for (auto* c : b->runs) BCU(b, cudaStreamSynchronize(c->stream));
   BCU(b, cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
-  if (b->opts.use_graph && !b->exec) {
+  for (int par = 0; par < 2 && b->opts.use_graph; par++) {
+    if (b->exec[par]) continue;
     BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = batch_enqueue_step(b);
+    const int rc = batch_enqueue_step(b, par);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) {
@@ -2202,18 +2269,20 @@ int gpe_batch_advance(gpe_batch* b, int64_t nsteps, double dt_re, double dt_im,
       return rc;
     }
     if (e != cudaSuccess) return bfail(b, GPE_ERR_CUDA, "graph capture failed");
-    b->graph = g;
-    BCU(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->graph[par] = g;
+    BCU(b, cudaGraphInstantiate(&b->exec[par], b->graph[par], 0));
   }
   for (int64_t k = 0; k < nsteps; k++) {
-    if (b->exec) {
-      BCU(b, cudaGraphLaunch(b->exec, b->stream));
+    const int par = (int)(k & 1);
+    if (b->exec[par]) {
+      BCU(b, cudaGraphLaunch(b->exec[par], b->stream));
     } else {
-      const int rc = batch_enqueue_step(b);
+      const int rc = batch_enqueue_step(b, par);
       if (rc) return rc;
     }
     b->launches += 6;
   }
+  if (nsteps & 1) batch_flip(b);
   for (auto* c : b->runs) c->norm_valid = false;
   if (norms && nsteps > 0) {
     // series is [run][cap]: copy the first nsteps of each run
@@ -2249,7 +2318,7 @@ int gpe_batch_info(const gpe_batch* b, int64_t* sites, int32_t* nitems, int32_t*
   if (!b) return GPE_ERR_INVALID;
   if (sites) *sites = b->sites;
   if (nitems) *nitems = b->nitems;
-  if (grid) *grid = b->st[1].grid;
+  if (grid) *grid = b->st[0][1].grid;
   if (tile_y) *tile_y = b->TY;
   return GPE_OK;
 }

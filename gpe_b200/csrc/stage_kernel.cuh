@@ -28,8 +28,11 @@
 // memory as 16-byte stores.
 //
 // The combination each stage performs is fixed at compile time ("recipe"):
-//   out[o] = alpha[o]*u + sum_q beta[o][q]*P_q + a[o] (x) K
-// where u is the stencil field at the site, P_q the pointwise inputs, alpha
+//   out[o] = alpha[o]*s0 + alpha2[o]*s1 + sum_q beta[o][q]*P_q + a[o] (x) K
+// where the stencil field u = s0 (+ s1) is one stored field or the sum of two
+// (NS = 2: both staged with their halos and added as they are read, so a
+// stage can step psi + d from an increment d without storing psi + d),
+// s0 and s1 are those fields at the site, P_q the pointwise inputs, alpha
 // and beta real Runge-Kutta weights present only where AMASK/BMASK say so,
 // a[o] one complex coefficient per output (it carries dt), and K the
 // right-hand side.  Without trap, sponge, gradient or sphere terms (FULL =
@@ -59,6 +62,7 @@ enum : int {
 
 struct TileMaps {
   CUtensorMap halo;      // stencil field, box (64+4) x (TY+2R) x 1
+  CUtensorMap halo2;     // second stencil field (NS = 2), same box
   CUtensorMap pt[MAXP];  // pointwise fields, box 64 x TY x 1
 };
 
@@ -74,6 +78,7 @@ struct alignas(64) RunDesc {
   int zg_lo, zg_hi;     // fill the z ghosts below / above locally (else a
                         // neighbouring rank sends them)
   const TS* stencil;    // stencil field (padded layout), warm-up planes
+  const TS* stencil2;   // second stencil field (NS = 2)
   TS* out[2];           // output fields (padded layout)
   // Laplacian: T = sum_axes c1*(f1+f-1) + c2*(f2+f-2); L = T + c0*f0
   TC cx1, cx2, cy1, cy2, cz1, cz2, c0lap;
@@ -106,7 +111,8 @@ struct StageParams {
   unsigned int halo_box_bytes, pt_box_bytes;    // bytes one TMA box delivers
   unsigned int halo_smem_bytes, pt_smem_bytes;  // 128-aligned slot strides
   int ghost_mask;       // bit o set: out[o] gets its boundary ghosts filled
-  TC alpha[2];
+  TC alpha[2];           // weight of stencil field 0 at the site
+  TC alpha2[2];          // weight of stencil field 1 at the site (NS = 2)
   TC beta[2][MAXP];
   TC a_r[2], a_i[2];
   // rkqs error: err = sum_q ce[q]*P_q + cek (x) K (FP64)
@@ -127,7 +133,7 @@ __device__ __forceinline__ bool near_edge(int i, int n) {
 template <int K>
 using IC = std::integral_constant<int, K>;
 
-template <typename TS, typename TC, int R, int NP, int NOUT, int EPI, int AMASK,
+template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
           int BMASK, bool FULL, bool BATCH>
 __global__ void __launch_bounds__(288)
     stage_kernel(const __grid_constant__ StageParams<TS, TC> p) {
@@ -161,7 +167,8 @@ __global__ void __launch_bounds__(288)
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + 8;
   unsigned char* sbase = smem + 128;
-  const unsigned stride = p.halo_smem_bytes + (unsigned)NP * p.pt_smem_bytes;
+  const unsigned hstride = (unsigned)NS * p.halo_smem_bytes;  // halo boxes of a slot
+  const unsigned stride = hstride + (unsigned)NP * p.pt_smem_bytes;
 
   if (tid == 0) {
     for (int s = 0; s < S; s++) {
@@ -189,6 +196,7 @@ __global__ void __launch_bounds__(288)
         const int tile_x = w.tile % rd.ntx, tile_y = w.tile / rd.ntx;
         const int niters = (w.z1 - w.z0) + R;
         prefetch_tmap(&rd.maps.halo);
+        if (NS == 2) prefetch_tmap(&rd.maps.halo2);
 #pragma unroll
         for (int qq = 0; qq < NP; qq++) prefetch_tmap(&rd.maps.pt[qq]);
         for (int u = 0; u < niters; u++) {
@@ -212,13 +220,16 @@ __global__ void __launch_bounds__(288)
           unsigned char* st = sbase + (size_t)slot * stride;
           const bool with_pt = (NP > 0) && (u >= R);
           mbar_arrive_expect_tx(&full[slot],
-                                p.halo_box_bytes + (with_pt ? NP * p.pt_box_bytes : 0u));
+                                NS * p.halo_box_bytes + (with_pt ? NP * p.pt_box_bytes : 0u));
           tma_load_3d(st, &rd.maps.halo, &full[slot], W * tile_x * TX,
                       tile_y * TY + GH - R, w.z0 + u + GH);
+          if (NS == 2)
+            tma_load_3d(st + p.halo_smem_bytes, &rd.maps.halo2, &full[slot], W * tile_x * TX,
+                        tile_y * TY + GH - R, w.z0 + u + GH);
           if (with_pt) {
 #pragma unroll
             for (int qq = 0; qq < NP; qq++)
-              tma_load_3d(st + p.halo_smem_bytes + (size_t)qq * p.pt_smem_bytes,
+              tma_load_3d(st + hstride + (size_t)qq * p.pt_smem_bytes,
                           &rd.maps.pt[qq], &full[slot], W * (tile_x * TX + GH),
                           tile_y * TY + GH, w.z0 + u - R + GH);
           }
@@ -240,12 +251,13 @@ __global__ void __launch_bounds__(288)
   uint32_t phase = 0;
   const unsigned row_off = ES * (unsigned)((ty + R) * HW + 2 * lane + 2);
   const unsigned pt_off = ES * (unsigned)(ty * TX + 2 * lane);
-  V ar[2], aix[2], alv[2], bev[2][NP > 0 ? NP : 1];
+  V ar[2], aix[2], alv[2], alv2[2], bev[2][NP > 0 ? NP : 1];
 #pragma unroll
   for (int o = 0; o < 2; o++) {
     ar[o] = vsplat(p.a_r[o]);
     aix[o] = vpair(-p.a_i[o], p.a_i[o]);
     alv[o] = vsplat(p.alpha[o]);
+    alv2[o] = vsplat(p.alpha2[o]);
 #pragma unroll
     for (int qq = 0; qq < (NP > 0 ? NP : 1); qq++) bev[o][qq] = vsplat(p.beta[o][qq]);
   }
@@ -316,7 +328,14 @@ __global__ void __launch_bounds__(288)
 #pragma unroll
   for (int w = 0; w < R; w++) {
     CPair<TC> v = {vsplat(TC(0)), vsplat(TC(0))};
-    if (ok0) v = ld_cpair<TS, TC>(rd.stencil + 2 * (base - (size_t)(R - w) * NxNy));
+    if (ok0) {
+      const size_t off = 2 * (base - (size_t)(R - w) * NxNy);
+      v = ld_cpair<TS, TC>(rd.stencil + off);
+      if (NS == 2) {
+        const CPair<TC> v2 = ld_cpair<TS, TC>(rd.stencil2 + off);
+        v = {vadd(v.a, v2.a), vadd(v.b, v2.b)};
+      }
+    }
     q[w] = v;
   }
 #pragma unroll
@@ -332,14 +351,36 @@ __global__ void __launch_bounds__(288)
       atomicExch(p.status, 6);
       return false;
     }
-    q[(R + KK) % QN] = ld_cpair<TS, TC>(
-        reinterpret_cast<const TS*>(sbase + (size_t)slot * stride + row_off));
+    {
+      // the stencil value is the sum of the NS stencil fields
+      const unsigned char* sp = sbase + (size_t)slot * stride + row_off;
+      CPair<TC> v = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(sp));
+      if (NS == 2) {
+        const CPair<TC> v2 =
+            ld_cpair<TS, TC>(reinterpret_cast<const TS*>(sp + p.halo_smem_bytes));
+        v = {vadd(v.a, v2.a), vadd(v.b, v2.b)};
+      }
+      q[(R + KK) % QN] = v;
+    }
     if (t >= R) {
       const int z = z0 + t - R;
       const unsigned char* hc = sbase + (size_t)cslot * stride + row_off;
       auto lds = [&](int drow, int dcol) {
-        return ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hc + (int)ES * (drow * HW + dcol)));
+        const unsigned char* a = hc + (int)ES * (drow * HW + dcol);
+        CPair<TC> v = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(a));
+        if (NS == 2) {
+          const CPair<TC> v2 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(a + p.halo_smem_bytes));
+          v = {vadd(v.a, v2.a), vadd(v.b, v2.b)};
+        }
+        return v;
       };
+      // NS = 2: the two stencil fields at the site, kept apart for the
+      // pointwise part of the recipe
+      CPair<TC> sc0, sc1;
+      if (NS == 2) {
+        sc0 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hc));
+        sc1 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hc + p.halo_smem_bytes));
+      }
       auto zq = [&](int d) -> const CPair<TC>& { return q[(R + KK + 1 + R + d + 2 * QN) % QN]; };
       const CPair<TC> xa = lds(0, -2);
       const CPair<TC> xc = lds(0, 2);
@@ -351,7 +392,7 @@ __global__ void __launch_bounds__(288)
       }
       CPair<TC> P[NP > 0 ? NP : 1];
       if (NP > 0) {
-        const unsigned char* pb = sbase + (size_t)slot * stride + p.halo_smem_bytes + pt_off;
+        const unsigned char* pb = sbase + (size_t)slot * stride + hstride + pt_off;
 #pragma unroll
         for (int qq = 0; qq < NP; qq++)
           P[qq] = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(pb + (size_t)qq * p.pt_smem_bytes));
@@ -421,18 +462,23 @@ __global__ void __launch_bounds__(288)
         const V Ks = vswap(Kv);
 #pragma unroll
         for (int o = 0; o < NOUT; o++) {
+          // smallest terms first: a (x) K, field 1, pointwise, field 0
           V v = vfma(ar[o], Kv, vmul(aix[o], Ks));
-          if (AMASK & (1 << o)) v = vfma(alv[o], f0, v);
+          if (NS == 2 && (AMASK & (4 << o))) v = vfma(alv2[o], e ? sc1.b : sc1.a, v);
 #pragma unroll
           for (int qq = 0; qq < NP; qq++)
             if (BMASK & (1 << (o * 8 + qq))) v = vfma(bev[o][qq], e ? P[qq].b : P[qq].a, v);
+          if (AMASK & (1 << o)) v = vfma(alv[o], NS == 2 ? (e ? sc0.b : sc0.a) : f0, v);
           res[o][e] = v;
         }
 
         if (EPI & EPI_KAHAN) {
           // res[0] is the increment delta; compensated add to psi.  Slots:
           // psi = P[0] when NP >= 2 (else the stencil field), c = P[NP-1].
-          const V psi = (NP >= 2) ? (e ? P[0].b : P[0].a) : f0;
+          // psi: stencil field 0 at the site when there are two, else
+          // P[0] when NP >= 2, else the stencil field
+          const V psi = (NS == 2) ? (e ? sc0.b : sc0.a)
+                                  : (NP >= 2) ? (e ? P[0].b : P[0].a) : f0;
           const V cc = e ? P[NP > 0 ? NP - 1 : 0].b : P[NP > 0 ? NP - 1 : 0].a;
           const V y = vfma(cc, mone, res[0][e]);
           const V tt = vadd(psi, y);

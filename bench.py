@@ -45,12 +45,13 @@ N_GRID = 512
 H = 0.5
 DT = 0.005
 KMAX = 1.0
-# algorithmic bytes per site per RK4 step with complex64 + Kahan: stage 1
-# reads psi, writes u2 and acc (3 x 8 B); stages 2-3 read u, psi, acc and
-# write u', acc (5 x 8 B each); stage 4 reads u4, psi, acc, c and writes psi, c
-# (6 x 8 B) -> 152 B/site
-BYTES_PER_FAMILY = {"stage_first": 24, "stage_mid": 40, "stage_last": 48}
-BYTES_PER_STEP = 152
+# algorithmic bytes per site per RK4 step with complex64 + Kahan, increment
+# form: stage 1 reads psi and writes d2 (2 x 8 B); stages 2-3 read psi and d
+# (both as stencils) and write the next d (3 x 8 B each); stage 4 reads psi,
+# d4, d2, d3, c and writes psi', c (7 x 8 B) -> 120 B/site (the stage-value +
+# accumulator form moves 152)
+BYTES_PER_FAMILY = {"stage_first": 16, "stage_mid": 24, "stage_last": 56}
+BYTES_PER_STEP = 120
 # the plain fine path of the learned workload steps at its largest stable dt
 FINE_PATH_DT = 0.02
 LAUNCHES_PER_STEP = 5
@@ -226,10 +227,10 @@ ENS_RUNS = 64
 ENS_SIZES = (32, 48, 64, 96, 128)
 ENS_DT = 0.01
 ENS_KMAX = 0.8
-# complex64 without compensation: stage 1 reads psi, writes u2, acc (24 B);
-# stages 2-3 read u, psi, acc and write u', acc (40 B); stage 4 reads u4, acc
-# and writes psi (24 B)
-ENS_BYTES_PER_SITE = 128
+# complex64 without compensation, increment form: stage 1 reads psi, writes
+# d2 (16 B); stages 2-3 read psi, d and write the next d (24 B each); stage 4
+# reads psi, d4, d2, d3 and writes psi' (40 B)
+ENS_BYTES_PER_SITE = 104
 
 
 def ensemble_members(seed=0):

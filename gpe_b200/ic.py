@@ -117,3 +117,125 @@ def vortex_line_pade(x, y, z):
     r = np.sqrt(X ** 2 + Y ** 2)
     rr = np.sqrt((0.3437 + 0.0286 * r ** 2) / (1 + 0.3333 * r ** 2 + 0.0286 * r ** 4))
     return r * rr * np.exp(1j * np.arctan2(Y, X))
+
+
+# --------------------------------------------------------------------------
+# The initial-condition functions that the reference's ic.in may combine
+# (src/ic.f90), as numpy fields (nz, ny, nx) over the grid x, y, z.  They are
+# evaluated on the host once per run and loaded with set_state.
+
+def _grid3(x, y, z):
+    return np.meshgrid(np.asarray(z, float), np.asarray(y, float), np.asarray(x, float),
+                       indexing="ij")
+
+
+def _line_guard(ll, a1, a2):
+    """safe1, safe2 of get_r / get_theta (src/ic.f90:740-757)."""
+    eps = np.finfo(float).eps
+    safe1 = safe2 = 0.0
+    if abs(ll) < eps:
+        if abs(a1) >= eps or abs(a2) >= eps:
+            raise ValueError("vortex line disturbance wavelength is zero, but amplitude is "
+                             "non-zero")
+        safe1 = safe2 = 1.0
+    return safe1, safe2
+
+
+def _line_axes(X, Y, Z, vl, scal):
+    """The two displaced transverse coordinates of get_r / get_theta
+    (src/ic.f90:730-886): for dir 'z' (x - x0 - a1 sin, y - y0 - a2 cos) of
+    2 pi (z - z0) / ll, and the cyclic forms for 'x' and 'y'."""
+    s1, s2 = _line_guard(vl["ll"], vl["amp1"], vl["amp2"])
+    a1, a2, ll = vl["amp1"], vl["amp2"], vl["ll"]
+    x0, y0, z0 = vl["x0"], vl["y0"], vl["z0"]
+    d = vl["dir"]
+    if d == "x":
+        ph1, ph2 = 2.0 * np.pi * (X - x0) / (ll + s1), 2.0 * np.pi * (X - x0) / (ll + s2)
+        return Y - y0 - a1 * np.sin(ph1), Z - z0 - a2 * np.cos(ph2)
+    if d == "y":
+        ph1, ph2 = 2.0 * np.pi * (Y - y0) / (ll + s1), 2.0 * np.pi * (Y - y0) / (ll + s2)
+        return Z - z0 - a1 * np.sin(ph1), X - x0 - a2 * np.cos(ph2)
+    if d == "z":
+        ph1, ph2 = 2.0 * np.pi * (Z - z0) / (ll + s1), 2.0 * np.pi * (Z - z0) / (ll + s2)
+        return X - x0 - a1 * np.sin(ph1), Y - y0 - a2 * np.cos(ph2)
+    raise ValueError(f"vortex line direction {d!r} is not x, y or z")
+
+
+def vortex_line(x, y, z, vl: dict, scal: float = 1.0):
+    """vortex_line(vl) (src/ic.f90:327-350): exp(i theta), times the core
+    amplitude 1 - exp(-0.7 r^1.15) unless vl['imprint_phase'].  vl holds the
+    line_param fields x0, y0, z0, amp1, amp2, ll, sgn, dir, imprint_phase."""
+    Z, Y, X = _grid3(x, y, z)
+    u, v = _line_axes(X, Y, Z, vl, scal)
+    theta = vl["sgn"] * np.arctan2(scal * v, scal * u)
+    if vl["imprint_phase"]:
+        return np.exp(1j * theta)
+    # get_r scales the squares, not the coordinates (src/ic.f90:762-788)
+    r = np.sqrt(scal * u ** 2 + scal * v ** 2)
+    return (1.0 - np.exp(-0.7 * r ** 1.15)) * np.exp(1j * theta)
+
+
+def vortex_ring(x, y, z, vr: dict, scal: float = 1.0):
+    """vortex_ring(vr) (src/ic.f90:352-511) in the plane vr['plane'] ('xy',
+    'xz' or 'yz'); vr holds the ring_param fields."""
+    Z, Y, X = _grid3(x, y, z)
+    plane = vr["plane"]
+    # (first in-plane, second in-plane, normal) coordinates and centres
+    axes = {"xy": ((X, vr["x0"]), (Y, vr["y0"]), (Z, vr["z0"])),
+            "xz": ((X, vr["x0"]), (Z, vr["z0"]), (Y, vr["y0"])),
+            "yz": ((Y, vr["y0"]), (Z, vr["z0"]), (X, vr["x0"]))}
+    if plane not in axes:
+        raise ValueError("Unrecognised vortex ring plane.")
+    (p1, c1), (p2, c2), (pn, cn) = axes[plane]
+    theta = np.arctan2(p2 - c2, p1 - c1)
+    s = np.sqrt((p1 - c1) ** 2 + (p2 - c2) ** 2) - vr["r1"] * np.sin(float(vr["kk"]) * theta)
+    dist = vr["amp"] * np.cos(float(vr["mm"]) * theta)
+    pp = pn - vr["r1"] * np.cos(float(vr["kk"]) * theta)
+    a = scal * (pp - cn)
+    b1 = scal * (s + vr["r0"] - dist)
+    b2 = scal * (s - vr["r0"] - dist)
+    d1 = np.sqrt(a ** 2 + b1 ** 2)
+    d2 = np.sqrt(a ** 2 + b2 ** 2)
+    return _rr(d1) * (a + vr["dir"] * 1j * b1) * _rr(d2) * (a - vr["dir"] * 1j * b2)
+
+
+def vtrap(x, y, z, omx, omy, omz):
+    """Vtrap (src/ic.f90:708-726)."""
+    Z, Y, X = _grid3(x, y, z)
+    return 0.5 * ((omx ** 2) * X ** 2 + (omy ** 2) * Y ** 2 + (omz ** 2) * Z ** 2)
+
+
+def fermi(x, y, z, mu, g, omx, omy, omz):
+    """fermi() (src/ic.f90:273-305): sqrt((mu - V)/g) where positive, else 0."""
+    f = (mu - vtrap(x, y, z, omx, omy, omz)) / g
+    return np.where(f >= 0.0, np.sqrt(np.maximum(f, 0.0)), 0.0).astype(np.complex128)
+
+
+def vortex_pair(x, y, z):
+    """vortex_pair() (src/ic.f90:586-632): the Pade vortex-pair profile in (x, y)."""
+    Z, Y, X = _grid3(x, y, z)
+    a0, a1, a2 = -1.14026, -0.150112, -0.0294564
+    b0, b1, b2 = -0.830953, -0.108296, -0.073641
+    c0, c1, c2, c3, c4 = 0.35022, 0.03032, 0.15905, 0.04123, 0.01402
+    x2, y2 = X ** 2, Y ** 2
+    den = 1.0 + c0 * x2 + c1 * X ** 4 + c2 * y2 + c3 * x2 * y2 + c4 * Y ** 4
+    return (1.0 + (a0 + a1 * x2 + a2 * y2) / den) + 1j * (X * (b0 + b1 * x2 + b2 * y2) / den)
+
+
+def sphere(x, y, z):
+    """sphere() (src/ic.f90:635-658): 0.5 (1 + tanh(r - 10 - 2))."""
+    Z, Y, X = _grid3(x, y, z)
+    return (0.5 * (1.0 + np.tanh(np.sqrt(X ** 2 + Y ** 2 + Z ** 2) - 10.0 - 2.0))).astype(
+        np.complex128)
+
+
+def sphere2(x, y, z):
+    """sphere2() (src/ic.f90:661-680): 100 exp(-r^2 / 10)."""
+    Z, Y, X = _grid3(x, y, z)
+    return (100.0 * np.exp(-(X ** 2 + Y ** 2 + Z ** 2) / 10.0)).astype(np.complex128)
+
+
+def wall(x, y, z):
+    """wall() (src/ic.f90:683-705): 0 for z <= -30, else 1."""
+    Z, Y, X = _grid3(x, y, z)
+    return np.where(Z <= -30.0, 0.0, 1.0).astype(np.complex128)

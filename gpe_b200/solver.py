@@ -436,7 +436,8 @@ def _cadence_outputs(s, run_dir, io: OutputParams, counters: dict) -> None:
 
 
 def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool = False,
-             record=None, run_dir: str | None = None, outputs: OutputParams | None = None):
+             record=None, run_dir: str | None = None, outputs: OutputParams | None = None,
+             end_time: float | None = None, imprint=None):
     """The per-step bookkeeping of the reference time loop (src/gpe.f90:134-278)
     with an explicit step count: solver, get_norm + relnorm (equation 4),
     imaginary-to-real switch at relnorm < 1e-12 (:251-268), renormalise.
@@ -451,6 +452,11 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
     (mass.dat, spectra, filtered surface) every save_rate3, idl_surface every
     save_rate2 and end_state every p_save time units, the counters starting
     from the current time (:126-128).
+    With end_time, the loop also stops once t + im_t > end_time, the
+    reference's loop condition (:134).  With imprint (a host field, the
+    vortex_line(vl1) of imprint_vl), every imaginary-time step of equation 4
+    ends with psi = |psi| * imprint (imprint_vortex_line,
+    src/variables.f90:1149-1163; src/gpe.f90:270).
     Returns the list of (t, im_t, norm, relnorm) after each step."""
     from . import output
     prm = s.prm
@@ -466,6 +472,8 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
                     "m": int(s.t / outputs.save_rate3)}
     norm = 0.0
     for _ in range(nsteps):
+        if end_time is not None and not (s.t + s.im_t <= end_time):
+            break
         if run_dir is not None and not os.path.exists(os.path.join(run_dir, "RUNNING")):
             _end_state(s, run_dir)
             break
@@ -504,6 +512,8 @@ def run_loop(s: GpeSolver, nsteps: int, *, renorm: bool = False, stop_imag: bool
                 s.dt = complex(abs(s.dt.imag), abs(s.dt.real))
             if renorm:
                 s.renormalise(norm)
+            if imprint is not None:
+                s.set_state(np.abs(s.get_state()) * imprint)
         prev_norm = norm
         s.p += 1
     return out

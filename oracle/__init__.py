@@ -250,10 +250,12 @@ def get_rr(r: float) -> float:
 
 
 def drive(orc: Oracle, psi, tm: OraTime, nsteps: int, *, renorm=False,
-          stop_imag=False):
+          stop_imag=False, imprint=None):
     """The per-step bookkeeping of the reference time loop (src/gpe.f90:134-278)
     with an explicit step count: solver, get_norm + relnorm (equation 4),
-    imaginary-to-real switch at relnorm < 1e-12, renormalise.  Returns
+    imaginary-to-real switch at relnorm < 1e-12, renormalise, and with
+    imprint (the vortex_line(vl1) field) psi = |psi| * imprint
+    (src/gpe.f90:270, src/variables.f90:1149-1163).  Returns
     (psi, list of (t, im_t, norm, relnorm))."""
     prm = orc.prm
     rec = []
@@ -280,6 +282,8 @@ def drive(orc: Oracle, psi, tm: OraTime, nsteps: int, *, renorm=False,
                 tm.dt_re, tm.dt_im = abs(tm.dt_im), abs(tm.dt_re)
             if renorm:
                 psi = orc.renormalise(psi, norm)
+            if imprint is not None:
+                psi = np.abs(psi) * imprint
         prev_norm = norm
         tm.p += 1
     return psi, rec

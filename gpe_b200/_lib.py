@@ -97,6 +97,13 @@ SIGNATURES = {
     "gpe_gpu_wait_probe": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "gpe_gpu_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "gpe_gpu_test_stall": (ctypes.c_int, [_vp, _i32]),
+    "gpe_group_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
+    "gpe_group_solver": (ctypes.c_int, [_vp, ctypes.POINTER(GpeTimeC),
+                                        ctypes.POINTER(GpeStepInfoC)]),
+    "gpe_group_norm": (ctypes.c_int, [_vp, _dp]),
+    "gpe_group_energy": (ctypes.c_int, [_vp, _dp, _dp]),
+    "gpe_group_destroy": (None, [_vp]),
+    "gpe_group_last_error": (ctypes.c_char_p, [_vp]),
     "gpe_gpu_linelength": (ctypes.c_int, [_vp, _dp]),
     "gpe_gpu_linelength_field": (ctypes.c_int, [_vp, _vp, _i32, _dp]),
     "gpe_gpu_zeros": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _dp, _i64]),
@@ -222,6 +229,12 @@ def check(rc: int, ctx=None) -> None:
 def check_cnn(rc: int, cnn=None) -> None:
     if rc != GPE_OK:
         msg = lib().gpe_cnn_last_error(cnn)
+        raise GpeError(rc, msg.decode() if msg else "")
+
+
+def check_group(rc: int, group=None) -> None:
+    if rc != GPE_OK:
+        msg = lib().gpe_group_last_error(group)
         raise GpeError(rc, msg.decode() if msg else "")
 
 

@@ -138,6 +138,19 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   }
 }
 
+// Slab group: combine d_scal[idx] of n members in member order (sum, or max
+// for op 1) and write the result back to every member.
+__global__ void combine_scalars_kernel(double* const* __restrict__ scal, int n, int idx,
+                                       int op) {
+  if (threadIdx.x != 0) return;
+  double a = scal[0][idx];
+  for (int m = 1; m < n; m++) {
+    const double v = scal[m][idx];
+    a = op ? fmax(a, v) : a + v;
+  }
+  for (int m = 0; m < n; m++) scal[m][idx] = a;
+}
+
 // Batched ensembles: one CTA per run sums slot 0 of the partials of every
 // work item of that run (fixed item order), times scale[r]; out[r] gets the
 // value and, when series is non-null, series[r * cap + *counter] too.

@@ -179,6 +179,20 @@ struct gpe_ctx {
   int (*post_step)(void*, gpe_ctx*) = nullptr;
   void* post_arg = nullptr;
   std::unique_ptr<gpe::Extension> ext[GPE_EXT_SLOTS];
+  // member of an in-process slab group (gpe_group_create): the group steps
+  // all members on its stream; the context's own stream is kept aside
+  gpe_group* group = nullptr;
+  cudaStream_t own_stream = nullptr;
+  bool ghosts_dirty = false;  // psi loaded alone; its z ghosts await the group
+  std::string err;
+};
+
+// z-slab contexts of one grid on one device, in z order, stepped together.
+struct gpe_group {
+  std::vector<gpe_ctx*> m;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  double** d_scal = nullptr;  // the members' d_scal pointers (device array)
   std::string err;
 };
 
@@ -359,7 +373,11 @@ struct StageSpec {
 using KernelFn = const void*;
 
 // Ring depth S and tile height TY from the shared-memory budget: as many
-// slots (up to 8) as fit two CTAs per SM, else one CTA per SM, else TY = 4.
+// slots (up to 8) as fit two CTAs per SM, as long as that leaves the R + 1
+// slots the compute warps hold plus one in flight, else one CTA per SM, else
+// TY = 4.  (Two CTAs with four slots beat one CTA with eight on the rk4
+// last stage at 512^3: 1.30 against 1.49 ms; the second CTA's warps hide
+// the first's latency better than a deeper ring.)
 LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1) {
   LaunchShape s{};
   int TY = tile_y > 0 ? tile_y : 8;
@@ -371,7 +389,7 @@ LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1) {
     s.pt_smem = (unsigned)round_up(s.pt_box, 128);
     const size_t stage = (size_t)ns * s.halo_smem + (size_t)np * s.pt_smem;
     int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
-    if (S < R + 3) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
+    if (S < R + 2) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
     if (S >= R + 2 || attempt == 1 || tile_y > 0) {
       s.S = std::max(S, R + 2);
       break;
@@ -681,6 +699,67 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   }
   c->launches++;
   c->last_nblk = (int)nblk;
+  return GPE_OK;
+}
+
+}  // namespace
+
+namespace {
+
+int launch_stage_one(gpe_ctx* c, const StageSpec& sp) {
+  if (sp.epi & EPI_ENERGY) {
+    if (c->es == 8) return launch_stage_t<float, double>(c, sp);
+    return launch_stage_t<double, double>(c, sp);
+  }
+  if (c->es == 8) return launch_stage_t<float, float>(c, sp);
+  return launch_stage_t<double, double>(c, sp);
+}
+
+// Copies of the two boundary planes of `field` into the z-neighbours' ghost
+// planes for every member of a slab group (the in-process form of
+// exchange_ghosts: the same planes, moved by cudaMemcpyAsync on the group's
+// stream after every member's kernel of the stage).
+int group_exchange(gpe_group* g, int field) {
+  const int n = (int)g->m.size();
+  for (int r = 0; r < n; r++) {
+    gpe_ctx* c = g->m[r];
+    const size_t plane = (size_t)c->Nx * c->Ny * (size_t)c->es;
+    unsigned char* f = static_cast<unsigned char*>(c->fld[field]);
+    if (c->exch_lo) {
+      const gpe_ctx* lo = g->m[c->nbr_lo];
+      const unsigned char* src = static_cast<const unsigned char*>(lo->fld[field]) +
+                                 (size_t)lo->nz * plane;  // its z = nz-2, nz-1
+      CU_CHECK(c, cudaMemcpyAsync(f, src, 2 * plane, cudaMemcpyDeviceToDevice, g->stream));
+    }
+    if (c->exch_hi) {
+      const gpe_ctx* hi = g->m[c->nbr_hi];
+      const unsigned char* src = static_cast<const unsigned char*>(hi->fld[field]) +
+                                 2 * plane;  // its z = 0, 1
+      CU_CHECK(c, cudaMemcpyAsync(f + (size_t)(c->nz + 2) * plane, src, 2 * plane,
+                                  cudaMemcpyDeviceToDevice, g->stream));
+    }
+  }
+  return GPE_OK;
+}
+
+// One stage: on a single context, or on every member of its slab group
+// followed by the group's ghost exchange; the z ghosts of a context with a
+// communicator go to its neighbours through NCCL.
+int launch_stage(gpe_ctx* c, const StageSpec& sp) {
+  if (c->group) {
+    for (gpe_ctx* m : c->group->m) {
+      const int rc = launch_stage_one(m, sp);
+      if (rc) return fail(c, rc, m->err);
+    }
+    for (int o = 0; o < sp.nout; o++)
+      if (sp.ghost_mask & (1 << o)) {
+        const int rc = group_exchange(c->group, sp.out[o]);
+        if (rc) return rc;
+      }
+    return GPE_OK;
+  }
+  int rc = launch_stage_one(c, sp);
+  if (rc) return rc;
   for (int o = 0; o < sp.nout; o++)
     if (sp.ghost_mask & (1 << o)) {
       rc = exchange_ghosts(c, sp.out[o]);
@@ -689,17 +768,21 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   return GPE_OK;
 }
 
-}  // namespace
-
-namespace {
-
-int launch_stage(gpe_ctx* c, const StageSpec& sp) {
-  if (sp.epi & EPI_ENERGY) {
-    if (c->es == 8) return launch_stage_t<float, double>(c, sp);
-    return launch_stage_t<double, double>(c, sp);
+// psi and its spare buffer (and the Kahan pair) trade roles on a context or
+// on every member of its group.
+void swap_psi(gpe_ctx* c) {
+  if (c->group) {
+    for (gpe_ctx* m : c->group->m) std::swap(m->psi_id, m->alt_id);
+  } else {
+    std::swap(c->psi_id, c->alt_id);
   }
-  if (c->es == 8) return launch_stage_t<float, float>(c, sp);
-  return launch_stage_t<double, double>(c, sp);
+}
+void swap_comp(gpe_ctx* c) {
+  if (c->group) {
+    for (gpe_ctx* m : c->group->m) std::swap(m->c_id, m->calt_id);
+  } else {
+    std::swap(c->c_id, c->calt_id);
+  }
 }
 
 Geom geom(const gpe_ctx* c) {
@@ -731,8 +814,8 @@ void end_timed(gpe_ctx* c, Launch& L) {
 }
 
 // partials -> d_scal[slot_out] (and optionally the per-step series).
-int finalize(gpe_ctx* c, int nblk, int slot, int op, double scale,
-             int out_index, bool series) {
+int finalize_one(gpe_ctx* c, int nblk, int slot, int op, double scale,
+                 int out_index, bool series) {
   Launch L{};
   begin_timed(c, L, GPE_FAM_REDUCE, 0);
   finalize_kernel<<<1, 1024, 0, c->stream>>>(
@@ -744,6 +827,23 @@ int finalize(gpe_ctx* c, int nblk, int slot, int op, double scale,
   return allreduce_scalars(c, out_index, 1, op);
 }
 
+// partials -> d_scal[out_index] (sum or max over blocks); in a slab group
+// each member reduces its own partials and the members' values are combined
+// in member order and written back to every member.
+int finalize(gpe_ctx* c, int nblk, int slot, int op, double scale,
+             int out_index, bool series) {
+  if (!c->group) return finalize_one(c, nblk, slot, op, scale, out_index, series);
+  gpe_group* g = c->group;
+  for (gpe_ctx* m : g->m) {
+    const int rc = finalize_one(m, m->last_nblk, slot, op, scale, out_index, false);
+    if (rc) return fail(c, rc, m->err);
+  }
+  combine_scalars_kernel<<<1, 32, 0, g->stream>>>(g->d_scal, (int)g->m.size(), out_index, op);
+  CU_CHECK(c, cudaGetLastError());
+  c->launches++;
+  return GPE_OK;
+}
+
 double cell_volume(const gpe_ctx* c) { return c->dx * c->dy * c->dz; }
 
 int read_scalars(gpe_ctx* c, double* dst, int first, int count) {
@@ -753,7 +853,7 @@ int read_scalars(gpe_ctx* c, double* dst, int first, int count) {
   return GPE_OK;
 }
 
-int check_status(gpe_ctx* c) {
+int check_status_one(gpe_ctx* c) {
   int st = 0;
   CU_CHECK(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int),
                               cudaMemcpyDeviceToHost, c->stream));
@@ -762,6 +862,15 @@ int check_status(gpe_ctx* c) {
     cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
     return fail(c, GPE_ERR_TIMEOUT,
                 "device-side wait limit expired in a stage kernel");
+  }
+  return GPE_OK;
+}
+
+int check_status(gpe_ctx* c) {
+  if (!c->group) return check_status_one(c);
+  for (gpe_ctx* m : c->group->m) {
+    const int rc = check_status_one(m);
+    if (rc) return fail(c, rc, m->err);
   }
   return GPE_OK;
 }
@@ -789,7 +898,7 @@ int step_euler(gpe_ctx* c, cd dt) {
   }
   int rc = launch_stage(c, s);
   if (rc) return rc;
-  std::swap(c->psi_id, c->alt_id);
+  swap_psi(c);
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
@@ -876,7 +985,7 @@ int step_rk4(gpe_ctx* c, cd dt) {
     const int rc = launch_stage(c, sp[st]);
     if (rc) return rc;
   }
-  std::swap(c->psi_id, c->alt_id);
+  swap_psi(c);
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
@@ -969,13 +1078,16 @@ int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
     {
       // errmax and the status word in one synchronisation: an attempt whose
       // kernels timed out has no valid error estimate
-      int st = 0;
+      std::vector<gpe_ctx*> members = c->group ? c->group->m : std::vector<gpe_ctx*>{c};
+      std::vector<int> st(members.size(), 0);
       CU_CHECK(c, cudaMemcpyAsync(&errmax, c->d_scal + 3, sizeof(double),
                                   cudaMemcpyDeviceToHost, c->stream));
-      CU_CHECK(c, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost,
-                                  c->stream));
+      for (size_t k = 0; k < members.size(); k++)
+        CU_CHECK(c, cudaMemcpyAsync(&st[k], members[k]->d_status, sizeof(int),
+                                    cudaMemcpyDeviceToHost, c->stream));
       CU_CHECK(c, cudaStreamSynchronize(c->stream));
-      if (st != 0) return check_status(c);
+      for (int v : st)
+        if (v != 0) return check_status(c);
     }
     if (!std::isfinite(errmax))
       return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate");
@@ -1004,8 +1116,8 @@ int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
   tm->im_t = tm->im_t + std::fabs(dt.imag());
   tm->dt_re = dt.real();
   tm->dt_im = dt.imag();
-  std::swap(c->psi_id, c->alt_id);
-  if (c->prm.kahan) std::swap(c->c_id, c->calt_id);
+  swap_psi(c);
+  if (c->prm.kahan) swap_comp(c);
   return GPE_OK;
 }
 
@@ -1183,6 +1295,9 @@ int load_stage(gpe_ctx* c, int elem_bytes) {
     CU_CHECK(c, cudaMemsetAsync(c->fld[c->c_id], 0, c->npad * (size_t)c->es,
                                 c->stream));
   c->norm_valid = false;
+  // a slab-group member's z ghosts come from its neighbours, which may not
+  // be loaded yet: the group refreshes them before its next step
+  if (c->group) c->ghosts_dirty = true;
   return exchange_ghosts(c, c->psi_id);
 }
 
@@ -1237,6 +1352,16 @@ int stage_out(gpe_ctx* c, int field, void* dst, int elem_bytes, bool device) {
 int check_ctx(gpe_ctx* c) {
   if (!c) return GPE_ERR_INVALID;
   CU_CHECK(c, cudaSetDevice(c->dev));
+  return GPE_OK;
+}
+
+// Entry points that step or reduce a whole grid refuse a slab-group member:
+// the group steps and reduces its members together.
+int check_solo(gpe_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (c->group)
+    return fail(c, GPE_ERR_INVALID, "context is a member of a slab group; use gpe_group_*");
   return GPE_OK;
 }
 
@@ -1645,6 +1770,15 @@ int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
 void gpe_gpu_destroy(gpe_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
+  if (c->group) {  // the group outlives no member: it stops stepping this one
+    gpe_group* g = c->group;
+    cudaStreamSynchronize(g->stream);
+    for (gpe_ctx* m : g->m) {
+      m->stream = m->own_stream;
+      m->group = nullptr;
+    }
+    g->m.clear();
+  }
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& e : c->ext) e.reset();
   if (c->comm && g_nccl.ok) g_nccl.CommDestroy(c->comm);
@@ -1775,7 +1909,7 @@ int gpe_gpu_get_plane(gpe_ctx* c, int32_t k, void* out, int32_t elem_bytes) {
 }
 
 int gpe_gpu_solver(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   if (!tm) return fail(c, GPE_ERR_INVALID, "tm is null");
   rc = do_step(c, tm, info);
@@ -1786,7 +1920,7 @@ int gpe_gpu_solver(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
 
 int gpe_gpu_solver_host(gpe_ctx* c, const void* var_in, void* var_out,
                         int32_t elem_bytes, gpe_time* tm, gpe_step_info* info) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   rc = check_elem(c, elem_bytes, var_in);
   if (rc) return rc;
@@ -1803,7 +1937,7 @@ int gpe_gpu_solver_host(gpe_ctx* c, const void* var_in, void* var_out,
 }
 
 int gpe_gpu_advance(gpe_ctx* c, int64_t nsteps, gpe_time* tm, double* norms) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   if (!tm || nsteps < 0) return fail(c, GPE_ERR_INVALID, "bad advance arguments");
   if ((size_t)nsteps > c->series_cap) {
@@ -1830,7 +1964,7 @@ int gpe_gpu_advance(gpe_ctx* c, int64_t nsteps, gpe_time* tm, double* norms) {
 }
 
 int gpe_gpu_norm(gpe_ctx* c, double* norm) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   if (!norm) return fail(c, GPE_ERR_INVALID, "norm is null");
   if (!c->norm_valid) {
@@ -1884,7 +2018,7 @@ int gpe_gpu_test_stall(gpe_ctx* c, int32_t plane) {
 }
 
 int gpe_gpu_diagnostics(gpe_ctx* c, double* mass, double* mom) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   if (!mass || !mom) return fail(c, GPE_ERR_INVALID, "null output");
   const Geom g = geom(c);
@@ -1921,7 +2055,7 @@ int gpe_gpu_diagnostics(gpe_ctx* c, double* mass, double* mom) {
 }
 
 int gpe_gpu_energy(gpe_ctx* c, double* E, double* H4) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   if (!E) return fail(c, GPE_ERR_INVALID, "E is null");
   StageSpec s;
@@ -1966,7 +2100,7 @@ int gpe_gpu_renormalise(gpe_ctx* c, double norm) {
 }
 
 static int rhs_like(gpe_ctx* c, void* out, int32_t elem_bytes, bool lap) {
-  int rc = check_ctx(c);
+  int rc = check_solo(c);
   if (rc) return rc;
   rc = check_elem(c, elem_bytes, out);
   if (rc) return rc;
@@ -2102,6 +2236,181 @@ void* gpe_gpu_host_alloc(size_t bytes) {
 
 void gpe_gpu_host_free(void* p) {
   if (p) cudaFreeHost(p);
+}
+
+// ----------------------------------------------------------------------------
+// In-process slab groups
+
+static int gfail(gpe_group* g, int code, const std::string& msg) {
+  if (g) g->err = msg;
+  else g_last_create_error = msg;
+  return code;
+}
+
+int gpe_group_create(gpe_ctx* const* members, int32_t n, gpe_group** out) {
+  if (!out || !members || n < 2) return gfail(nullptr, GPE_ERR_INVALID, "a slab group needs >= 2 members");
+  *out = nullptr;
+  const gpe_ctx* c0 = members[0];
+  if (!c0) return gfail(nullptr, GPE_ERR_INVALID, "null member");
+  int z = 0;
+  for (int r = 0; r < n; r++) {
+    const gpe_ctx* c = members[r];
+    if (!c) return gfail(nullptr, GPE_ERR_INVALID, "null member");
+    if (c->group || c->comm)
+      return gfail(nullptr, GPE_ERR_INVALID, "member already in a group or joined to a communicator");
+    const gpe_params &a = c->prm, &b = c0->prm;
+    if (c->dev != c0->dev || c->nx != c0->nx || c->ny != c0->ny || c->es != c0->es ||
+        a.scheme != b.scheme || a.order != b.order || a.bcs != b.bcs ||
+        a.eqn_to_solve != b.eqn_to_solve || a.kahan != b.kahan || a.real_time != b.real_time ||
+        a.xr != b.xr || a.yr != b.yr || a.zr != b.zr || c->nzg != c0->nzg)
+      return gfail(nullptr, GPE_ERR_INVALID,
+                   "members must share device, nx, ny, precision, scheme, order, boundary, "
+                   "equation, time direction, box and global z axis");
+    if (c->z_off != z) return gfail(nullptr, GPE_ERR_INVALID, "members must be consecutive z-slabs from z = 0");
+    if (c->nz < (c->prm.bcs == 2 ? 4 : 2))
+      return gfail(nullptr, GPE_ERR_INVALID, "slab too thin");
+    z += c->nz;
+  }
+  if (z != c0->nzg) return gfail(nullptr, GPE_ERR_INVALID, "slabs do not cover the global z axis");
+  gpe_group* g = new gpe_group();
+  g->dev = c0->dev;
+  if (cudaSetDevice(g->dev) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&g->d_scal, sizeof(double*) * n) != cudaSuccess) {
+    cudaGetLastError();
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return gfail(nullptr, GPE_ERR_CUDA, "group stream or scalar table allocation failed");
+  }
+  std::vector<double*> ptrs;
+  for (int r = 0; r < n; r++) {
+    gpe_ctx* c = members[r];
+    cudaStreamSynchronize(c->stream);
+    g->m.push_back(c);
+    ptrs.push_back(c->d_scal);
+    c->group = g;
+    c->own_stream = c->stream;
+    c->stream = g->stream;
+    c->rank = r;
+    c->nranks = n;
+    c->nbr_lo = (r - 1 + n) % n;
+    c->nbr_hi = (r + 1) % n;
+    const bool periodic = c->prm.bcs == 1;
+    c->exch_lo = periodic || r > 0;
+    c->exch_hi = periodic || r < n - 1;
+    c->ghosts_dirty = true;
+    c->norm_valid = false;
+    c->maps.clear();
+    c->shapes.clear();
+  }
+  cudaMemcpy(g->d_scal, ptrs.data(), sizeof(double*) * n, cudaMemcpyHostToDevice);
+  *out = g;
+  return GPE_OK;
+}
+
+void gpe_group_destroy(gpe_group* g) {
+  if (!g) return;
+  cudaSetDevice(g->dev);
+  cudaStreamSynchronize(g->stream);
+  for (gpe_ctx* c : g->m) {
+    c->stream = c->own_stream;
+    c->group = nullptr;
+    c->rank = 0;
+    c->nranks = 1;
+    c->exch_lo = c->exch_hi = false;
+    c->maps.clear();
+    c->shapes.clear();
+  }
+  if (g->d_scal) cudaFree(g->d_scal);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+const char* gpe_group_last_error(const gpe_group* g) {
+  return g ? g->err.c_str() : g_last_create_error.c_str();
+}
+
+static int group_ready(gpe_group* g) {
+  if (!g || g->m.empty()) return gfail(g, GPE_ERR_INVALID, "empty or destroyed group");
+  gpe_ctx* c = g->m[0];
+  if (cudaSetDevice(g->dev) != cudaSuccess) return gfail(g, GPE_ERR_CUDA, "cudaSetDevice failed");
+  bool dirty = false;
+  for (gpe_ctx* m : g->m) dirty = dirty || m->ghosts_dirty;
+  if (dirty) {
+    const int rc = group_exchange(g, c->psi_id);
+    if (rc) return gfail(g, rc, c->err);
+    for (gpe_ctx* m : g->m) m->ghosts_dirty = false;
+  }
+  return GPE_OK;
+}
+
+int gpe_group_solver(gpe_group* g, gpe_time* tm, gpe_step_info* info) {
+  int rc = group_ready(g);
+  if (rc) return rc;
+  if (!tm) return gfail(g, GPE_ERR_INVALID, "tm is null");
+  gpe_ctx* c = g->m[0];
+  rc = do_step(c, tm, info);
+  if (rc) return gfail(g, rc, c->err);
+  if (cudaStreamSynchronize(g->stream) != cudaSuccess)
+    return gfail(g, GPE_ERR_CUDA, "group stream synchronisation failed");
+  rc = check_status(c);
+  if (rc) return gfail(g, rc, c->err);
+  for (gpe_ctx* m : g->m) m->norm_valid = c->norm_valid;
+  return GPE_OK;
+}
+
+int gpe_group_norm(gpe_group* g, double* norm) {
+  int rc = group_ready(g);
+  if (rc) return rc;
+  if (!norm) return gfail(g, GPE_ERR_INVALID, "norm is null");
+  gpe_ctx* c = g->m[0];
+  if (!c->norm_valid) {
+    for (gpe_ctx* m : g->m) {
+      const Geom gm = geom(m);
+      const int nb = elementwise_blocks(m->nint);
+      if (m->es == 8)
+        norm_kernel<float><<<nb, 256, 0, g->stream>>>((const float*)m->fld[m->psi_id], gm,
+                                                      m->tabW[0], m->tabW[1], m->tabW[2],
+                                                      m->d_partials);
+      else
+        norm_kernel<double><<<nb, 256, 0, g->stream>>>((const double*)m->fld[m->psi_id], gm,
+                                                       m->tabW[0], m->tabW[1], m->tabW[2],
+                                                       m->d_partials);
+      m->launches++;
+      rc = finalize_one(m, nb, 0, 0, cell_volume(m), 0, false);
+      if (rc) return gfail(g, rc, m->err);
+    }
+    combine_scalars_kernel<<<1, 32, 0, g->stream>>>(g->d_scal, (int)g->m.size(), 0, 0);
+    if (cudaGetLastError() != cudaSuccess) return gfail(g, GPE_ERR_CUDA, "norm launch failed");
+  }
+  if (cudaMemcpyAsync(norm, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, g->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(g->stream) != cudaSuccess)
+    return gfail(g, GPE_ERR_CUDA, "norm read-back failed");
+  for (gpe_ctx* m : g->m) m->norm_valid = true;
+  if (!std::isfinite(*norm)) return gfail(g, GPE_ERR_NAN, "non-finite norm");
+  return GPE_OK;
+}
+
+int gpe_group_energy(gpe_group* g, double* E, double* H4) {
+  int rc = group_ready(g);
+  if (rc) return rc;
+  if (!E) return gfail(g, GPE_ERR_INVALID, "E is null");
+  gpe_ctx* c = g->m[0];
+  StageSpec s;
+  s.stencil = c->psi_id;
+  s.epi = EPI_ENERGY;
+  s.family = GPE_FAM_ENERGY;
+  rc = launch_stage(c, s);
+  if (!rc) rc = finalize(c, c->last_nblk, 0, 0, cell_volume(c), 1, false);
+  if (!rc) rc = finalize(c, c->last_nblk, 1, 0, cell_volume(c), 2, false);
+  double v[2] = {0.0, 0.0};
+  if (!rc) rc = read_scalars(c, v, 1, 2);
+  if (!rc) rc = check_status(c);
+  if (rc) return gfail(g, rc, c->err);
+  *E = v[0];
+  if (H4) *H4 = v[1];
+  return GPE_OK;
 }
 
 // ----------------------------------------------------------------------------

@@ -18,7 +18,7 @@ from dataclasses import dataclass, replace
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import GpeStepInfoC, check, check_group, lib
 from .solver import GpeParams, GpeSolver
 
 
@@ -114,3 +114,76 @@ class SlabSolver(GpeSolver):
         """Load this rank's planes of a global (nz_global, ny, nx) array."""
         a, b = self.plan.z_range
         self.set_state(np.ascontiguousarray(np.asarray(psi_global)[a:b + 1]))
+
+
+class SlabGroup:
+    """The z-slabs of one grid as separate contexts on one GPU, stepped
+    together by the library (gpe_group_*): the slab tables, z-ghost rules,
+    ghost-plane exchange and cross-slab reductions of the multi-rank path,
+    with the planes moved by device copies instead of NCCL.  Members follow
+    the reference's para_range split (SlabPlan)."""
+
+    def __init__(self, prm: GpeParams, nslabs: int, *, dt=None, tau=None):
+        self.global_prm = prm
+        self.plans = [SlabPlan(prm.nz, nslabs, r, prm.bcs) for r in range(nslabs)]
+        self.members = []
+        try:
+            for pl in self.plans:
+                pl.validate()
+                m = GpeSolver(slab_params(prm, pl, prm.device), dt=dt, tau=tau)
+                check(lib().gpe_gpu_set_slab(m.handle, prm.nz, pl.z_offset), m.handle)
+                self.members.append(m)
+            arr = (ctypes.c_void_p * nslabs)(*[m.handle.value for m in self.members])
+            self._g = ctypes.c_void_p()
+            check_group(lib().gpe_group_create(arr, nslabs, ctypes.byref(self._g)), None)
+        except Exception:
+            for m in self.members:
+                m.close()
+            raise
+        m0 = self.members[0]
+        self.t, self.im_t, self.p, self.dt = m0.t, m0.im_t, m0.p, m0.dt
+        self.last_info = None
+
+    def close(self) -> None:
+        if getattr(self, "_g", None):
+            lib().gpe_group_destroy(self._g)
+            self._g = ctypes.c_void_p()
+        for m in self.members:
+            m.close()
+        self.members = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_global_state(self, psi_global) -> None:
+        a = np.asarray(psi_global)
+        for pl, m in zip(self.plans, self.members):
+            lo, hi = pl.z_range
+            m.set_state(np.ascontiguousarray(a[lo:hi + 1]))
+
+    def get_global_state(self, dtype=np.complex128) -> np.ndarray:
+        return np.concatenate([m.get_state(dtype) for m in self.members], axis=0)
+
+    def solver(self):
+        from ._lib import GpeTimeC
+        tm = GpeTimeC(self.t, self.im_t, self.dt.real, self.dt.imag, self.p, 0)
+        info = GpeStepInfoC()
+        check_group(lib().gpe_group_solver(self._g, ctypes.byref(tm), ctypes.byref(info)),
+                    self._g)
+        self.t, self.im_t, self.p = tm.t, tm.im_t, tm.p
+        self.dt = complex(tm.dt_re, tm.dt_im)
+        self.last_info = info
+        return info
+
+    def get_norm(self) -> float:
+        v = ctypes.c_double()
+        check_group(lib().gpe_group_norm(self._g, ctypes.byref(v)), self._g)
+        return v.value
+
+    def energy(self):
+        e, h = ctypes.c_double(), ctypes.c_double()
+        check_group(lib().gpe_group_energy(self._g, ctypes.byref(e), ctypes.byref(h)), self._g)
+        return e.value, h.value

@@ -334,6 +334,30 @@ int gpe_gpu_comm_init(gpe_ctx* ctx, const void* id128, int32_t rank,
  * replayed.  Members share scheme (rk4), order, bcs, equation, precision,
  * kahan, device and time direction; grids, box sizes, g, mu and trap may
  * differ. */
+/* In-process slab group: z-slab contexts of one grid on one device (each
+ * created with its slab's nz and placed with gpe_gpu_set_slab, consecutive
+ * from z = 0, covering the global axis), stepped together as the reference
+ * steps its MPI ranks (src/variables.f90:98-358, src/solve.f90:189): every
+ * stage runs on every member, then each member's two boundary planes go to
+ * its neighbours' ghost planes (cudaMemcpyAsync on the group's stream, the
+ * same planes the NCCL path sends), and the norm, energy and rk45 error are
+ * combined across members (sum / max) so every member takes the same rk45
+ * decision.  Members keep their own fields and tables; while grouped they run
+ * on the group's stream and the per-context step / reduce entry points
+ * refuse them (GPE_ERR_INVALID).  State is loaded and read per member
+ * (gpe_gpu_set_state / get_state); the group refreshes the z ghosts before
+ * its next step.  Destroying the group returns the members to their own
+ * streams; destroying a member first empties the group. */
+typedef struct gpe_group gpe_group;
+int gpe_group_create(gpe_ctx* const* members, int32_t n, gpe_group** out);
+/* One solver() step of every member (t, im_t, dt, info as gpe_gpu_solver). */
+int gpe_group_solver(gpe_group* g, gpe_time* tm, gpe_step_info* info);
+/* get_norm / energy of the whole grid. */
+int gpe_group_norm(gpe_group* g, double* norm);
+int gpe_group_energy(gpe_group* g, double* E, double* H4);
+void gpe_group_destroy(gpe_group* g);
+const char* gpe_group_last_error(const gpe_group* g);
+
 typedef struct gpe_batch gpe_batch;
 typedef struct gpe_batch_opts {
   int32_t struct_size;  /* sizeof(gpe_batch_opts) */

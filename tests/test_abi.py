@@ -18,7 +18,7 @@ HEADER = os.path.join(ROOT, "include", "gpe_gpu.h")
 def declared_functions():
     src = open(HEADER).read() + open(os.path.join(ROOT, "include", "gpe_cnn.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = set(re.findall(r"\b(gpe_(?:gpu|batch|cnn)_\w+)\s*\(", src))
+    names = set(re.findall(r"\b(gpe_(?:gpu|batch|cnn|group)_\w+)\s*\(", src))
     return names
 
 
@@ -33,7 +33,7 @@ def test_every_declared_symbol_is_exported(L):
     assert len(names) >= 20
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
                          text=True, check=True).stdout
-    exported = set(re.findall(r"\bT (gpe_(?:gpu|batch|cnn)_\w+)", out))
+    exported = set(re.findall(r"\bT (gpe_(?:gpu|batch|cnn|group)_\w+)", out))
     assert names == exported, (names ^ exported)
     for n in names:
         assert hasattr(L, n)

@@ -97,6 +97,7 @@ SIGNATURES = {
     "gpe_gpu_wait_probe": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "gpe_gpu_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "gpe_gpu_test_stall": (ctypes.c_int, [_vp, _i32]),
+    "gpe_gpu_step_series": (ctypes.c_int, [_vp, _i64, _dp, ctypes.POINTER(_i32)]),
     "gpe_group_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, ctypes.POINTER(_vp)]),
     "gpe_group_solver": (ctypes.c_int, [_vp, ctypes.POINTER(GpeTimeC),
                                         ctypes.POINTER(GpeStepInfoC)]),

@@ -138,6 +138,101 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   }
 }
 
+// ---------------------------------------------------------------------------
+// rkqs step control on the device (src/solve.f90:158-244).  A step is: begin
+// (first attempt's dt), then attempts of the six Cash-Karp stages, each
+// followed by rk45_control_kernel, until one is accepted.  The stage kernels
+// read dt from `dt_r, dt_i, dt0_r, dt0_i` (contiguous, in this order).
+
+struct DevTime {
+  double dt_r, dt_i, dt0_r, dt0_i;  // this attempt's dt, the step's first dt
+  double t, im_t;
+  double errmax, did_r, did_i;       // last accepted attempt
+  double errcon;                     // (5 / safety)^(1 / dt_increase)
+  int attempts, underflow, halt, steps;  // halt: 0, or the GPE status code
+  int real_time, pad;
+};
+
+// Sets the while node's condition (when it is one) and starts a step.
+__global__ void rk45_begin_kernel(DevTime* T, cudaGraphConditionalHandle h, int use_cond) {
+  if (threadIdx.x != 0) return;
+  T->attempts = 0;
+  T->dt0_r = T->dt_r;
+  T->dt0_i = T->dt_i;
+  if (use_cond) cudaGraphSetConditional(h, T->halt ? 0u : 1u);
+}
+
+// After an attempt whose error maximum (over all sites, already reduced
+// across slabs) is scal[3] and whose trial-state norm is scal[0]: accept and
+// advance t, dt (recording the step in the series), or shrink dt and retry.
+// The arithmetic is the reference's: errmax <= 1 accepts; a rejected dt
+// shrinks to max(safety dt errmax^dt_decrease, dt / 10) along the time
+// direction; an accepted one grows to safety dt errmax^dt_increase, or 5 dt
+// when errmax <= errcon; t advances by the accepted dt and im_t by the new
+// |Im dt|.
+__global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
+                                    double* __restrict__ s_norm, double* __restrict__ s_dt,
+                                    int* __restrict__ s_att, int cap,
+                                    cudaGraphConditionalHandle h, int use_cond) {
+  if (threadIdx.x != 0) return;
+  const double safety = 0.9, dt_decrease = -0.25, dt_increase = -0.20;
+  if (T->halt) {
+    if (use_cond) cudaGraphSetConditional(h, 0u);
+    return;
+  }
+  const double errmax = scal[3];
+  T->attempts += 1;
+  T->errmax = errmax;
+  bool done = false;
+  if (!isfinite(errmax)) {
+    T->halt = 5;  // GPE_ERR_NAN
+    done = true;
+  } else if (errmax <= 1.0) {
+    const double dr = T->dt_r, di = T->dt_i;
+    double nr, ni;
+    if (errmax > T->errcon) {
+      const double f = pow(errmax, dt_increase);
+      nr = (safety * dr) * f;
+      ni = (safety * di) * f;
+    } else {
+      nr = 5.0 * dr;
+      ni = 5.0 * di;
+    }
+    T->t = T->t + dr;
+    T->did_r = dr;
+    T->did_i = di;
+    T->dt_r = nr;
+    T->dt_i = ni;
+    T->im_t = T->im_t + fabs(ni);
+    const int k = T->steps;
+    if (k < cap) {
+      if (s_norm) s_norm[k] = scal[0];
+      if (s_dt) s_dt[k] = dr;
+      if (s_att) s_att[k] = T->attempts;
+    }
+    T->steps = k + 1;
+    done = true;
+  } else {
+    const double dr = T->dt_r, di = T->dt_i;
+    const double f = pow(errmax, dt_decrease);
+    const double tr = (safety * dr) * f, ti = (safety * di) * f;
+    const double mag = fmax(hypot(tr, ti), 0.1 * hypot(dr, di));
+    if (T->real_time) {
+      T->dt_r = mag;
+      T->dt_i = 0.0;
+      if (T->t + mag == T->t) T->underflow = 1;
+    } else {
+      T->dt_r = 0.0;
+      T->dt_i = -mag;
+    }
+    if (T->attempts > 10000) {
+      T->halt = 8;  // GPE_ERR_UNDERFLOW
+      done = true;
+    }
+  }
+  if (use_cond) cudaGraphSetConditional(h, done ? 0u : 1u);
+}
+
 // Slab group: combine d_scal[idx] of n members in member order (sum, or max
 // for op 1) and write the result back to every member.
 __global__ void combine_scalars_kernel(double* const* __restrict__ scal, int n, int idx,

@@ -46,8 +46,9 @@ constexpr double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0,
 constexpr double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0,
                  DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0,
                  DC6 = C6 - 0.25;
-// Adaptive step constants (src/parameters.f90:89-92).
-constexpr double RK_EPS = 1e-6, SAFETY = 0.9, DT_DECREASE = -0.25,
+// Adaptive step constants (src/parameters.f90:89-92); dt_decrease (-0.25)
+// is applied in rk45_control_kernel.
+constexpr double RK_EPS = 1e-6, SAFETY = 0.9,
                  DT_INCREASE = -0.20;
 // Extended-Simpson end weights (src/variables.f90:49-51).
 constexpr double W1 = 3.0 / 8.0, W2 = 7.0 / 6.0, W3 = 23.0 / 24.0;
@@ -158,6 +159,7 @@ struct gpe_ctx {
   double* d_scal = nullptr;  // [0] norm [1] E [2] H4 [3] errmax
   double* d_series = nullptr;
   size_t series_cap = 0;
+  int64_t series_steps = 0;  // steps the last rk45 advance recorded
   int* d_counter = nullptr;
   int* d_status = nullptr;
   void* d_stage = nullptr;  // dense staging, nint * 16 bytes
@@ -183,6 +185,14 @@ struct gpe_ctx {
   // all members on its stream; the context's own stream is kept aside
   gpe_group* group = nullptr;
   cudaStream_t own_stream = nullptr;
+  // rk45 step control on the device: time state, per-step series of the
+  // last advance (dt taken, attempts) and one captured step per psi buffer
+  gpe::DevTime* d_time = nullptr;
+  double* d_ser_dt = nullptr;
+  int* d_ser_att = nullptr;
+  cudaGraph_t rk_graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t rk_exec[2] = {nullptr, nullptr};
+  int rk_psi[2] = {-1, -1};  // psi buffer each captured step starts from
   bool ghosts_dirty = false;  // psi loaded alone; its z ghosts await the group
   std::string err;
 };
@@ -367,6 +377,11 @@ struct StageSpec {
   cd cek = cd(0);
   cd dt0 = cd(0);
   double inv_absdt = 0.0;
+  // rk45 with device step control: a[o] = a_mul[o] dt, cek = cek_mul dt,
+  // dt and dt0 read from device memory by the kernel
+  const double* dyn = nullptr;
+  double a_mul[2] = {0.0, 0.0};
+  double cek_mul = 0.0;
   int family = GPE_FAM_OTHER;
 };
 
@@ -640,6 +655,11 @@ void fill_common(const StageSpec& sp, bool fold, const LaunchShape& sh,
   p->cek_r = cek.real(); p->cek_i = cek.imag();
   p->dt0_r = sp.dt0.real(); p->dt0_i = sp.dt0.imag();
   p->inv_absdt = sp.inv_absdt;
+  p->dyn = sp.dyn;
+  p->a_mul[0] = sp.a_mul[0];
+  p->a_mul[1] = sp.a_mul[1];
+  p->cek_mul = sp.cek_mul;
+  p->fold = fold ? 1 : 0;
   p->wait_limit_ns = WAIT_LIMIT_NS;
   p->stall_plane = -1;
 }
@@ -991,7 +1011,7 @@ int step_rk4(gpe_ctx* c, cd dt) {
 
 // rkck (src/solve.f90:248-378) with the psi_scal / errmax reduction of rkqs
 // (:176-190) fused into the last stage.  Writes the trial state to alt.
-int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
+int attempt_rkck(gpe_ctx* c, cd dt, cd dt0, const double* dyn = nullptr) {
   const bool K = c->prm.kahan != 0;
   const int psi = c->psi_id;
   const int stencils[6] = {psi, F_UA, F_UB, F_UA, F_UB, F_UA};
@@ -1024,6 +1044,9 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
       }
     }
     s.a[1] = B[st][st] * dt;
+    s.dyn = dyn;
+    s.a_mul[0] = 1.0;
+    s.a_mul[1] = B[st][st];
     s.family = st == 0 ? GPE_FAM_STAGE_FIRST : GPE_FAM_STAGE_MID;
     rc = launch_stage(c, s);
     if (rc) return rc;
@@ -1039,6 +1062,9 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
   s.inv_absdt = 1.0 / std::abs(dt);
   s.a[0] = C6 * dt;
   s.cek = DC6 * dt;
+  s.dyn = dyn;
+  s.a_mul[0] = C6;
+  s.cek_mul = DC6;
   // pointwise slots: psi, k1, k3, k4, k5 [, c]  (the kernel takes psi from
   // slot 0, k1 from slot 1 and the compensation from the last slot)
   s.pt[0] = psi;
@@ -1063,61 +1089,226 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0) {
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
 }
 
-// rkqs (src/solve.f90:158-244) with device stages and host step control.
-int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
-  const double errcon = std::pow(5.0 / SAFETY, 1.0 / DT_INCREASE);
-  cd dt(tm->dt_re, tm->dt_im);
-  const cd dt0 = dt;
-  const bool real_time = c->prm.real_time != 0;
-  double errmax = 0.0;
-  int attempts = 0, underflow = 0;
-  for (;;) {
-    attempts++;
-    int rc = attempt_rkck(c, dt, dt0);
-    if (rc) return rc;
-    {
-      // errmax and the status word in one synchronisation: an attempt whose
-      // kernels timed out has no valid error estimate
-      std::vector<gpe_ctx*> members = c->group ? c->group->m : std::vector<gpe_ctx*>{c};
-      std::vector<int> st(members.size(), 0);
-      CU_CHECK(c, cudaMemcpyAsync(&errmax, c->d_scal + 3, sizeof(double),
-                                  cudaMemcpyDeviceToHost, c->stream));
-      for (size_t k = 0; k < members.size(); k++)
-        CU_CHECK(c, cudaMemcpyAsync(&st[k], members[k]->d_status, sizeof(int),
-                                    cudaMemcpyDeviceToHost, c->stream));
-      CU_CHECK(c, cudaStreamSynchronize(c->stream));
-      for (int v : st)
-        if (v != 0) return check_status(c);
+// ---------------------------------------------------------------------------
+// rkqs (src/solve.f90:158-244) with the step control on the device
+// (rk45_control_kernel): an attempt is the six Cash-Karp stages reading dt
+// from the context's DevTime, the error-maximum and norm reductions, then the
+// control kernel, which accepts (advancing t and dt) or shrinks dt.  A step
+// repeats attempts until one is accepted.  Where the stream can be captured
+// (one context or a slab group; not with NCCL or per-launch timing) a step is
+// one CUDA graph, a conditional WHILE node around the attempt, so a run of
+// steps needs no host synchronisation; otherwise the host repeats the
+// attempt, reading back two integers after each.  Both run the same kernels,
+// so their step sequences are identical.
+
+double rk45_errcon() { return std::pow(5.0 / SAFETY, 1.0 / DT_INCREASE); }
+
+// The leader's DevTime (the group's first member steps the group).
+DevTime* rk45_time(gpe_ctx* c) { return c->group ? c->group->m[0]->d_time : c->d_time; }
+
+void rk45_drop_graphs(gpe_ctx* c) {
+  for (int k = 0; k < 2; k++) {
+    if (c->rk_exec[k]) cudaGraphExecDestroy(c->rk_exec[k]);
+    if (c->rk_graph[k]) cudaGraphDestroy(c->rk_graph[k]);
+    c->rk_exec[k] = nullptr;
+    c->rk_graph[k] = nullptr;
+    c->rk_psi[k] = -1;
+  }
+}
+
+bool rk45_capturable(const gpe_ctx* c) { return !c->comm && !c->timing; }
+
+// Enqueues one attempt and its control kernel (use_cond: inside the WHILE
+// node whose handle is h).
+int rk45_attempt(gpe_ctx* c, cudaGraphConditionalHandle h, int use_cond) {
+  DevTime* T = rk45_time(c);
+  const double* dyn = reinterpret_cast<const double*>(T);  // dt_r, dt_i, dt0_r, dt0_i
+  int rc = attempt_rkck(c, cd(1.0, 0.0), cd(1.0, 0.0), dyn);
+  if (rc) return rc;
+  rk45_control_kernel<<<1, 32, 0, c->stream>>>(T, c->d_scal, c->d_series, c->d_ser_dt,
+                                                c->d_ser_att, (int)c->series_cap, h, use_cond);
+  CU_CHECK(c, cudaGetLastError());
+  c->launches++;
+  return GPE_OK;
+}
+
+// Captures the step that starts from the current psi buffer into slot k.
+int rk45_build_graph(gpe_ctx* c, int k) {
+  cudaGraph_t g = nullptr;
+  CU_CHECK(c, cudaGraphCreate(&g, 0));
+  auto bail = [&](int rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  };
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+    return bail(fail(c, GPE_ERR_CUDA, "cudaGraphConditionalHandleCreate failed"));
+  const bool timing = c->timing;
+  c->timing = false;
+  // the begin kernel, then the WHILE node around one attempt
+  cudaError_t e = cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rk45_begin_kernel<<<1, 32, 0, c->stream>>>(rk45_time(c), h, 1);
+    cudaGraph_t tmp = nullptr;
+    e = cudaStreamEndCapture(c->stream, &tmp);
+  }
+  if (e != cudaSuccess) {
+    c->timing = timing;
+    return bail(fail(c, GPE_ERR_CUDA, std::string("rk45 graph capture: ") + cudaGetErrorString(e)));
+  }
+  cudaGraphNode_t begin = nullptr;
+  size_t nn = 1;
+  cudaGraphGetNodes(g, &begin, &nn);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cond = nullptr;
+  e = cudaGraphAddNode(&cond, g, &begin, 1, &cp);
+  if (e != cudaSuccess) {
+    c->timing = timing;
+    return bail(fail(c, GPE_ERR_CUDA, std::string("rk45 WHILE node: ") + cudaGetErrorString(e)));
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  int rc = GPE_OK;
+  if (e == cudaSuccess) {
+    rc = rk45_attempt(c, h, 1);
+    cudaGraph_t tmp = nullptr;
+    e = cudaStreamEndCapture(c->stream, &tmp);
+  }
+  c->timing = timing;
+  if (rc) return bail(rc);
+  if (e != cudaSuccess)
+    return bail(fail(c, GPE_ERR_CUDA, std::string("rk45 attempt capture: ") + cudaGetErrorString(e)));
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  if (e != cudaSuccess)
+    return bail(fail(c, GPE_ERR_CUDA, std::string("rk45 graph instantiate: ") + cudaGetErrorString(e)));
+  c->rk_graph[k] = g;
+  c->rk_exec[k] = x;
+  c->rk_psi[k] = c->psi_id;
+  return GPE_OK;
+}
+
+// Reads the DevTime back (one synchronisation).
+int rk45_read(gpe_ctx* c, DevTime* h) {
+  CU_CHECK(c, cudaMemcpyAsync(h, rk45_time(c), sizeof(DevTime), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  return GPE_OK;
+}
+
+// Up to n steps from the time state in the DevTime; returns the steps taken
+// in *done (fewer than n only if the control halted).  psi (and the Kahan
+// pair) end in the buffers of the last accepted step.
+int rk45_steps(gpe_ctx* c, int64_t n, int64_t* done) {
+  *done = 0;
+  if (n <= 0) return GPE_OK;
+  DevTime h{};
+  if (rk45_capturable(c)) {
+    for (int k = 0; k < 2; k++) {
+      // slot k starts from the psi buffer (k == 0: the current one)
+      const int want = (k == 0) ? c->psi_id : c->alt_id;
+      if (c->rk_psi[k] != want || !c->rk_exec[k]) {
+        if (c->rk_exec[k]) cudaGraphExecDestroy(c->rk_exec[k]);
+        if (c->rk_graph[k]) cudaGraphDestroy(c->rk_graph[k]);
+        c->rk_exec[k] = nullptr;
+        c->rk_graph[k] = nullptr;
+        if (k == 1) {
+          swap_psi(c);
+          if (c->prm.kahan) swap_comp(c);
+        }
+        const int rc = rk45_build_graph(c, k);
+        if (k == 1) {
+          swap_psi(c);
+          if (c->prm.kahan) swap_comp(c);
+        }
+        if (rc) return rc;
+      }
     }
-    if (!std::isfinite(errmax))
-      return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate");
-    if (errmax <= 1.0) break;
-    const cd dt_temp = SAFETY * dt * std::pow(errmax, DT_DECREASE);
-    const double mag = std::max(std::abs(dt_temp), 0.1 * std::abs(dt));
-    dt = real_time ? cd(mag, 0.0) : cd(0.0, -mag);
-    if (real_time && tm->t + dt.real() == tm->t) underflow = 1;
-    if (attempts > 10000)
-      return fail(c, GPE_ERR_UNDERFLOW, "rk45: step size control did not converge");
+    for (int64_t s = 0; s < n; s++)
+      CU_CHECK(c, cudaGraphLaunch(c->rk_exec[s & 1], c->stream));
+    int rc = rk45_read(c, &h);
+    if (rc) return rc;
+    *done = h.steps;
+    // graph replays: per step a begin kernel and per attempt 6 stages, 2
+    // reductions and the control kernel
+  } else {
+    for (int64_t s = 0; s < n; s++) {
+      rk45_begin_kernel<<<1, 32, 0, c->stream>>>(rk45_time(c), 0, 0);
+      CU_CHECK(c, cudaGetLastError());
+      c->launches++;
+      for (;;) {
+        int rc = rk45_attempt(c, 0, 0);
+        if (rc) return rc;
+        rc = rk45_read(c, &h);
+        if (rc) return rc;
+        if (h.halt || h.steps > s) break;
+      }
+      if (h.halt) break;
+      swap_psi(c);
+      if (c->prm.kahan) swap_comp(c);
+    }
+    *done = h.steps;
+    return GPE_OK;
   }
-  cd dt_next;
-  if (errmax > errcon)
-    dt_next = SAFETY * dt * std::pow(errmax, DT_INCREASE);
-  else
-    dt_next = 5.0 * dt;
-  tm->t = tm->t + dt.real();
+  if (*done & 1) {
+    swap_psi(c);
+    if (c->prm.kahan) swap_comp(c);
+  }
+  return GPE_OK;
+}
+
+// Loads the host time state into the DevTime (steps counted from 0).
+int rk45_load(gpe_ctx* c, const gpe_time* tm) {
+  DevTime h{};
+  h.dt_r = tm->dt_re;
+  h.dt_i = tm->dt_im;
+  h.dt0_r = tm->dt_re;
+  h.dt0_i = tm->dt_im;
+  h.t = tm->t;
+  h.im_t = tm->im_t;
+  h.errcon = rk45_errcon();
+  h.real_time = c->prm.real_time ? 1 : 0;
+  CU_CHECK(c, cudaMemcpyAsync(rk45_time(c), &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  return GPE_OK;
+}
+
+int rk45_halted(gpe_ctx* c, const DevTime& h) {
+  if (h.halt == GPE_ERR_NAN) return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate");
+  if (h.halt) return fail(c, GPE_ERR_UNDERFLOW, "rk45: step size control did not converge");
+  return GPE_OK;
+}
+
+int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
+  int rc = rk45_load(c, tm);
+  if (rc) return rc;
+  int64_t done = 0;
+  rc = rk45_steps(c, 1, &done);
+  if (rc) return rc;
+  DevTime h{};
+  rc = rk45_read(c, &h);
+  if (rc) return rc;
+  // a timed-out stage leaves no valid error estimate
+  rc = check_status(c);
+  if (rc) return rc;
+  if (done != 1) return rk45_halted(c, h);
+  c->launches += rk45_capturable(c) ? 1 + 9 * (int64_t)h.attempts : 0;
+  tm->t = h.t;
+  tm->im_t = h.im_t;
+  tm->dt_re = h.dt_r;
+  tm->dt_im = h.dt_i;
   if (info) {
-    info->errmax = errmax;
-    info->attempts = attempts;
-    info->underflow = underflow;
-    info->dt_did_re = dt.real();
-    info->dt_did_im = dt.imag();
+    info->errmax = h.errmax;
+    info->attempts = h.attempts;
+    info->underflow = h.underflow;
+    info->dt_did_re = h.did_r;
+    info->dt_did_im = h.did_i;
   }
-  dt = dt_next;
-  tm->im_t = tm->im_t + std::fabs(dt.imag());
-  tm->dt_re = dt.real();
-  tm->dt_im = dt.imag();
-  swap_psi(c);
-  if (c->prm.kahan) swap_comp(c);
   return GPE_OK;
 }
 
@@ -1412,7 +1603,8 @@ struct gpe_batch {
   double* d_scale = nullptr;
   double* d_norm = nullptr;
   double* d_series = nullptr;
-  size_t series_cap = 0;  // steps per run
+  size_t series_cap = 0;
+  int64_t series_steps = 0;  // steps the last rk45 advance recorded  // steps per run
   int* d_counter = nullptr;
   int* d_status = nullptr;
   // Two prepared step forms: RK4 leaves psi in the members' other buffer
@@ -1756,6 +1948,15 @@ int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
   }
   c->device_bytes += (int64_t)(2 * sizeof(double) * c->partials_cap +
                                16 * sizeof(double) + 2 * sizeof(int) + c->nint * 16);
+  if (p.scheme == GPE_SCHEME_RK45) {
+    if (cudaMalloc(&c->d_time, sizeof(DevTime)) != cudaSuccess) {
+      cudaGetLastError();
+      c->err = "cudaMalloc of the rk45 time state failed";
+      return bail(GPE_ERR_OOM);
+    }
+    cudaMemset(c->d_time, 0, sizeof(DevTime));
+    c->device_bytes += (int64_t)sizeof(DevTime);
+  }
   cudaMemset(c->d_scal, 0, 16 * sizeof(double));
   cudaMemset(c->d_status, 0, sizeof(int));
   cudaMemset(c->d_counter, 0, sizeof(int));
@@ -1776,6 +1977,7 @@ void gpe_gpu_destroy(gpe_ctx* c) {
     for (gpe_ctx* m : g->m) {
       m->stream = m->own_stream;
       m->group = nullptr;
+      rk45_drop_graphs(m);
     }
     g->m.clear();
   }
@@ -1791,6 +1993,10 @@ void gpe_gpu_destroy(gpe_ctx* c) {
   if (c->d_counter) cudaFree(c->d_counter);
   if (c->d_status) cudaFree(c->d_status);
   if (c->d_stage) cudaFree(c->d_stage);
+  rk45_drop_graphs(c);
+  if (c->d_time) cudaFree(c->d_time);
+  if (c->d_ser_dt) cudaFree(c->d_ser_dt);
+  if (c->d_ser_att) cudaFree(c->d_ser_att);
   for (auto& L : c->timed) {
     cudaEventDestroy(L.a);
     cudaEventDestroy(L.b);
@@ -1941,11 +2147,55 @@ int gpe_gpu_advance(gpe_ctx* c, int64_t nsteps, gpe_time* tm, double* norms) {
   if (rc) return rc;
   if (!tm || nsteps < 0) return fail(c, GPE_ERR_INVALID, "bad advance arguments");
   if ((size_t)nsteps > c->series_cap) {
+    // the captured rk45 steps hold the old series pointers
+    CU_CHECK(c, cudaStreamSynchronize(c->stream));
+    rk45_drop_graphs(c);
     if (c->d_series) cudaFree(c->d_series);
+    if (c->d_ser_dt) cudaFree(c->d_ser_dt);
+    if (c->d_ser_att) cudaFree(c->d_ser_att);
     c->d_series = nullptr;
+    c->d_ser_dt = nullptr;
+    c->d_ser_att = nullptr;
+    c->series_cap = 0;
     const size_t cap = std::max<size_t>((size_t)nsteps, 1024);
     CU_CHECK(c, cudaMalloc(&c->d_series, cap * sizeof(double)));
+    CU_CHECK(c, cudaMalloc(&c->d_ser_dt, cap * sizeof(double)));
+    CU_CHECK(c, cudaMalloc(&c->d_ser_att, cap * sizeof(int)));
     c->series_cap = cap;
+  }
+  if (c->prm.scheme == GPE_SCHEME_RK45 && !c->post_step) {
+    // nsteps accepted steps with the step control on the device
+    c->norm_valid = false;
+    rc = rk45_load(c, tm);
+    if (rc) return rc;
+    int64_t done = 0;
+    rc = rk45_steps(c, nsteps, &done);
+    if (rc) return rc;
+    DevTime h{};
+    rc = rk45_read(c, &h);
+    if (rc) return rc;
+    rc = check_status(c);
+    if (rc) return rc;
+    tm->t = h.t;
+    tm->im_t = h.im_t;
+    tm->dt_re = h.dt_r;
+    tm->dt_im = h.dt_i;
+    tm->p += (int32_t)done;
+    if (done > 0) {
+      if (norms)
+        CU_CHECK(c, cudaMemcpy(norms, c->d_series, sizeof(double) * done, cudaMemcpyDeviceToHost));
+      if (rk45_capturable(c)) {
+        std::vector<int> att((size_t)done);
+        CU_CHECK(c, cudaMemcpy(att.data(), c->d_ser_att, sizeof(int) * done,
+                               cudaMemcpyDeviceToHost));
+        for (int a : att) c->launches += 9 * (int64_t)a;
+        c->launches += done;
+      }
+    }
+    c->series_steps = done;
+    if (done < nsteps) return rk45_halted(c, h);
+    c->norm_valid = true;
+    return GPE_OK;
   }
   CU_CHECK(c, cudaMemsetAsync(c->d_counter, 0, sizeof(int), c->stream));
   for (int64_t s = 0; s < nsteps; s++) {
@@ -2008,12 +2258,29 @@ int gpe_gpu_wait_probe(gpe_ctx* c, uint64_t limit_ns) {
 int gpe_gpu_set_wait_limit(gpe_ctx* c, uint64_t limit_ns) {
   if (!c) return GPE_ERR_INVALID;
   c->wait_limit_ns = limit_ns ? (unsigned long long)limit_ns : WAIT_LIMIT_NS;
+  cudaStreamSynchronize(c->stream);
+  rk45_drop_graphs(c);
   return GPE_OK;
 }
 
 int gpe_gpu_test_stall(gpe_ctx* c, int32_t plane) {
   if (!c) return GPE_ERR_INVALID;
   c->stall_plane = plane >= 0 ? plane : -1;
+  cudaStreamSynchronize(c->stream);
+  rk45_drop_graphs(c);
+  return GPE_OK;
+}
+
+int gpe_gpu_step_series(gpe_ctx* c, int64_t n, double* dt_did, int32_t* attempts) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (n < 0 || n > c->series_steps)
+    return fail(c, GPE_ERR_INVALID, "the last rk45 advance recorded fewer steps");
+  if (n == 0) return GPE_OK;
+  if (dt_did)
+    CU_CHECK(c, cudaMemcpy(dt_did, c->d_ser_dt, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (attempts)
+    CU_CHECK(c, cudaMemcpy(attempts, c->d_ser_att, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
   return GPE_OK;
 }
 
@@ -2170,6 +2437,7 @@ int gpe_gpu_set_slab(gpe_ctx* c, int32_t nz_global, int32_t z_offset) {
   if (c->prm.bcs == 2 && c->nz < 4 && nz_global > c->nz)
     return fail(c, GPE_ERR_INVALID, "reflective slabs need at least 4 planes");
   CU_CHECK(c, cudaStreamSynchronize(c->stream));
+  rk45_drop_graphs(c);
   c->nzg = nz_global;
   c->z_off = z_offset;
   // get_grid on the global axis, keeping this slab's planes
@@ -2302,6 +2570,7 @@ int gpe_group_create(gpe_ctx* const* members, int32_t n, gpe_group** out) {
     c->norm_valid = false;
     c->maps.clear();
     c->shapes.clear();
+    rk45_drop_graphs(c);
   }
   cudaMemcpy(g->d_scal, ptrs.data(), sizeof(double*) * n, cudaMemcpyHostToDevice);
   *out = g;
@@ -2320,6 +2589,7 @@ void gpe_group_destroy(gpe_group* g) {
     c->exch_lo = c->exch_hi = false;
     c->maps.clear();
     c->shapes.clear();
+    rk45_drop_graphs(c);
   }
   if (g->d_scal) cudaFree(g->d_scal);
   if (g->stream) cudaStreamDestroy(g->stream);

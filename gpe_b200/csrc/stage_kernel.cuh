@@ -124,6 +124,13 @@ struct StageParams {
   unsigned long long wait_limit_ns;
   int stall_plane;        // >= 0: failure-detection test, the producer stops
                           // issuing when it reaches this plane of an item
+  // rk45 with device step control: dt lives in device memory ([0..1] dt of
+  // this attempt, [2..3] dt of the step's first attempt) and a[o] =
+  // a_mul[o] dt, cek = cek_mul dt (times i when fold), replacing a_r, a_i,
+  // cek_r, cek_i, dt0_r, dt0_i and inv_absdt above
+  const double* dyn;
+  double a_mul[2], cek_mul;
+  int fold;
 };
 
 __device__ __forceinline__ bool near_edge(int i, int n) {
@@ -252,10 +259,39 @@ __global__ void __launch_bounds__(288)
   const unsigned row_off = ES * (unsigned)((ty + R) * HW + 2 * lane + 2);
   const unsigned pt_off = ES * (unsigned)(ty * TX + 2 * lane);
   V ar[2], aix[2], alv[2], alv2[2], bev[2][NP > 0 ? NP : 1];
+  TC a_re[2] = {p.a_r[0], p.a_r[1]}, a_im[2] = {p.a_i[0], p.a_i[1]};
+  double cek_r = p.cek_r, cek_i = p.cek_i, dt0_r = p.dt0_r, dt0_i = p.dt0_i,
+         inv_absdt = p.inv_absdt;
+  if (p.dyn) {
+    // the same arithmetic as the host's coefficient set-up: m * dt, and for
+    // fold the complex product (0, 1) * (m dt)
+    const double dr = p.dyn[0], di = p.dyn[1];
+    auto coef = [&](double mul, double& cr, double& ci) {
+      const double xr = __dmul_rn(mul, dr), xi = __dmul_rn(mul, di);
+      if (p.fold) {
+        cr = __dsub_rn(__dmul_rn(0.0, xr), xi);
+        ci = __dadd_rn(__dmul_rn(0.0, xi), xr);
+      } else {
+        cr = xr;
+        ci = xi;
+      }
+    };
+#pragma unroll
+    for (int o = 0; o < 2; o++) {
+      double cr, ci;
+      coef(p.a_mul[o], cr, ci);
+      a_re[o] = (TC)cr;
+      a_im[o] = (TC)ci;
+    }
+    coef(p.cek_mul, cek_r, cek_i);
+    dt0_r = p.dyn[2];
+    dt0_i = p.dyn[3];
+    inv_absdt = __drcp_rn(hypot(dr, di));
+  }
 #pragma unroll
   for (int o = 0; o < 2; o++) {
-    ar[o] = vsplat(p.a_r[o]);
-    aix[o] = vpair(-p.a_i[o], p.a_i[o]);
+    ar[o] = vsplat(a_re[o]);
+    aix[o] = vpair(-a_im[o], a_im[o]);
     alv[o] = vsplat(p.alpha[o]);
     alv2[o] = vsplat(p.alpha2[o]);
 #pragma unroll
@@ -493,8 +529,8 @@ __global__ void __launch_bounds__(288)
         if (ok && (EPI & EPI_ERR)) {
           // err = sum_q ce[q] P_q + cek (x) K; psi = P[0], k1 = P[1]
           const double kr = (double)Kv.x, ki = (double)Kv.y;
-          double er = p.cek_r * kr - p.cek_i * ki;
-          double ei = p.cek_r * ki + p.cek_i * kr;
+          double er = cek_r * kr - cek_i * ki;
+          double ei = cek_r * ki + cek_i * kr;
 #pragma unroll
           for (int qq = 1; qq < NP; qq++) {
             const V pv = e ? P[qq].b : P[qq].a;
@@ -504,8 +540,8 @@ __global__ void __launch_bounds__(288)
           const V psi0 = e ? P[0].b : P[0].a;
           const V k1 = e ? P[NP > 1 ? 1 : 0].b : P[NP > 1 ? 1 : 0].a;
           const double apsi = hypot((double)psi0.x, (double)psi0.y);
-          const double m = hypot((double)k1.x, (double)k1.y) * p.inv_absdt;
-          const double sr = apsi + p.dt0_r * m + 1e-30, si = p.dt0_i * m;
+          const double m = hypot((double)k1.x, (double)k1.y) * inv_absdt;
+          const double sr = apsi + dt0_r * m + 1e-30, si = dt0_i * m;
           red1 = fmax(red1, hypot(er, ei) / hypot(sr, si));
         }
       }

@@ -197,8 +197,19 @@ class GpeSolver:
         self.last_info = info
         return out
 
+    def step_series(self, n: int):
+        """(dt taken, attempts) of the first n steps of the last rk45 advance."""
+        dts = np.zeros(max(n, 1))
+        att = np.zeros(max(n, 1), dtype=np.int32)
+        check(lib().gpe_gpu_step_series(self._ctx, int(n),
+                                        dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        att.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+              self._ctx)
+        return dts[:n], att[:n]
+
     def advance(self, nsteps: int) -> np.ndarray:
-        """nsteps fixed-step solver() calls with the per-step norm."""
+        """nsteps solver() calls with the per-step norm (rk45: nsteps accepted
+        steps, step control on the device)."""
         norms = np.zeros(max(nsteps, 1), dtype=np.float64)
         tm = self._tm()
         check(lib().gpe_gpu_advance(self._ctx, int(nsteps), ctypes.byref(tm),

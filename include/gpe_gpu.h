@@ -175,12 +175,27 @@ int gpe_gpu_solver_host(gpe_ctx* ctx, const void* var_in, void* var_out,
                         int32_t elem_bytes, gpe_time* tm,
                         gpe_step_info* info);
 
-/* nsteps fixed-step solver() calls (euler/rk2/rk4) replayed from one CUDA
- * graph, with get_norm after every step as the reference loop does
- * (src/gpe.f90:241-243); norms (HOST, may be NULL) receives nsteps values.
- * tm->p is advanced by nsteps.  rk45 is stepped one call at a time. */
+/* nsteps solver() calls with get_norm after every step as the reference
+ * loop does (src/gpe.f90:241-243); norms (HOST, may be NULL) receives nsteps
+ * values; tm->p is advanced by the steps taken.  euler/rk2/rk4 steps are
+ * enqueued back to back with no host synchronisation until the end.  rk45
+ * takes nsteps accepted steps with the rkqs step control on the device
+ * (src/solve.f90:158-244): each step is one CUDA graph, a conditional WHILE
+ * node around the six Cash-Karp stages, the error and norm reductions and a
+ * one-thread control kernel that accepts and grows dt or shrinks it and
+ * retries, so no attempt waits for the host (contexts joined to NCCL, or
+ * with timing on, run the same kernels with one read-back per attempt).  A
+ * non-finite error estimate or 10000 rejected attempts stop the run early
+ * (GPE_ERR_NAN / GPE_ERR_UNDERFLOW, tm then holds the last accepted step).
+ * With a post-step correction attached, rk45 steps go one at a time. */
 int gpe_gpu_advance(gpe_ctx* ctx, int64_t nsteps, gpe_time* tm,
                     double* norms);
+
+/* The accepted dt (real part) and attempt count of the first n steps of the
+ * last rk45 gpe_gpu_advance (HOST arrays, either may be NULL); n beyond the
+ * steps it took is GPE_ERR_INVALID.  No reference counterpart: the
+ * reference writes dt to timestep.dat every save_rate steps (rkqs). */
+int gpe_gpu_step_series(gpe_ctx* ctx, int64_t n, double* dt_did, int32_t* attempts);
 
 /* get_norm (src/variables.f90:537-559 with integrate_x/y/z :713-823) of the
  * resident state, FP64. */

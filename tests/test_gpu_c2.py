@@ -21,8 +21,10 @@ steps and to 3e-5 by t = 20, and the next dt (errmax^-0.2) to 1e-8 and
   count at every step; accepted dt and next dt within 1e-7 over the first 100
   steps and 5e-5 over the run; psi at the end within 5e-8 relative L2, norm
   and energy within 1e-10;
-* free run (the GPU on its own step sequence): the same numbers of steps and
-  attempts, end time within 1e-7, psi within 2e-7;
+* free run (the GPU on its own step sequence, one advance with the step
+  control on the device): the same attempt count at every step, the dt
+  sequence within the lockstep margins, end time within 1e-7, psi within
+  2e-7;
 * complex64 + Kahan with FP64 step control, on its own step sequence:
   density within 5e-3 of the oracle (FP32 error estimates choose other steps
   and its last step ends at a slightly different time).
@@ -47,12 +49,6 @@ def c2_runs():
     oracle.set_threads(os.cpu_count() or 1)
     psi0 = bench.c2_initial_state()
     p = bench.c2_params(16, False)
-    free = GpeSolver(p, dt=0.005)
-    free.set_state(psi0)
-    free_steps = free_attempts = 0
-    while free.t + free.im_t <= T_END:
-        free_attempts += free.solver().attempts
-        free_steps += 1
     lock = GpeSolver(p, dt=0.005)
     lock.set_state(psi0)
     o = oracle.Oracle(oracle.OracleParams(nx=p.nx, ny=p.ny, nz=p.nz, xr=p.xr, yr=p.yr,
@@ -68,10 +64,16 @@ def c2_runs():
         q, em, att = o.solver(q, tm)
         rows.append((info.attempts, att, info.dt_did_re, tm.t - t_before, lock.dt.real,
                      tm.dt_re))
+    # the free run: as many accepted steps in one advance, step control on
+    # the device, no host synchronisation between attempts
+    free = GpeSolver(p, dt=0.005)
+    free.set_state(psi0)
+    free.advance(len(rows))
+    free_dt, free_att = free.step_series(len(rows))
     out = {"rows": rows, "t": tm.t, "psi": q, "norm": o.get_norm(q), "E": o.energy(q),
            "lock_psi": lock.get_state(), "lock_norm": lock.get_norm(),
            "lock_E": lock.energy()[0], "free_psi": free.get_state(), "free_t": free.t,
-           "free_steps": free_steps, "free_attempts": free_attempts}
+           "free_dt": free_dt, "free_att": free_att}
     for s in (free, lock):
         s.close()
     o.close()
@@ -97,8 +99,9 @@ def test_c2_complex128_state_matches_oracle(c2_runs):
 
 def test_c2_free_run_matches_oracle(c2_runs):
     r = c2_runs
-    assert r["free_steps"] == len(r["rows"])
-    assert r["free_attempts"] == sum(row[1] for row in r["rows"])
+    assert list(r["free_att"]) == [row[1] for row in r["rows"]]
+    for k, (d, row) in enumerate(zip(r["free_dt"], r["rows"])):
+        assert d == pytest.approx(row[3], rel=1e-7 if k < 100 else 5e-5), f"step {k + 1}"
     assert r["free_t"] == pytest.approx(r["t"], rel=1e-7)
     assert rel_l2(r["free_psi"], r["psi"]) < 2e-7
 

@@ -422,3 +422,54 @@ def test_stage_kernel_waits_run_out_and_the_context_survives(scheme, order, bcs,
     exp, _, _ = o.solver(psi, tm)
     assert rel_l2(g.get_state(), exp) < (2e-6 if kahan else 1e-12)
     g.close()
+
+
+@pytest.mark.parametrize("precision,kahan,bcs,rt", [(16, False, 2, True), (8, True, 1, True),
+                                                    (16, False, 1, False)])
+def test_rk45_advance_equals_single_steps(precision, kahan, bcs, rt):
+    """rk45 advance(n): n accepted steps from captured WHILE-node graphs with
+    the step control on the device, bitwise equal to n solver() calls (which
+    run the same kernels) and to the host-driven attempt loop (timing on),
+    with the per-step dt and attempts recorded."""
+    n = (40, 20, 16)
+    kw = dict(precision=precision, kahan=kahan, omx=0.3, omy=0.2, omz=0.4, g=1.3, mu=0.9)
+    psi = random_field((n[2], n[1], n[0]), seed=21)
+    dt0 = 0.02 if rt else -0.02j
+    runs = []
+    for mode in ("advance", "solver", "timed"):
+        g, _ = pair(n, (8.0, 4.0, 3.5), "rk45", 4, bcs, 4, rt, **kw)
+        g.dt = dt0
+        g.set_state(psi)
+        if mode == "timed":
+            g.set_timing(True)
+        if mode == "solver":
+            infos = [g.solver() for _ in range(12)]
+            series = ([i.dt_did_re if rt else i.dt_did_im for i in infos],
+                      [i.attempts for i in infos])
+            norms = None
+        else:
+            norms = g.advance(12)
+            d, a = g.step_series(12)
+            series = (list(d), list(a))
+        runs.append((g.get_state(np.complex128), g.t, g.im_t, g.dt, series, norms))
+        g.close()
+    (s0, t0, i0, d0, ser0, n0), (s1, t1, i1, d1, ser1, _), (s2, t2, i2, d2, ser2, n2) = runs
+    assert np.array_equal(s0, s1) and np.array_equal(s0, s2)
+    assert (t0, i0, d0) == (t1, i1, d1) == (t2, i2, d2)
+    if rt:
+        assert ser0 == ser1 == ser2
+    assert np.array_equal(n0, n2)
+    assert max(ser0[1]) >= 1
+
+
+def test_rk45_advance_halts_on_a_non_finite_error_estimate():
+    n = (24, 10, 8)
+    g, _ = pair(n, (6.0, 3.0, 2.5), "rk45", 4, 1, 2, True)
+    psi = random_field((n[2], n[1], n[0]), seed=4)
+    psi[3, 4, 5] = np.nan
+    g.dt = 0.01
+    g.set_state(psi)
+    with pytest.raises(GpeError) as e:
+        g.advance(5)
+    assert e.value.code == 5
+    g.close()

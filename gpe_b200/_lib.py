@@ -41,6 +41,7 @@ class GpeParamsC(ctypes.Structure):
         ("omx", ctypes.c_double), ("omy", ctypes.c_double), ("omz", ctypes.c_double),
         ("kahan", ctypes.c_int32), ("device", ctypes.c_int32),
         ("tile_y", ctypes.c_int32), ("zchunk", ctypes.c_int32),
+        ("fd_match", ctypes.c_double),
     ]
 
 

@@ -603,9 +603,13 @@ int fill_run(gpe_ctx* c, const StageSpec& sp, int R, const LaunchShape& sh,
   for (int o = 0; o < sp.nout; o++) rd->out[o] = static_cast<TS*>(c->fld[sp.out[o]]);
   const double h2[3] = {c->dx * c->dx, c->dy * c->dy, c->dz * c->dz};
   double c1[3], c2[3];
+  const double r2 = c->prm.fd_match * c->prm.fd_match;
   for (int a = 0; a < 3; a++) {
     if (R == 1) { c1[a] = 1.0 / h2[a]; c2[a] = 0.0; }
-    else { c1[a] = 16.0 / (12.0 * h2[a]); c2[a] = -1.0 / (12.0 * h2[a]); }
+    else if (c->prm.fd_match > 0.0) {
+      c1[a] = (4.0 - r2) / (3.0 * h2[a]);
+      c2[a] = (r2 - 1.0) / (12.0 * h2[a]);
+    } else { c1[a] = 16.0 / (12.0 * h2[a]); c2[a] = -1.0 / (12.0 * h2[a]); }
   }
   rd->cx1 = (TC)c1[0]; rd->cx2 = (TC)c2[0];
   rd->cy1 = (TC)c1[1]; rd->cy2 = (TC)c2[1];
@@ -1868,6 +1872,8 @@ int gpe_gpu_create(const gpe_params* prm, gpe_ctx** out) {
     return fail(nullptr, GPE_ERR_INVALID, "tile_y must be 0, 4 or 8");
   if (p.xr <= 0 || p.yr <= 0 || p.zr <= 0)
     return fail(nullptr, GPE_ERR_INVALID, "xr, yr, zr must be positive");
+  if (p.fd_match != 0.0 && (p.order != 4 || !(p.fd_match > 0.0 && p.fd_match < 1.5)))
+    return fail(nullptr, GPE_ERR_INVALID, "fd_match needs order 4 and 0 < fd_match < 1.5");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p.device || p.device < 0) {
     cudaGetLastError();
@@ -2530,7 +2536,8 @@ int gpe_group_create(gpe_ctx* const* members, int32_t n, gpe_group** out) {
     if (c->dev != c0->dev || c->nx != c0->nx || c->ny != c0->ny || c->es != c0->es ||
         a.scheme != b.scheme || a.order != b.order || a.bcs != b.bcs ||
         a.eqn_to_solve != b.eqn_to_solve || a.kahan != b.kahan || a.real_time != b.real_time ||
-        a.xr != b.xr || a.yr != b.yr || a.zr != b.zr || c->nzg != c0->nzg)
+        a.xr != b.xr || a.yr != b.yr || a.zr != b.zr || a.fd_match != b.fd_match ||
+        c->nzg != c0->nzg)
       return gfail(nullptr, GPE_ERR_INVALID,
                    "members must share device, nx, ny, precision, scheme, order, boundary, "
                    "equation, time direction, box and global z axis");

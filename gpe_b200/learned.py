@@ -65,16 +65,23 @@ class LearnedConfig:
     t_end: float = 50.0
     checkpoints: list = field(default_factory=lambda: [1.0, 5.0, 10.0, 20.0, 50.0])
     device: int = 0
+    # coarse base: order 2, or order 4 with coarse_match = r > 0 (a Laplacian
+    # that disperses like the 2nd-order one at spacing r h: r = 0.5 matches
+    # the fine grid), or plain order 4 with coarse_order = 4, coarse_match = 0
+    coarse_order: int = 2
+    coarse_match: float = 0.0
 
     @property
     def coarse_h(self) -> float:
         return self.fine_h * self.fine_n / self.coarse_n
 
 
-def params(n: int, h: float, precision: int, kahan: bool = False, device: int = 0) -> GpeParams:
+def params(n: int, h: float, precision: int, kahan: bool = False, device: int = 0,
+           order: int = 2, fd_match: float = 0.0) -> GpeParams:
     xr = (n - 1) * h / 2
     return GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
-                     order=2, precision=precision, kahan=kahan, g=1.0, mu=1.0, device=device)
+                     order=order, precision=precision, kahan=kahan, g=1.0, mu=1.0, device=device,
+                     fd_match=fd_match)
 
 
 def fine_solver(cfg: LearnedConfig, seed: int, precision: int = 16, kahan: bool = False,
@@ -91,7 +98,8 @@ def fine_solver(cfg: LearnedConfig, seed: int, precision: int = 16, kahan: bool 
 
 
 def coarse_solver(cfg: LearnedConfig) -> GpeSolver:
-    return GpeSolver(params(cfg.coarse_n, cfg.coarse_h, 8, cfg.coarse_kahan, cfg.device), dt=cfg.dt)
+    return GpeSolver(params(cfg.coarse_n, cfg.coarse_h, 8, cfg.coarse_kahan, cfg.device,
+                            cfg.coarse_order, cfg.coarse_match), dt=cfg.dt)
 
 
 def restricted(cfg: LearnedConfig, fine: GpeSolver):
@@ -261,6 +269,10 @@ def main(argv=None) -> int:
     ap.add_argument("--rollout", type=int)
     ap.add_argument("--noise", type=float)
     ap.add_argument("--dt", type=float, help="coarse step (a multiple of the fine 0.01)")
+    ap.add_argument("--checkpoints", help="comma-separated times, or start:stop:step")
+    ap.add_argument("--coarse-order", type=int, choices=[2, 4])
+    ap.add_argument("--coarse-match", type=float, help="order-4 dispersion match r (0.5: fine grid)")
+    ap.add_argument("--no-net", action="store_true", help="evaluate the coarse base alone")
     a = ap.parse_args(argv)
     cfg = LearnedConfig()
     if a.iters is not None:
@@ -288,10 +300,28 @@ def main(argv=None) -> int:
     if a.dt is not None:
         cfg.fine_substeps = int(round(a.dt / (cfg.dt / cfg.fine_substeps)))
         cfg.dt = a.dt
+    if a.coarse_match is not None:
+        cfg.coarse_order, cfg.coarse_match = 4, a.coarse_match
+    if a.coarse_order is not None:
+        cfg.coarse_order = a.coarse_order
+    if a.checkpoints:
+        if ":" in a.checkpoints:
+            t0_, t1_, st_ = (float(v) for v in a.checkpoints.split(":"))
+            cfg.checkpoints = [round(v, 10) for v in np.arange(t0_, t1_ + 1e-9, st_)]
+        else:
+            cfg.checkpoints = [float(v) for v in a.checkpoints.split(",")]
     import torch
     torch.cuda.set_device(cfg.device)
     n = cfg.coarse_n
     report = {"config": asdict(cfg)}
+    if a.no_net:
+        res = evaluate(cfg, None, cfg.eval_seeds, cfg.t_end, cfg.checkpoints)
+        report["eval"] = res
+        report["summary"] = summarize(res)
+        with open(a.out, "w") as fh:
+            json.dump(report, fh, indent=1)
+        print(json.dumps(report["summary"]))
+        return 0
     if a.load:
         z = np.load(a.load)
         w, b = z["w"], z["b"]

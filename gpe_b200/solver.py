@@ -52,6 +52,7 @@ class GpeParams:
     device: int = 0
     tile_y: int = 0
     zchunk: int = 0
+    fd_match: float = 0.0  # order 4: Laplacian dispersing like 2nd order at spacing fd_match*h
 
     def to_c(self) -> GpeParamsC:
         c = GpeParamsC()

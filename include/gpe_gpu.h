@@ -77,6 +77,14 @@ typedef struct gpe_params {
   int32_t device;       /* CUDA device ordinal */
   int32_t tile_y;       /* 0 = auto; else rows per tile (4 or 8) */
   int32_t zchunk;       /* 0 = auto; else z-planes per block */
+  double fd_match;      /* order 4 only, 0 = the centred 4th-order Laplacian.
+                           r in (0, 1.5): per-axis coefficients
+                           c1 = (4 - r^2)/(3 h^2), c2 = (r^2 - 1)/(12 h^2),
+                           whose symbol k^2 - k^4 (r h)^2 / 12 + O(k^6 h^4)
+                           is that of the 2nd-order Laplacian on a grid of
+                           spacing r h: a coarse grid that disperses like a
+                           finer one (the learned correction's base).  No
+                           reference counterpart. */
 } gpe_params;
 
 /* The solver's time globals: t, im_t, dt (complex), p

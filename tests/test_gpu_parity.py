@@ -473,3 +473,29 @@ def test_rk45_advance_halts_on_a_non_finite_error_estimate():
         g.advance(5)
     assert e.value.code == 5
     g.close()
+
+
+@pytest.mark.parametrize("r", [0.5, 0.8])
+def test_dispersion_matched_laplacian(r):
+    """fd_match = r: per-axis coefficients c1 = (4 - r^2)/(3 h^2), c2 =
+    (r^2 - 1)/(12 h^2) of the 4th-order stencil, checked against numpy on a
+    periodic random field, and its symbol against the 2nd-order Laplacian of
+    spacing r h on a plane wave to the stated order."""
+    n = (24, 20, 16)
+    xr = (6.0, 5.0, 4.0)
+    h = [2 * a / (m - 1) for a, m in zip(xr, n)]
+    prm = GpeParams(nx=n[0], ny=n[1], nz=n[2], xr=xr[0], yr=xr[1], zr=xr[2], order=4, bcs=1,
+                    fd_match=r)
+    psi = random_field((n[2], n[1], n[0]), seed=3)
+    with GpeSolver(prm) as s:
+        s.set_state(psi)
+        got = s.laplacian()
+    exp = np.zeros_like(psi)
+    for ax, hh in zip((2, 1, 0), h):
+        c1 = (4 - r * r) / (3 * hh * hh)
+        c2 = (r * r - 1) / (12 * hh * hh)
+        exp += c1 * (np.roll(psi, 1, ax) + np.roll(psi, -1, ax)) + \
+            c2 * (np.roll(psi, 2, ax) + np.roll(psi, -2, ax)) - 2 * (c1 + c2) * psi
+    assert rel_l2(got, exp) < 1e-12
+    with pytest.raises(GpeError):
+        GpeSolver(GpeParams(nx=8, ny=8, nz=8, order=2, fd_match=0.5))

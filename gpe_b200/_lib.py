@@ -222,6 +222,32 @@ def device_field(t, shape, device: int, what: str, elem_bytes: int | None = None
     return eb
 
 
+class _PinnedBlock:
+    """Page-locked host memory from gpe_gpu_host_alloc, freed with the object."""
+
+    def __init__(self, nbytes: int):
+        self.ptr = lib().gpe_gpu_host_alloc(max(int(nbytes), 1))
+        if not self.ptr:
+            raise GpeError(4, f"cudaHostAlloc of {nbytes} bytes failed")
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().gpe_gpu_host_free(self.ptr)
+            self.ptr = None
+
+
+def pinned_empty(shape, dtype):
+    """A numpy array in page-locked host memory (device-to-host copies into it
+    run at the link's full rate); the memory lives as long as the array."""
+    import numpy as np
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape)) if len(shape) else 1
+    blk = _PinnedBlock(n * dt.itemsize)
+    buf = (ctypes.c_char * max(n * dt.itemsize, 1)).from_address(blk.ptr)
+    buf._block = blk  # keeps the memory alive with the buffer
+    return np.frombuffer(buf, dtype=dt, count=n).reshape(shape)
+
+
 def check(rc: int, ctx=None) -> None:
     if rc != GPE_OK:
         msg = lib().gpe_gpu_last_error(ctx)

@@ -184,7 +184,9 @@ __global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
   T->attempts += 1;
   T->errmax = errmax;
   bool done = false;
-  if (!isfinite(errmax)) {
+  // the error maximum skips NaN sites (fmax, as maxval does), so a state
+  // that went non-finite shows in the fused norm of the trial state
+  if (!isfinite(errmax) || !isfinite(scal[0])) {
     T->halt = 5;  // GPE_ERR_NAN
     done = true;
   } else if (errmax <= 1.0) {

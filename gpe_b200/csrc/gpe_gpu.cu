@@ -1283,7 +1283,8 @@ int rk45_load(gpe_ctx* c, const gpe_time* tm) {
 }
 
 int rk45_halted(gpe_ctx* c, const DevTime& h) {
-  if (h.halt == GPE_ERR_NAN) return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate");
+  if (h.halt == GPE_ERR_NAN)
+    return fail(c, GPE_ERR_NAN, "non-finite rk45 error estimate or trial-state norm");
   if (h.halt) return fail(c, GPE_ERR_UNDERFLOW, "rk45: step size control did not converge");
   return GPE_OK;
 }

@@ -305,11 +305,14 @@ def main(argv=None) -> int:
     if a.coarse_order is not None:
         cfg.coarse_order = a.coarse_order
     if a.checkpoints:
-        if ":" in a.checkpoints:
-            t0_, t1_, st_ = (float(v) for v in a.checkpoints.split(":"))
-            cfg.checkpoints = [round(v, 10) for v in np.arange(t0_, t1_ + 1e-9, st_)]
-        else:
-            cfg.checkpoints = [float(v) for v in a.checkpoints.split(",")]
+        ck = []
+        for item in a.checkpoints.split(","):
+            if ":" in item:
+                t0_, t1_, st_ = (float(v) for v in item.split(":"))
+                ck += [round(v, 10) for v in np.arange(t0_, t1_ + 1e-9, st_)]
+            else:
+                ck.append(float(item))
+        cfg.checkpoints = sorted(set(ck))
     import torch
     torch.cuda.set_device(cfg.device)
     n = cfg.coarse_n

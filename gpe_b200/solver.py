@@ -304,10 +304,12 @@ class GpeSolver:
     def zeros(self):
         """get_zeros / get_extra_zeros / get_re_im_zeros (src/io.f90:895-1402)
         -> (counts[12], points (n, 3)), sections in the reference's order."""
+        from ._lib import pinned_empty
         counts = np.zeros(12, dtype=np.int64)
         P64 = ctypes.POINTER(ctypes.c_int64)
         check(lib().gpe_gpu_zeros(self._ctx, counts.ctypes.data_as(P64), None, 0), self._ctx)
-        pts = np.zeros((max(int(counts.sum()), 1), 3))
+        # page-locked: the point list can run to gigabytes
+        pts = pinned_empty((max(int(counts.sum()), 1), 3), np.float64)
         check(lib().gpe_gpu_zeros(self._ctx, counts.ctypes.data_as(P64),
                                   pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                   pts.shape[0]), self._ctx)

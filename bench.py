@@ -20,7 +20,9 @@ by the batched launches (autotuned launch shape), next to the same runs
 stepped one context at a time.
 
 N > 1 (launched by torchrun): every rank advances its own 512^3 replica
-(weak scaling, no data-path collective); device time is the max over ranks.
+(weak scaling, no data-path collective); with --decomp slab the ranks share
+one 512^3 grid as NCCL z-slabs (strong scaling).  Device time is the max over
+ranks.
 --impl reference times the CPU restatement of the reference's path (the
 reference's Fortran build is unavailable in this image) on the host cores.
 """
@@ -757,6 +759,9 @@ def main():
     ap.add_argument("--workload", default="cube",
                     choices=["cube", "ensemble", "learned", "rkf45", "spectrum"])
     ap.add_argument("--t-end", type=float, default=20.0, help="rkf45 workload end time")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="N > 1: independent 512^3 replicas per GPU (weak scaling), or one "
+                         "512^3 grid split into NCCL z-slabs (strong scaling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -796,10 +801,19 @@ def main():
     xr = H * (n - 1) / 2
     prm = GpeParams(nx=n, ny=n, nz=n, xr=xr, yr=xr, zr=xr, scheme="rk4", eqn_to_solve=4, bcs=1,
                     order=4, precision=8, kahan=True, g=1.0, mu=1.0, device=local)
-    s = GpeSolver(prm, tau=DT)
+    slab = world > 1 and args.decomp == "slab"
     from gpe_b200.ic import random_phase
     psi0 = random_phase(torch, n, H, KMAX, 0, torch.device("cuda", local))
-    s.set_state(psi0)
+    if slab:
+        # one grid, z-slabs by para_range, NCCL ghost exchange after every
+        # stage and all-reduced norms (the reference's MPI decomposition)
+        from gpe_b200.dist import SlabSolver
+        s = SlabSolver(prm, rank, world, dist, device=local, tau=DT)
+        a, b = s.plan.z_range
+        s.set_state(psi0[a:b + 1].contiguous())
+    else:
+        s = GpeSolver(prm, tau=DT)
+        s.set_state(psi0)
     del psi0
     torch.cuda.empty_cache()
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
@@ -836,8 +850,10 @@ def main():
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_max = float(t.item())
-    sites = n ** 3
-    value = world * sites * args.steps / (ms_max / 1e3)
+    # sites this rank steps, and the job's site-updates per step
+    sites = n * n * (s.plan.nz if slab else n)
+    job_sites = n ** 3 if slab else world * n ** 3
+    value = job_sites * args.steps / (ms_max / 1e3)
 
     # roofline of the dominant kernel family and of the whole step
     peak, peak_kind = load_peaks()
@@ -894,7 +910,7 @@ def main():
         e2e_ms = float(t.item())
     L.gpe_gpu_host_free(ctypes.c_void_p(hin))
     L.gpe_gpu_host_free(ctypes.c_void_p(hout))
-    e2e = {"value": world * sites / (e2e_ms / 1e3), "unit": "site-updates/s",
+    e2e = {"value": job_sites / (e2e_ms / 1e3), "unit": "site-updates/s",
            "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": e2e_ms,
            "form": "gpe_gpu_solver_host: pinned host psi in -> step -> host psi out, per step"}
 
@@ -906,7 +922,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize(local)
     res_ms = e0.elapsed_time(e1) / ke
-    e2e_resident = {"value": world * sites / (res_ms / 1e3), "unit": "site-updates/s",
+    e2e_resident = {"value": job_sites / (res_ms / 1e3), "unit": "site-updates/s",
                     "h2d_bytes_per_step": ctypes.sizeof(GpeTimeC), "d2h_bytes_per_step": 8,
                     "ms_per_step": res_ms,
                     "form": "psi resident; per step gpe_gpu_solver + gpe_gpu_norm (8 B read back)"}
@@ -925,9 +941,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong" if slab else "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random-phase IC, |k|<=1.0, torch Philox seed 0)",
-            "config": workload_config(world, n),
+            "config": dict(workload_config(world, n),
+                           parallelism=(f"z-slabs x{world} (NCCL)" if slab else
+                                        workload_config(world, n)["parallelism"])),
             "hbm_gbs_step": step_gbs,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_resident": e2e_resident,
             "clocks": clocks, "gpu_launches": int(launches),

@@ -393,7 +393,7 @@ using KernelFn = const void*;
 // TY = 4.  (Two CTAs with four slots beat one CTA with eight on the rk4
 // last stage at 512^3: 1.30 against 1.49 ms; the second CTA's warps hide
 // the first's latency better than a deeper ring.)
-LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1) {
+LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1, int max_ctas = 2) {
   LaunchShape s{};
   int TY = tile_y > 0 ? tile_y : 8;
   for (int attempt = 0; attempt < 2; attempt++) {
@@ -403,6 +403,14 @@ LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1) {
     s.halo_smem = (unsigned)round_up(s.halo_box, 128);
     s.pt_smem = (unsigned)round_up(s.pt_box, 128);
     const size_t stage = (size_t)ns * s.halo_smem + (size_t)np * s.pt_smem;
+    if (max_ctas >= 3) {
+      // three CTAs per SM when their rings still keep two planes in flight
+      const int S3 = (int)std::min<size_t>(8, (72 * 1024 - 128) / stage);
+      if (S3 >= R + 3) {
+        s.S = S3;
+        break;
+      }
+    }
     int S = (int)std::min<size_t>(8, (110 * 1024 - 128) / stage);
     if (S < R + 2) S = (int)std::min<size_t>(8, (220 * 1024 - 128) / stage);
     if (S >= R + 2 || attempt == 1 || tile_y > 0) {
@@ -420,13 +428,16 @@ LaunchShape ring_shape(int es, int R, int np, int tile_y, int ns = 1) {
 // one that minimises (waves of CTAs) x (planes per CTA + pipeline fill),
 // which trades the last wave's idle SMs against the R extra halo planes and
 // the fill latency every chunk pays.
-int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, int ns, LaunchShape* out) {
+int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, int ns, bool occ3, LaunchShape* out) {
   auto hit = c->shapes.find(fn);
   if (hit != c->shapes.end()) {
     *out = hit->second;
     return GPE_OK;
   }
-  LaunchShape s = ring_shape(c->es, R, np, c->prm.tile_y, ns);
+  // occ3_recipe: complex64 stencil-only recipes are built for 3 CTAs/SM (the
+  // energy recipe computes in FP64 and is not one of them)
+  const int max_ctas = occ3 ? 3 : 2;
+  LaunchShape s = ring_shape(c->es, R, np, c->prm.tile_y, ns, max_ctas);
   s.ntx = (c->nx + TX - 1) / TX;
   s.nty = (c->ny + s.TY - 1) / s.TY;
   CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -461,12 +472,31 @@ int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, int ns, LaunchShape* ou
 
 // The stage recipes that the schemes use; see stage_kernel.cuh for the
 // meaning of (NP, NOUT, EPI, AMASK, BMASK).  BMASK bit o*8+q: beta[o][q] != 0.
+// The recipes built for three CTAs per SM (stage_kernel_occ3): complex64
+// single-run stages that stage only stencil planes.
+template <typename TS, typename TC>
+constexpr bool occ3_recipe(int np, bool full, bool batch) {
+  return std::is_same<TS, float>::value && std::is_same<TC, float>::value && np == 0 && !full &&
+         !batch;
+}
+
+// The entry of one recipe (only that one is instantiated).
+template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AM, int BM,
+          bool FULL, bool BATCH>
+KernelFn kernel_for() {
+  if constexpr (occ3_recipe<TS, TC>(NP, FULL, BATCH))
+    return reinterpret_cast<KernelFn>(
+        &stage_kernel_occ3<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FULL, BATCH>);
+  else
+    return reinterpret_cast<KernelFn>(
+        &stage_kernel<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FULL, BATCH>);
+}
+
 template <typename TS, typename TC, int R, bool FULL, bool BATCH>
 KernelFn pick_kernel(int ns, int np, int nout, int epi, int am, int bm) {
 #define GPE_CASE(NS_, NP_, NOUT_, EPI_, AM_, BM_)                                      \
   if (ns == NS_ && np == NP_ && nout == NOUT_ && epi == (EPI_) && am == AM_ && bm == BM_) \
-    return reinterpret_cast<KernelFn>(                                                 \
-        &stage_kernel<TS, TC, R, NS_, NP_, NOUT_, (EPI_), AM_, BM_, FULL, BATCH>);
+    return kernel_for<TS, TC, R, NS_, NP_, NOUT_, (EPI_), AM_, BM_, FULL, BATCH>();
   if constexpr (BATCH) {
     // batched ensembles step with rk4
     if constexpr (std::is_same<TS, TC>::value) {
@@ -690,7 +720,8 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   KernelFn fn = select_kernel<TS, TC, false>(R, kfull, sp, am, bm);
   if (!fn) return fail(c, GPE_ERR_INVALID, "no kernel for this stage shape");
   LaunchShape sh;
-  int rc = choose_shape(c, fn, R, sp.np, sp.stencil2 >= 0 ? 2 : 1, &sh);
+  int rc = choose_shape(c, fn, R, sp.np, sp.stencil2 >= 0 ? 2 : 1,
+                        occ3_recipe<TS, TC>(sp.np, kfull, false), &sh);
   if (rc) return rc;
   StageParams<TS, TC> p;
   memset(&p, 0, sizeof(p));

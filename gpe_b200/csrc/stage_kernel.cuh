@@ -140,10 +140,11 @@ __device__ __forceinline__ bool near_edge(int i, int n) {
 template <int K>
 using IC = std::integral_constant<int, K>;
 
+// The kernel body; the __global__ entries below differ only in their
+// register budget.
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
           int BMASK, bool FULL, bool BATCH>
-__global__ void __launch_bounds__(288)
-    stage_kernel(const __grid_constant__ StageParams<TS, TC> p) {
+__device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   using V = typename VT<TC>::T;
   using RD = RunDesc<TS, TC>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -664,6 +665,25 @@ __global__ void __launch_bounds__(288)
     for (int u = max(0, issued - S); u < issued; u++)
       mbar_wait_bounded(&full[u % S], (uint32_t)((u / S) & 1), drain);
   }
+}
+
+// Budget left to the compiler (one to two CTAs per SM, by shared memory).
+template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
+          int BMASK, bool FULL, bool BATCH>
+__global__ void __launch_bounds__(288)
+    stage_kernel(const __grid_constant__ StageParams<TS, TC> p) {
+  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FULL, BATCH>(p);
+}
+
+// Registers capped for three resident CTAs per SM: the complex64 recipes
+// that stage only stencil planes, whose warps mostly wait on fixed-latency
+// and shared-memory dependencies, so more warps per scheduler hide more of
+// it (their three rings of slots fit in shared memory).
+template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
+          int BMASK, bool FULL, bool BATCH>
+__global__ void __launch_bounds__(288, 3)
+    stage_kernel_occ3(const __grid_constant__ StageParams<TS, TC> p) {
+  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FULL, BATCH>(p);
 }
 
 }  // namespace gpe

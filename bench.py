@@ -373,7 +373,8 @@ def run_learned(args):
     import torch
 
     from gpe_b200.cnn import CoarseCorrector, init_weights
-    from gpe_b200.learned import LearnedConfig, coarse_solver, fine_solver, restricted
+    from gpe_b200.learned import (LearnedConfig, coarse_solver, config_from_weights,
+                                  fine_solver, restricted)
 
     torch.cuda.set_device(0)
     cfg = LearnedConfig()
@@ -382,6 +383,7 @@ def run_learned(args):
     if os.path.exists(wpath):
         z = np.load(wpath)
         w, b = z["w"], z["b"]
+        cfg = config_from_weights(z, cfg)
         wsrc = "trained (gpe_b200/data/cnn_weights.npz)"
     else:
         w, b = init_weights(7)
@@ -408,7 +410,7 @@ def run_learned(args):
     ms_fine = timed(fine, steps)
     ms_plain = timed(c, steps)
     n = cfg.coarse_n
-    net = CoarseCorrector(n, n, n, out_scale=cfg.out_scale)
+    net = CoarseCorrector(n, n, n, out_scale=cfg.out_scale, preserve_norm=cfg.preserve_norm)
     net.set_weights(w, b)
     st = torch.cuda.ExternalStream(c.stream_handle())
     for _ in range(3):

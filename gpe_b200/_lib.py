@@ -71,7 +71,7 @@ class GpeBatchOptsC(ctypes.Structure):
 class GpeCnnParamsC(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
                 ("nz", ctypes.c_int32), ("device", ctypes.c_int32), ("train", ctypes.c_int32),
-                ("out_scale", ctypes.c_float), ("reserved", ctypes.c_int32)]
+                ("out_scale", ctypes.c_float), ("preserve_norm", ctypes.c_int32)]
 
 
 # Every symbol include/gpe_gpu.h and include/gpe_cnn.h declare, with (restype, argtypes).

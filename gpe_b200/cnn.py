@@ -42,10 +42,11 @@ def _fptr(a):
 
 class CoarseCorrector:
     def __init__(self, nx: int, ny: int, nz: int, device: int = 0, train: bool = False,
-                 out_scale: float = 0.01):
+                 out_scale: float = 0.01, preserve_norm: bool = False):
         p = GpeCnnParamsC()
         lib().gpe_cnn_default_params(ctypes.byref(p), nx, ny, nz)
         p.device, p.train, p.out_scale = device, int(bool(train)), float(out_scale)
+        p.preserve_norm = int(bool(preserve_norm))
         self._h = ctypes.c_void_p()
         check_cnn(lib().gpe_cnn_create(ctypes.byref(p), ctypes.byref(self._h)), None)
         self.shape = (nz, ny, nx)

@@ -74,6 +74,19 @@ __global__ void scale_kernel(TS* __restrict__ f, size_t nscalars, double snn,
   }
 }
 
+// The same rescaling with the factor sqrt(target / current) read on the
+// device (both norms left in device memory by earlier reductions).
+template <typename TS>
+__global__ void rescale_to_kernel(TS* __restrict__ f, size_t nscalars,
+                                  const double* __restrict__ target,
+                                  const double* __restrict__ current) {
+  const double s = sqrt(target[0] / current[0]);
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nscalars;
+       q += (size_t)gridDim.x * blockDim.x) {
+    f[q] = (TS)((double)f[q] * s);
+  }
+}
+
 // Weighted |psi|^2 per CTA into partials[2*blk] (get_norm without a stencil).
 template <typename TS>
 __global__ void norm_kernel(const TS* __restrict__ f, Geom g,

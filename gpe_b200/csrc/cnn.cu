@@ -227,7 +227,9 @@ int post_step_hook(void* arg, gpe_ctx* c) {
   gpe_cnn* n = static_cast<gpe_cnn*>(arg);
   FieldView v;
   if (gpe_internal_field_view(c, &v)) return GPE_ERR_INVALID;
-  return enqueue_apply(n, v, v.status);
+  const int rc = enqueue_apply(n, v, v.status);
+  if (rc || !n->prm.preserve_norm) return rc;
+  return gpe_internal_restore_norm(c);
 }
 
 // Training-path forward into d_delta (keeps T1..T3, P0..P2).

@@ -1617,6 +1617,36 @@ void gpe_internal_time_end(gpe_ctx* c, gpe::TimedRegion* r) {
 }
 int gpe_internal_load_stage(gpe_ctx* c) { return load_stage(c, c->es); }
 
+// psi rescaled on the context's stream so that its norm equals the norm the
+// last step fused into d_scal[0] (before any post-step correction); the
+// norm of psi as it stands goes to d_scal[8].  No host synchronisation.
+int gpe_internal_restore_norm(gpe_ctx* c) {
+  const Geom g = geom(c);
+  const int nb = elementwise_blocks(c->nint);
+  if (c->es == 8)
+    norm_kernel<float><<<nb, 256, 0, c->stream>>>((const float*)c->fld[c->psi_id], g,
+                                                  c->tabW[0], c->tabW[1], c->tabW[2],
+                                                  c->d_partials);
+  else
+    norm_kernel<double><<<nb, 256, 0, c->stream>>>((const double*)c->fld[c->psi_id], g,
+                                                   c->tabW[0], c->tabW[1], c->tabW[2],
+                                                   c->d_partials);
+  CU_CHECK(c, cudaGetLastError());
+  finalize_kernel<<<1, 1024, 0, c->stream>>>(c->d_partials, nb, 0, 0, cell_volume(c),
+                                              c->d_scal + 8, nullptr, c->d_counter);
+  const size_t n = c->npad * 2;
+  const int sb = elementwise_blocks(n);
+  if (c->es == 8)
+    rescale_to_kernel<float><<<sb, 256, 0, c->stream>>>((float*)c->fld[c->psi_id], n,
+                                                        c->d_scal, c->d_scal + 8);
+  else
+    rescale_to_kernel<double><<<sb, 256, 0, c->stream>>>((double*)c->fld[c->psi_id], n,
+                                                         c->d_scal, c->d_scal + 8);
+  CU_CHECK(c, cudaGetLastError());
+  c->launches += 3;
+  return GPE_OK;
+}
+
 // ==========================================================================
 // Batched ensembles: independent runs of uneven grids stepped by one
 // persistent launch per RK4 stage.  Each member is a full context (fields,

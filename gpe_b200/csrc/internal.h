@@ -59,5 +59,8 @@ std::unique_ptr<gpe::Extension>& gpe_internal_extension(gpe_ctx* c, int slot);
 int gpe_internal_load_stage(gpe_ctx* c);
 void gpe_internal_time_begin(gpe_ctx* c, gpe::TimedRegion* r, int family, int64_t sites);
 void gpe_internal_time_end(gpe_ctx* c, gpe::TimedRegion* r);
+// Enqueues psi *= sqrt(norm of the last step / norm of psi now) (the norm
+// kept through a post-step correction).
+int gpe_internal_restore_norm(gpe_ctx* c);
 // Adds n to the context's launch counter (kernels enqueued by other units).
 void gpe_internal_count_launches(gpe_ctx* c, int64_t n);

@@ -70,10 +70,30 @@ class LearnedConfig:
     # the fine grid), or plain order 4 with coarse_order = 4, coarse_match = 0
     coarse_order: int = 2
     coarse_match: float = 0.0
+    # rescale psi after every correction to the norm of the step it corrects
+    preserve_norm: bool = False
 
     @property
     def coarse_h(self) -> float:
         return self.fine_h * self.fine_n / self.coarse_n
+
+
+def config_from_weights(z, cfg: LearnedConfig | None = None) -> LearnedConfig:
+    """The coarse method a weights file was trained for (its dt, stencil,
+    output scale and norm handling), on top of cfg or the defaults."""
+    cfg = cfg or LearnedConfig()
+    if "out_scale" in z:
+        cfg.out_scale = float(z["out_scale"])
+    if "dt" in z:
+        dt = float(z["dt"])
+        cfg.fine_substeps = int(round(dt / (cfg.dt / cfg.fine_substeps)))
+        cfg.dt = dt
+    if "coarse_order" in z:
+        cfg.coarse_order = int(z["coarse_order"])
+        cfg.coarse_match = float(z["coarse_match"])
+    if "preserve_norm" in z:
+        cfg.preserve_norm = bool(z["preserve_norm"])
+    return cfg
 
 
 def params(n: int, h: float, precision: int, kahan: bool = False, device: int = 0,
@@ -273,6 +293,8 @@ def main(argv=None) -> int:
     ap.add_argument("--coarse-order", type=int, choices=[2, 4])
     ap.add_argument("--coarse-match", type=float, help="order-4 dispersion match r (0.5: fine grid)")
     ap.add_argument("--no-net", action="store_true", help="evaluate the coarse base alone")
+    ap.add_argument("--preserve-norm", action="store_true",
+                    help="keep the stepped norm through every correction")
     a = ap.parse_args(argv)
     cfg = LearnedConfig()
     if a.iters is not None:
@@ -304,6 +326,8 @@ def main(argv=None) -> int:
         cfg.coarse_order, cfg.coarse_match = 4, a.coarse_match
     if a.coarse_order is not None:
         cfg.coarse_order = a.coarse_order
+    if a.preserve_norm:
+        cfg.preserve_norm = True
     if a.checkpoints:
         ck = []
         for item in a.checkpoints.split(","):
@@ -328,8 +352,13 @@ def main(argv=None) -> int:
     if a.load:
         z = np.load(a.load)
         w, b = z["w"], z["b"]
+        if a.dt is None and a.coarse_match is None and a.coarse_order is None:
+            cfg = config_from_weights(z, cfg)  # the method the weights were trained for
+            cfg.preserve_norm = cfg.preserve_norm or a.preserve_norm
+            report["config"] = asdict(cfg)
     else:
-        net = CoarseCorrector(n, n, n, cfg.device, train=True, out_scale=cfg.out_scale)
+        net = CoarseCorrector(n, n, n, cfg.device, train=True, out_scale=cfg.out_scale,
+                              preserve_norm=cfg.preserve_norm)
         t0 = time.perf_counter()
         data = [generate(cfg, s, cfg.t_train) for s in cfg.train_seeds]
         report["generate_seconds"] = time.perf_counter() - t0
@@ -344,9 +373,13 @@ def main(argv=None) -> int:
                            "loss_first": float(np.mean(h[:m])), "loss_last": float(np.mean(h[-m:])),
                            "checks (iter, k, m, loss, zero-correction loss)": tr["checks"]}
         w, b = net.get_weights()
-        np.savez_compressed(a.weights, w=w, b=b, out_scale=cfg.out_scale)
+        # the weights carry the coarse method they were trained for
+        np.savez_compressed(a.weights, w=w, b=b, out_scale=cfg.out_scale, dt=cfg.dt,
+                            coarse_order=cfg.coarse_order, coarse_match=cfg.coarse_match,
+                            preserve_norm=cfg.preserve_norm)
         net.close()
-    net = CoarseCorrector(n, n, n, cfg.device, out_scale=cfg.out_scale)
+    net = CoarseCorrector(n, n, n, cfg.device, out_scale=cfg.out_scale,
+                          preserve_norm=cfg.preserve_norm)
     net.set_weights(w, b)
     t0 = time.perf_counter()
     res = evaluate(cfg, net, cfg.eval_seeds, cfg.t_end, cfg.checkpoints)

@@ -36,7 +36,9 @@ typedef struct gpe_cnn_params {
   int32_t device;
   int32_t train;         /* 1: allocate training buffers */
   float out_scale;       /* delta = out_scale * last layer output (default 0.01) */
-  int32_t reserved;
+  int32_t preserve_norm; /* 1: after each attached correction, psi is rescaled
+                            to the norm of the step it corrects (the
+                            correction then moves no mass) */
 } gpe_cnn_params;
 
 #define GPE_CNN_LAYERS 4

@@ -223,3 +223,33 @@ def test_trained_network_beats_the_plain_coarse_step_on_held_out_pairs():
             r.close()
         assert errs["learned"] < errs["plain"], errs
         c.close()
+
+
+def test_norm_preserving_correction_keeps_the_stepped_norm():
+    """preserve_norm: after the attached correction psi is rescaled to the norm
+    of the step it corrects, so the corrected state's norm equals the norm of
+    the same step taken without the network (complex64 storage: 1e-6)."""
+    n = (32, 16, 8)
+    psi = random_field((n[2], n[1], n[0]), seed=17).astype(np.complex64)
+    w, b = weights(3, last=0.3)
+    with CoarseCorrector(*n, out_scale=0.05, preserve_norm=True) as net, \
+            CoarseCorrector(*n, out_scale=0.05) as free:
+        net.set_weights(w, b)
+        free.set_weights(w, b)
+        plain, c = solver(n), solver(n)
+        c.set_state(psi)
+        net.attach(c)
+        c.advance(3)
+        start = c.get_state(np.complex64)
+        plain.set_state(start)
+        plain.solver()
+        c.solver()
+        assert c.get_norm() == pytest.approx(plain.get_norm(), rel=1e-6)
+        # the correction alone does move the norm
+        plain.set_state(start)
+        before = plain.get_norm()
+        free.apply(plain)
+        assert abs(plain.get_norm() - before) / before > 1e-5
+        CoarseCorrector.detach(c)
+        plain.close()
+        c.close()

@@ -118,3 +118,26 @@ def test_batch_create_validates_members_without_gpu(L):
     assert L.gpe_batch_advance(None, 1, 0.01, 0.0, None) == 1
     assert L.gpe_batch_launch_count(None) == -1
     L.gpe_batch_destroy(None)
+
+
+def test_new_entry_points_validate_without_a_device(L):
+    # slab groups need >= 2 members; null arguments are refused
+    g = ctypes.c_void_p()
+    assert L.gpe_group_create(None, 0, ctypes.byref(g)) == 1 and not g
+    assert b"2 members" in L.gpe_group_last_error(None)
+    arr = (ctypes.c_void_p * 2)(None, None)
+    assert L.gpe_group_create(arr, 2, ctypes.byref(g)) == 1
+    assert b"null member" in L.gpe_group_last_error(None)
+    # per-context hooks refuse a null context
+    assert L.gpe_gpu_set_wait_limit(None, 1000) == 1
+    assert L.gpe_gpu_test_stall(None, 0) == 1
+    assert L.gpe_gpu_step_series(None, 1, None, None) == 1
+    # fd_match needs order 4 and 0 < r < 1.5, checked before any device call
+    p = _lib.GpeParamsC()
+    L.gpe_gpu_default_params(ctypes.byref(p), 16, 16, 16)
+    p.order, p.fd_match = 2, 0.5
+    h = ctypes.c_void_p()
+    assert L.gpe_gpu_create(ctypes.byref(p), ctypes.byref(h)) == 1
+    assert b"fd_match" in L.gpe_gpu_last_error(None)
+    p.order, p.fd_match = 4, 2.0
+    assert L.gpe_gpu_create(ctypes.byref(p), ctypes.byref(h)) == 1

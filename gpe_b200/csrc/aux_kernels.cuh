@@ -127,7 +127,6 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
                                 double* __restrict__ series,
                                 int* __restrict__ counter) {
   __shared__ double s[1024];
-  pdl_wait();
   double a = 0.0;
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
     const double v = partials[2 * (size_t)b + slot];
@@ -169,7 +168,6 @@ struct DevTime {
 
 // Sets the while node's condition (when it is one) and starts a step.
 __global__ void rk45_begin_kernel(DevTime* T, cudaGraphConditionalHandle h, int use_cond) {
-  pdl_wait();
   if (threadIdx.x != 0) return;
   T->attempts = 0;
   T->dt0_r = T->dt_r;
@@ -189,7 +187,6 @@ __global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
                                     double* __restrict__ s_norm, double* __restrict__ s_dt,
                                     int* __restrict__ s_att, int cap,
                                     cudaGraphConditionalHandle h, int use_cond) {
-  pdl_wait();
   if (threadIdx.x != 0) return;
   const double safety = 0.9, dt_decrease = -0.25, dt_increase = -0.20;
   if (T->halt) {
@@ -255,7 +252,6 @@ __global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
 // for op 1) and write the result back to every member.
 __global__ void combine_scalars_kernel(double* const* __restrict__ scal, int n, int idx,
                                        int op) {
-  pdl_wait();
   if (threadIdx.x != 0) return;
   double a = scal[0][idx];
   for (int m = 1; m < n; m++) {

@@ -539,28 +539,6 @@ KernelFn pick_kernel(int ns, int np, int nout, int epi, int am, int bm) {
   return nullptr;
 }
 
-// Launches with programmatic stream serialisation: the kernel may start
-// while the previous one in the stream finishes (its blocks signal
-// pdl_launch_dependents when they are done with field data), and waits in
-// pdl_wait() for that kernel to complete before touching any of its
-// results.  Only kernels that begin with pdl_wait() are launched this way.
-constexpr bool kProgrammaticLaunch = true;
-
-cudaError_t launch_pdl(const void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                       void** args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = kProgrammaticLaunch ? 1 : 0;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelExC(&cfg, fn, args);
-}
-
 cudaEvent_t pool_event(gpe_ctx* c) {
   if (!c->ev_pool.empty()) {
     cudaEvent_t e = c->ev_pool.back();
@@ -769,7 +747,7 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
     L.sites = (int64_t)c->nint;
     cudaEventRecord(L.a, c->stream);
   }
-  CU_CHECK(c, launch_pdl(fn, grid, block, sh.smem, c->stream, args));
+  CU_CHECK(c, cudaLaunchKernel(fn, grid, block, args, sh.smem, c->stream));
   if (c->timing) {
     cudaEventRecord(L.b, c->stream);
     c->timed.push_back(L);
@@ -895,15 +873,10 @@ int finalize_one(gpe_ctx* c, int nblk, int slot, int op, double scale,
                  int out_index, bool series) {
   Launch L{};
   begin_timed(c, L, GPE_FAM_REDUCE, 0);
-  {
-    const double* partials = c->d_partials;
-    double* outp = c->d_scal + out_index;
-    double* ser = series ? c->d_series : nullptr;
-    int* counter = c->d_counter;
-    void* args[] = {&partials, &nblk, &slot, &op, &scale, &outp, &ser, &counter};
-    CU_CHECK(c, launch_pdl(reinterpret_cast<const void*>(&finalize_kernel), dim3(1), dim3(1024), 0,
-                           c->stream, args));
-  }
+  finalize_kernel<<<1, 1024, 0, c->stream>>>(
+      c->d_partials, nblk, slot, op, scale, c->d_scal + out_index,
+      series ? c->d_series : nullptr, c->d_counter);
+  CU_CHECK(c, cudaGetLastError());
   end_timed(c, L);
   c->launches++;
   return allreduce_scalars(c, out_index, 1, op);
@@ -1187,16 +1160,9 @@ int rk45_attempt(gpe_ctx* c, cudaGraphConditionalHandle h, int use_cond) {
   const double* dyn = reinterpret_cast<const double*>(T);  // dt_r, dt_i, dt0_r, dt0_i
   int rc = attempt_rkck(c, cd(1.0, 0.0), cd(1.0, 0.0), dyn);
   if (rc) return rc;
-  {
-    const double* scal = c->d_scal;
-    double* sn = c->d_series;
-    double* sd = c->d_ser_dt;
-    int* sa = c->d_ser_att;
-    int cap = (int)c->series_cap;
-    void* args[] = {&T, &scal, &sn, &sd, &sa, &cap, &h, &use_cond};
-    CU_CHECK(c, launch_pdl(reinterpret_cast<const void*>(&rk45_control_kernel), dim3(1), dim3(32),
-                           0, c->stream, args));
-  }
+  rk45_control_kernel<<<1, 32, 0, c->stream>>>(T, c->d_scal, c->d_series, c->d_ser_dt,
+                                                c->d_ser_att, (int)c->series_cap, h, use_cond);
+  CU_CHECK(c, cudaGetLastError());
   c->launches++;
   return GPE_OK;
 }
@@ -1824,8 +1790,8 @@ int batch_enqueue_step(gpe_batch* b, int par) {
   for (int s = 0; s < 4; s++) {
     auto& S = b->st[par][s];
     void* args[] = {S.params.data()};
-    BCU(b, launch_pdl(S.fn, dim3((unsigned)S.grid), dim3(32, (unsigned)S.sh.TY + 1),
-                      S.sh.smem, b->stream, args));
+    BCU(b, cudaLaunchKernel(S.fn, dim3((unsigned)S.grid), dim3(32, (unsigned)S.sh.TY + 1),
+                            args, S.sh.smem, b->stream));
   }
   batch_finalize_kernel<<<(unsigned)b->runs.size(), 256, 0, b->stream>>>(
       b->d_partials, b->d_item_run, b->nitems, b->d_scale, b->d_norm, b->d_series,

@@ -189,9 +189,6 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
     s_stop = 0;
   }
   __syncthreads();
-  // the previous stage's outputs are this stage's inputs: nothing global is
-  // touched before the grid this one may overlap has completed
-  pdl_wait();
 
   if (ty == TY) {
     // ---------------- producer warp: lane 0 streams the planes -------------
@@ -655,8 +652,6 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   }  // items
   }  // compute warps
 
-  // this block reads and writes no more field data: the next grid may launch
-  pdl_launch_dependents();
   __syncthreads();
   // After a timed-out wait, let the copies already in flight land (bounded)
   // before the CTA's shared memory is released: the last load issued into

@@ -6,10 +6,15 @@ grid, h = 0.5, 4th-order centred differences, RK4 with dt = 0.005, equation 4
 (g = mu = 1, no trap), complex64 psi with Kahan-compensated accumulation and
 FP64 norm reduction every step; seeded random-phase initial condition
 (|k| <= 1.0, unit amplitudes, uniform phases, rescaled to mean density 1).
-Metric: site-updates/s (sites x steps / device time), whole job.
+Metric: site-updates/s (sites x steps / device time), whole job.  On one
+GPU the same line then carries, under "configs", the short results of the
+other workloads measured after it (--workload rkf45, ensemble and learned at
+reduced step counts; --no-others skips them).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
   python bench.py --workload ensemble [--steps 500]
+  python bench.py --workload rkf45 [--t-end 20]
+  python bench.py --workload learned [--steps 200]
   python bench.py --workload spectrum [--grid 512] [--steps 20]
 
 --workload ensemble: 64 independent complex64 runs, cubic grids drawn from
@@ -253,7 +258,12 @@ def ensemble_members(seed=0):
 
 
 def run_ensemble(args):
-    """The batched-ensemble workload: one JSON line."""
+    print(json.dumps(measure_ensemble(args)), flush=True)
+    return 0
+
+
+def measure_ensemble(args):
+    """The batched-ensemble workload (config C4): its JSON line as a dict."""
     import numpy as np
     import torch
 
@@ -359,11 +369,15 @@ def run_ensemble(args):
         "clocks": clocks, "gpu_launches": int(launches),
         "final_norm_min": float(norms[:, -1].min()), "final_norm_max": float(norms[:, -1].max()),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_learned(args):
+    print(json.dumps(measure_learned(args)), flush=True)
+    return 0
+
+
+def measure_learned(args):
     """Time to t = 50 of the learned coarse path (128^3 complex64 + Kahan RK4
     at the coarse step the network was trained for, network correction after
     every step) against the plain fine path (256^3, h = 0.25, complex64 +
@@ -468,8 +482,7 @@ def run_learned(args):
         "gpu_launches_per_apply": launches_per_apply,
         "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def c2_params(precision, kahan):
@@ -493,6 +506,11 @@ def c2_initial_state():
 
 
 def run_rkf45(args):
+    print(json.dumps(measure_rkf45(args)), flush=True)
+    return 0
+
+
+def measure_rkf45(args):
     """C2: 128^3 reflective, 4th order, adaptive rkf45 (tolerance 1e-6, initial
     dt 0.005) to t = 20, complex128 and complex64 + Kahan.  An untimed pass
     counts the accepted steps the reference loop takes (while t + im_t <=
@@ -574,8 +592,7 @@ def run_rkf45(args):
         "note": "step control on the device: each step is one CUDA graph (conditional WHILE "
                 "node around the attempt); the whole run is one advance call",
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def spectrum_cpu_sample(n: int = 128, min_seconds: float = 10.0, max_calls: int = 20):
@@ -735,6 +752,37 @@ def run_spectrum(args):
     return 0
 
 
+def measure_others(args):
+    """C2, C4 and C5 in short form for the default line: each one's metric,
+    value, roofline and end-to-end figures from a run of its own workload
+    (rkf45 to t = 20; 200 ensemble steps; 200 learned and fine steps)."""
+    import torch
+
+    def short(line, keep):
+        out = {k: line[k] for k in ("metric", "value", "unit", "ms_per_step", "higher_is_better",
+                                    "config", "roofline", "clocks") if k in line}
+        out.update({k: line[k] for k in keep if k in line})
+        return out
+
+    res = {}
+    ns = argparse.Namespace(t_end=20.0, warmup=3)
+    res["c2_rkf45"] = short(measure_rkf45(ns), ("runs", "density_rel_l2_f32_vs_f64",
+                                                 "gpu_launches"))
+    torch.cuda.empty_cache()
+    ns = argparse.Namespace(steps=200, warmup=5)
+    ens = measure_ensemble(ns)
+    ens["launch"] = {k: v for k, v in ens["launch"].items() if k != "table_ms"}
+    res["c4_ensemble"] = short(ens, ("sequential", "speedup_vs_sequential", "e2e", "launch",
+                                     "gpu_launches"))
+    torch.cuda.empty_cache()
+    ns = argparse.Namespace(steps=200, warmup=5)
+    res["c5_learned"] = short(measure_learned(ns), (
+        "fine_ms_per_step", "coarse_ms_per_step", "network_ms_per_apply", "learned_ms_per_step",
+        "time_to_t50_s", "gpu_launches_per_apply"))
+    torch.cuda.empty_cache()
+    return res
+
+
 def workload_config(ngpus, n=N_GRID, storage="complex64+kahan"):
     form = ("complex64 psi + Kahan compensation" if storage == "complex64+kahan"
             else "complex128 psi (the reference's FP64 path)")
@@ -756,6 +804,8 @@ def main():
     ap.add_argument("--impl", default="gpe_b200", choices=["gpe_b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-others", action="store_true",
+                    help="default workload: skip the C2 / C4 / C5 measurements that follow C3")
     ap.add_argument("--grid", type=int, default=N_GRID,
                     help="cube edge (default 512; smaller sizes are for profiling captures)")
     ap.add_argument("--workload", default="cube",
@@ -862,8 +912,10 @@ def main():
     dominant = max(("stage_first", "stage_mid", "stage_last"), key=lambda f: fam[f]["ms"])
     d = fam[dominant]
     per_launch_ms = d["ms"] / max(d["launches"], 1)
-    alg_bytes = BYTES_PER_FAMILY[dominant] * sites
-    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    # bytes from the sites the family's launches covered (a slab's stage is
+    # two launches when its ghost exchange overlaps the interior planes)
+    alg_bytes = BYTES_PER_FAMILY[dominant] * d["sites"] / max(d["launches"], 1)
+    achieved = BYTES_PER_FAMILY[dominant] * d["sites"] / (d["ms"] / 1e3) / 1e9
     traffic = load_traffic().get(dominant)
     kernel_ms_step = sum(fam[f]["ms"] for f in ("stage_first", "stage_mid", "stage_last",
                                                 "reduce")) / args.steps
@@ -930,6 +982,13 @@ def main():
                     "form": "psi resident; per step gpe_gpu_solver + gpe_gpu_norm (8 B read back)"}
     s.close()
 
+    # the other configurations, measured in the same run on the same GPU after
+    # the C3 timing: adaptive rkf45 to t = 20 (C2), the 64-run ensemble (C4)
+    # and the learned coarse path against the fine path (C5)
+    others = None
+    if world == 1 and not args.no_others:
+        others = measure_others(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -955,6 +1014,8 @@ def main():
             "gpu_launches_per_step": launches / args.steps,
             "final_norm": float(norms[-1]) if len(norms) else None,
         }
+        if others is not None:
+            line["configs"] = others
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

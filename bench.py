@@ -268,7 +268,8 @@ def measure_ensemble(args):
     import torch
 
     from gpe_b200 import GpeBatch, GpeSolver
-    from gpe_b200.autotune import time_steps, tune
+    from gpe_b200.autotune import tune
+    from gpe_b200.batch import BatchOpts
     from gpe_b200.ic import trapped_random_phase
 
     dev = torch.device("cuda", 0)
@@ -279,7 +280,14 @@ def measure_ensemble(args):
             for r, p in enumerate(prms)]
     b = GpeBatch(prms, ENS_DT)
     b.set_states(host)
-    best, table = tune(b, steps=4)
+    if getattr(args, "ens_shape", None):
+        # a fixed launch shape (profiling captures): no tuning pass
+        ty, zc, cp = (int(v) for v in args.ens_shape.split(","))
+        best = BatchOpts(tile_y=ty, zchunk=zc, ctas_per_sm=cp)
+        b.set_opts(best)
+        table = []
+    else:
+        best, table = tune(b, steps=4)
     b.set_states(host)
     b.advance(args.warmup, want_norms=False)
     b.set_states(host)
@@ -811,6 +819,9 @@ def main():
     ap.add_argument("--workload", default="cube",
                     choices=["cube", "ensemble", "learned", "rkf45", "spectrum"])
     ap.add_argument("--t-end", type=float, default=20.0, help="rkf45 workload end time")
+    ap.add_argument("--ens-shape", default=None,
+                    help="ensemble workload: fixed launch shape 'tile_y,zchunk,ctas_per_sm' "
+                         "instead of the autotuner's choice")
     ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
                     help="N > 1: independent 512^3 replicas per GPU (weak scaling), or one "
                          "512^3 grid split into NCCL z-slabs (strong scaling)")

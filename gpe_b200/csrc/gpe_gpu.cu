@@ -185,6 +185,9 @@ struct gpe_ctx {
   // all members on its stream; the context's own stream is kept aside
   gpe_group* group = nullptr;
   cudaStream_t own_stream = nullptr;
+  // the ghost exchange overlapping a stage's interior planes (communicator)
+  cudaStream_t xstream = nullptr;
+  cudaEvent_t xev[2] = {nullptr, nullptr};  // boundary planes done, exchange done
   // rk45 step control on the device: time state, per-step series of the
   // last advance (dt taken, attempts) and one captured step per psi buffer
   gpe::DevTime* d_time = nullptr;
@@ -202,6 +205,8 @@ struct gpe_group {
   std::vector<gpe_ctx*> m;
   int dev = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t xstream = nullptr;           // ghost copies beside the interiors
+  cudaEvent_t xev[2] = {nullptr, nullptr};  // boundary planes done, copies done
   double** d_scal = nullptr;  // the members' d_scal pointers (device array)
   std::string err;
 };
@@ -327,8 +332,9 @@ int get_map(gpe_ctx* c, int field, int kind, int TY, int R,
                                          g_nccl.GetErrorString(r_));         \
   } while (0)
 
-int exchange_ghosts(gpe_ctx* c, int field) {
+int exchange_ghosts(gpe_ctx* c, int field, cudaStream_t st = nullptr) {
   if (!c->comm || !(c->exch_lo || c->exch_hi)) return GPE_OK;
+  if (!st) st = c->stream;
   const size_t plane = (size_t)c->Nx * c->Ny * (size_t)c->es;  // bytes
   unsigned char* f = static_cast<unsigned char*>(c->fld[field]);
   // padded plane index pz = z + 2
@@ -338,10 +344,10 @@ int exchange_ghosts(gpe_ctx* c, int field) {
   unsigned char* ghost_hi = f + (size_t)(c->nz + 2) * plane; // z = nz, nz+1
   const size_t n = 2 * plane;
   NCCL_CHECK(c, g_nccl.GroupStart());
-  if (c->exch_hi) NCCL_CHECK(c, g_nccl.Send(top, n, ncclUint8, c->nbr_hi, c->comm, c->stream));
-  if (c->exch_lo) NCCL_CHECK(c, g_nccl.Send(bottom, n, ncclUint8, c->nbr_lo, c->comm, c->stream));
-  if (c->exch_lo) NCCL_CHECK(c, g_nccl.Recv(ghost_lo, n, ncclUint8, c->nbr_lo, c->comm, c->stream));
-  if (c->exch_hi) NCCL_CHECK(c, g_nccl.Recv(ghost_hi, n, ncclUint8, c->nbr_hi, c->comm, c->stream));
+  if (c->exch_hi) NCCL_CHECK(c, g_nccl.Send(top, n, ncclUint8, c->nbr_hi, c->comm, st));
+  if (c->exch_lo) NCCL_CHECK(c, g_nccl.Send(bottom, n, ncclUint8, c->nbr_lo, c->comm, st));
+  if (c->exch_lo) NCCL_CHECK(c, g_nccl.Recv(ghost_lo, n, ncclUint8, c->nbr_lo, c->comm, st));
+  if (c->exch_hi) NCCL_CHECK(c, g_nccl.Recv(ghost_hi, n, ncclUint8, c->nbr_hi, c->comm, st));
   NCCL_CHECK(c, g_nccl.GroupEnd());
   return GPE_OK;
 }
@@ -708,8 +714,12 @@ KernelFn select_kernel(int R, bool kfull, const StageSpec& sp, int am, int bm) {
                : pick_kernel<TS, TC, 2, false, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
 }
 
+// part 0: the whole slab; part 1: its boundary planes z = 0, 1 and nz-2,
+// nz-1 (the planes the z-neighbours' ghosts take); part 2: the planes
+// between them.  Parts 1 and 2 write their per-CTA partials one after the
+// other, so a finalize after part 2 reduces both.
 template <typename TS, typename TC>
-int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
+int launch_stage_t(gpe_ctx* c, const StageSpec& sp, int part) {
   const int R = c->prm.order / 2;
   const RhsForm f = rhs_form(c);
   const bool special = (sp.epi & (EPI_LAP | EPI_ENERGY)) != 0;
@@ -730,11 +740,26 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
   fill_common<TS, TC>(sp, fold, sh, &p);
   p.wait_limit_ns = c->wait_limit_ns;
   p.stall_plane = c->stall_plane;
-  p.partials = c->d_partials;
   p.status = c->d_status;
-  const size_t nblk = (size_t)sh.ntx * sh.nty * sh.nchunks;
-  if (nblk > c->partials_cap)
+  int nchunks = sh.nchunks, planes = c->nz;
+  size_t first_blk = 0;
+  p.zr[0] = 0; p.zr[1] = c->nz; p.zr[2] = p.zr[3] = 0;
+  if (part == 1) {
+    p.run.zchunk = 2;
+    p.zr[1] = 2; p.zr[2] = c->nz - 2; p.zr[3] = c->nz;
+    nchunks = 2;
+    planes = 4;
+  } else if (part == 2) {
+    p.zr[0] = 2; p.zr[1] = c->nz - 2;
+    planes = c->nz - 4;
+    nchunks = (planes + sh.zchunk - 1) / sh.zchunk;
+    first_blk = (size_t)c->last_nblk;
+  }
+  p.nch_a = part == 1 ? 1 : nchunks;
+  const size_t nblk = (size_t)sh.ntx * sh.nty * nchunks;
+  if (first_blk + nblk > c->partials_cap)
     return fail(c, GPE_ERR_INVALID, "partials buffer too small");
+  p.partials = c->d_partials + 2 * first_blk;
   p.nitems = (int)nblk;
   dim3 grid((unsigned)nblk, 1, 1);
   dim3 block(32, (unsigned)sh.TY + 1, 1);
@@ -744,7 +769,7 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
     L.family = sp.family;
     L.a = pool_event(c);
     L.b = pool_event(c);
-    L.sites = (int64_t)c->nint;
+    L.sites = (int64_t)c->nx * c->ny * planes;
     cudaEventRecord(L.a, c->stream);
   }
   CU_CHECK(c, cudaLaunchKernel(fn, grid, block, args, sh.smem, c->stream));
@@ -753,7 +778,7 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
     c->timed.push_back(L);
   }
   c->launches++;
-  c->last_nblk = (int)nblk;
+  c->last_nblk = (int)(first_blk + nblk);
   return GPE_OK;
 }
 
@@ -761,20 +786,21 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp) {
 
 namespace {
 
-int launch_stage_one(gpe_ctx* c, const StageSpec& sp) {
+int launch_stage_one(gpe_ctx* c, const StageSpec& sp, int part = 0) {
   if (sp.epi & EPI_ENERGY) {
-    if (c->es == 8) return launch_stage_t<float, double>(c, sp);
-    return launch_stage_t<double, double>(c, sp);
+    if (c->es == 8) return launch_stage_t<float, double>(c, sp, part);
+    return launch_stage_t<double, double>(c, sp, part);
   }
-  if (c->es == 8) return launch_stage_t<float, float>(c, sp);
-  return launch_stage_t<double, double>(c, sp);
+  if (c->es == 8) return launch_stage_t<float, float>(c, sp, part);
+  return launch_stage_t<double, double>(c, sp, part);
 }
 
 // Copies of the two boundary planes of `field` into the z-neighbours' ghost
 // planes for every member of a slab group (the in-process form of
 // exchange_ghosts: the same planes, moved by cudaMemcpyAsync on the group's
 // stream after every member's kernel of the stage).
-int group_exchange(gpe_group* g, int field) {
+int group_exchange(gpe_group* g, int field, cudaStream_t st = nullptr) {
+  if (!st) st = g->stream;
   const int n = (int)g->m.size();
   for (int r = 0; r < n; r++) {
     gpe_ctx* c = g->m[r];
@@ -784,16 +810,46 @@ int group_exchange(gpe_group* g, int field) {
       const gpe_ctx* lo = g->m[c->nbr_lo];
       const unsigned char* src = static_cast<const unsigned char*>(lo->fld[field]) +
                                  (size_t)lo->nz * plane;  // its z = nz-2, nz-1
-      CU_CHECK(c, cudaMemcpyAsync(f, src, 2 * plane, cudaMemcpyDeviceToDevice, g->stream));
+      CU_CHECK(c, cudaMemcpyAsync(f, src, 2 * plane, cudaMemcpyDeviceToDevice, st));
     }
     if (c->exch_hi) {
       const gpe_ctx* hi = g->m[c->nbr_hi];
       const unsigned char* src = static_cast<const unsigned char*>(hi->fld[field]) +
                                  2 * plane;  // its z = 0, 1
       CU_CHECK(c, cudaMemcpyAsync(f + (size_t)(c->nz + 2) * plane, src, 2 * plane,
-                                  cudaMemcpyDeviceToDevice, g->stream));
+                                  cudaMemcpyDeviceToDevice, st));
     }
   }
+  return GPE_OK;
+}
+
+// The boundary planes go first when a stage's ghosts cross to a neighbour
+// and the slab is deep enough: the exchange then runs on the side stream
+// while the interior planes are computed, and the next stage waits for it.
+// Not inside a stream capture (the rk45 step graphs keep one stream).
+bool split_stage(const gpe_ctx* c) {
+  if (c->nz < 8) return false;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return cs == cudaStreamCaptureStatusNone;
+}
+
+// Side stream and the two events of the split form, made on first use.
+int ensure_side(gpe_ctx* c, cudaStream_t* xs, cudaEvent_t* ev) {
+  if (!*xs && cudaStreamCreateWithFlags(xs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    *xs = nullptr;
+    return fail(c, GPE_ERR_CUDA, "side stream creation failed");
+  }
+  for (int k = 0; k < 2; k++)
+    if (!ev[k] && cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      ev[k] = nullptr;
+      return fail(c, GPE_ERR_CUDA, "event creation failed");
+    }
   return GPE_OK;
 }
 
@@ -801,25 +857,59 @@ int group_exchange(gpe_group* g, int field) {
 // followed by the group's ghost exchange; the z ghosts of a context with a
 // communicator go to its neighbours through NCCL.
 int launch_stage(gpe_ctx* c, const StageSpec& sp) {
+  bool ghosts = false;
+  for (int o = 0; o < sp.nout; o++) ghosts = ghosts || (sp.ghost_mask & (1 << o));
   if (c->group) {
-    for (gpe_ctx* m : c->group->m) {
-      const int rc = launch_stage_one(m, sp);
+    gpe_group* g = c->group;
+    bool split = ghosts;
+    for (gpe_ctx* m : g->m) split = split && split_stage(m);
+    if (split) {
+      const int rc = ensure_side(c, &g->xstream, g->xev);
+      if (rc) return rc;
+    }
+    for (gpe_ctx* m : g->m) {
+      const int rc = launch_stage_one(m, sp, split ? 1 : 0);
       if (rc) return fail(c, rc, m->err);
+    }
+    if (split) {
+      CU_CHECK(c, cudaEventRecord(g->xev[0], g->stream));
+      CU_CHECK(c, cudaStreamWaitEvent(g->xstream, g->xev[0], 0));
     }
     for (int o = 0; o < sp.nout; o++)
       if (sp.ghost_mask & (1 << o)) {
-        const int rc = group_exchange(c->group, sp.out[o]);
+        const int rc = group_exchange(g, sp.out[o], split ? g->xstream : g->stream);
         if (rc) return rc;
       }
+    if (split) {
+      CU_CHECK(c, cudaEventRecord(g->xev[1], g->xstream));
+      for (gpe_ctx* m : g->m) {
+        const int rc = launch_stage_one(m, sp, 2);
+        if (rc) return fail(c, rc, m->err);
+      }
+      CU_CHECK(c, cudaStreamWaitEvent(g->stream, g->xev[1], 0));
+    }
     return GPE_OK;
   }
-  int rc = launch_stage_one(c, sp);
+  const bool split = ghosts && c->comm && (c->exch_lo || c->exch_hi) && split_stage(c);
+  int rc = split ? ensure_side(c, &c->xstream, c->xev) : GPE_OK;
   if (rc) return rc;
+  rc = launch_stage_one(c, sp, split ? 1 : 0);
+  if (rc) return rc;
+  if (split) {
+    CU_CHECK(c, cudaEventRecord(c->xev[0], c->stream));
+    CU_CHECK(c, cudaStreamWaitEvent(c->xstream, c->xev[0], 0));
+  }
   for (int o = 0; o < sp.nout; o++)
     if (sp.ghost_mask & (1 << o)) {
-      rc = exchange_ghosts(c, sp.out[o]);
+      rc = exchange_ghosts(c, sp.out[o], split ? c->xstream : c->stream);
       if (rc) return rc;
     }
+  if (split) {
+    CU_CHECK(c, cudaEventRecord(c->xev[1], c->xstream));
+    rc = launch_stage_one(c, sp, 2);
+    if (rc) return rc;
+    CU_CHECK(c, cudaStreamWaitEvent(c->stream, c->xev[1], 0));
+  }
   return GPE_OK;
 }
 
@@ -2070,6 +2160,12 @@ void gpe_gpu_destroy(gpe_ctx* c) {
     cudaEventDestroy(L.b);
   }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->xstream) {
+    cudaStreamSynchronize(c->xstream);
+    cudaStreamDestroy(c->xstream);
+  }
+  for (auto e : c->xev)
+    if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -2661,6 +2757,12 @@ void gpe_group_destroy(gpe_group* g) {
     rk45_drop_graphs(c);
   }
   if (g->d_scal) cudaFree(g->d_scal);
+  if (g->xstream) {
+    cudaStreamSynchronize(g->xstream);
+    cudaStreamDestroy(g->xstream);
+  }
+  for (auto e : g->xev)
+    if (e) cudaEventDestroy(e);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }

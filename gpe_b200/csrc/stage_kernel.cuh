@@ -107,6 +107,9 @@ struct StageParams {
   const RunDesc<TS, TC>* runs;   // batched launch: per-run descriptors
   const WorkItem* items;         // batched launch: the work list
   int nitems;
+  // single-run launch: planes [zr[0], zr[1]) in nch_a chunks, then planes
+  // [zr[2], zr[3]) (a slab's boundary planes, or its interior, alone)
+  int zr[4], nch_a;
   int TY, stages;
   unsigned int halo_box_bytes, pt_box_bytes;    // bytes one TMA box delivers
   unsigned int halo_smem_bytes, pt_smem_bytes;  // 128-aligned slot strides
@@ -161,10 +164,12 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   // item it -> run descriptor, tile and z range
   auto item_of = [&](int it) -> WorkItem {
     if (BATCH) return p.items[it];
+    // the chunks of the launch's first z range, then those of its second
     const int ntiles = p.run.ntx * p.run.nty;
     const int ch = it / ntiles;
-    const int z0 = ch * p.run.zchunk;
-    return WorkItem{0, it - ch * ntiles, z0, min(z0 + p.run.zchunk, p.run.nz)};
+    const bool first = ch < p.nch_a;
+    const int z0 = (first ? p.zr[0] : p.zr[2]) + (first ? ch : ch - p.nch_a) * p.run.zchunk;
+    return WorkItem{0, it - ch * ntiles, z0, min(z0 + p.run.zchunk, first ? p.zr[1] : p.zr[3])};
   };
   auto run_of = [&](const WorkItem& w) -> const RD& {
     if (BATCH) return p.runs[w.run];

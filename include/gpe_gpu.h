@@ -343,9 +343,12 @@ int gpe_gpu_set_slab(gpe_ctx* ctx, int32_t nz_global, int32_t z_offset);
 int gpe_gpu_comm_unique_id(void* id128);
 /* Join the ranks' NCCL communicator (rank r owns the r-th slab from the
  * bottom).  From then on every kernel that writes a stencil field is
- * followed, on the context's stream, by a send of its two boundary planes
- * into the z-neighbours' ghost planes, and every norm / energy / rk45 error
- * reduction by an all-reduce, so all ranks take the same rk45 decision. */
+ * followed by a send of its two boundary planes into the z-neighbours' ghost
+ * planes, and every norm / energy / rk45 error reduction by an all-reduce,
+ * so all ranks take the same rk45 decision.  On a slab of 8 planes or more
+ * the stage computes its boundary planes first and the send runs on a side
+ * stream while the interior planes are computed; the context's stream waits
+ * for it before the next stage. */
 int gpe_gpu_comm_init(gpe_ctx* ctx, const void* id128, int32_t rank,
                       int32_t nranks);
 
@@ -362,8 +365,9 @@ int gpe_gpu_comm_init(gpe_ctx* ctx, const void* id128, int32_t rank,
  * from z = 0, covering the global axis), stepped together as the reference
  * steps its MPI ranks (src/variables.f90:98-358, src/solve.f90:189): every
  * stage runs on every member, then each member's two boundary planes go to
- * its neighbours' ghost planes (cudaMemcpyAsync on the group's stream, the
- * same planes the NCCL path sends), and the norm, energy and rk45 error are
+ * its neighbours' ghost planes (cudaMemcpyAsync, the same planes the NCCL
+ * path sends; on a side stream beside the interior planes when every slab
+ * has 8 planes or more), and the norm, energy and rk45 error are
  * combined across members (sum / max) so every member takes the same rk45
  * decision.  Members keep their own fields and tables; while grouped they run
  * on the group's stream and the per-context step / reduce entry points

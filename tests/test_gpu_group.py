@@ -28,7 +28,10 @@ def _prm(scheme, bcs, order, precision=16, kahan=False, **kw):
                      g=1.2, mu=0.8, **kw)
 
 
-@pytest.mark.parametrize("nslabs", [2, 3])
+# 2 and 3 slabs (12-19 planes): every stage computes the boundary planes
+# first and copies them on a side stream while the interior planes run;
+# 5 slabs (7-8 planes): slabs under 8 planes step in one launch per stage
+@pytest.mark.parametrize("nslabs", [2, 3, 5])
 @pytest.mark.parametrize("bcs", [1, 2])
 @pytest.mark.parametrize("scheme,order", [("rk4", 4), ("rk45", 4), ("rk2", 2), ("euler", 4)])
 def test_group_matches_single_domain_and_oracle(nslabs, bcs, scheme, order):
@@ -74,6 +77,34 @@ def test_group_complex64_kahan_is_bitwise_single_domain(bcs):
             g.solver()
             s.solver()
         assert np.array_equal(g.get_global_state(np.complex64), s.get_state(np.complex64))
+
+
+@pytest.mark.parametrize("nslabs", [2, 5])
+def test_group_stage_launches_boundary_planes_apart_when_slabs_are_deep(nslabs):
+    """Slabs of 8 planes or more: each stage is two launches per slab (the
+    four boundary planes, then the interior) with the ghost copies between
+    them on a side stream; one slab under 8 planes keeps the whole group at
+    one launch per stage.  Either way every plane is computed once."""
+    prm = _prm("rk4", 1, 4)
+    psi = random_field((N[2], N[1], N[0]), seed=3)
+    with SlabGroup(prm, nslabs, dt=0.02) as g, GpeSolver(prm, dt=0.02) as s:
+        g.set_global_state(psi)
+        s.set_state(psi)
+        for m in g.members:
+            m.set_timing(True)
+            m.timing()
+        g.solver()
+        s.solver()
+        deep = all(pl.nz >= 8 for pl in g.plans)
+        assert deep == (nslabs == 2)
+        for m, pl in zip(g.members, g.plans):
+            fam = m.timing()
+            for f in ("stage_first", "stage_mid", "stage_last"):
+                per_stage = 2 if f == "stage_mid" else 1
+                assert fam[f]["launches"] == per_stage * (2 if deep else 1), (f, pl.nz)
+                assert fam[f]["sites"] == per_stage * N[0] * N[1] * pl.nz
+            m.set_timing(False)
+        assert np.array_equal(g.get_global_state(), s.get_state())
 
 
 def test_group_members_refuse_stepping_alone():

@@ -488,21 +488,23 @@ constexpr bool occ3_recipe(int np, bool full, bool batch) {
 
 // The entry of one recipe (only that one is instantiated).
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AM, int BM,
-          bool FULL, bool BATCH>
+          int FORM, bool BATCH>
 KernelFn kernel_for() {
-  if constexpr (occ3_recipe<TS, TC>(NP, FULL, BATCH))
+  if constexpr (occ3_recipe<TS, TC>(NP, FORM == FORM_FULL, BATCH))
     return reinterpret_cast<KernelFn>(
-        &stage_kernel_occ3<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FULL, BATCH>);
+        &stage_kernel_occ3<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FORM, BATCH>);
   else
     return reinterpret_cast<KernelFn>(
-        &stage_kernel<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FULL, BATCH>);
+        &stage_kernel<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FORM, BATCH>);
 }
 
-template <typename TS, typename TC, int R, bool FULL, bool BATCH>
+// FORM_TRAP recipes exist for rk4 only; the other schemes step a trap with
+// the FORM_FULL recipes (nullptr here, and the caller falls back).
+template <typename TS, typename TC, int R, int FORM, bool BATCH>
 KernelFn pick_kernel(int ns, int np, int nout, int epi, int am, int bm) {
 #define GPE_CASE(NS_, NP_, NOUT_, EPI_, AM_, BM_)                                      \
   if (ns == NS_ && np == NP_ && nout == NOUT_ && epi == (EPI_) && am == AM_ && bm == BM_) \
-    return kernel_for<TS, TC, R, NS_, NP_, NOUT_, (EPI_), AM_, BM_, FULL, BATCH>();
+    return kernel_for<TS, TC, R, NS_, NP_, NOUT_, (EPI_), AM_, BM_, FORM, BATCH>();
   if constexpr (BATCH) {
     // batched ensembles step with rk4
     if constexpr (std::is_same<TS, TC>::value) {
@@ -513,8 +515,17 @@ KernelFn pick_kernel(int ns, int np, int nout, int epi, int am, int bm) {
         GPE_CASE(2, 3, 2, EPI_KAHAN | EPI_NORM, 4, 0x3)   // rk4 stage 4 (compensated)
       }
     }
+  } else if constexpr (FORM == FORM_TRAP) {
+    if constexpr (std::is_same<TS, TC>::value) {
+      GPE_CASE(1, 0, 1, 0, 0, 0)                   // rk4 stage 1, get_rhs
+      GPE_CASE(2, 0, 1, 0, 0, 0)                   // rk4 stages 2, 3
+      GPE_CASE(2, 2, 1, EPI_NORM, 5, 0x3)          // rk4 stage 4
+      if constexpr (std::is_same<TS, float>::value) {
+        GPE_CASE(2, 3, 2, EPI_KAHAN | EPI_NORM, 4, 0x3)   // rk4 stage 4 (compensated)
+      }
+    }
   } else {
-  if constexpr (std::is_same<TC, double>::value && !FULL) {
+  if constexpr (std::is_same<TC, double>::value && FORM == FORM_PLAIN) {
     GPE_CASE(1, 0, 0, EPI_ENERGY, 0, 0)
   }
   if constexpr (std::is_same<TS, TC>::value) {
@@ -530,7 +541,7 @@ KernelFn pick_kernel(int ns, int np, int nout, int epi, int am, int bm) {
     GPE_CASE(1, 4, 2, 0, 0, 0xF00)               // rkck stage 4
     GPE_CASE(1, 5, 2, 0, 0, 0x1F00)              // rkck stage 5
     GPE_CASE(1, 5, 1, EPI_NORM | EPI_ERR, 0, 0xF)  // rkck stage 6
-    if constexpr (!FULL) {
+    if constexpr (FORM == FORM_PLAIN) {
       GPE_CASE(1, 0, 1, EPI_LAP, 0, 0)           // laplacian
     }
     if constexpr (std::is_same<TS, float>::value) {
@@ -585,20 +596,26 @@ void fill_rhs_coeffs(const gpe_ctx* c, double& ar0, double& ard, double& ai,
 }
 
 // The right-hand side coefficients of a context, in the form the kernels
-// take: for the plain right-hand side (no trap, sponge, gradient or sphere)
-// f = i*ai*(cL*L + (c0 + cn|u|^2)u); the kernel forms K = ai*(...) and the
-// factor i moves into the output coefficients (`fold`).
+// take: without sponge, gradient or sphere terms
+// f = i*ai*(cL*L + (c0 + cV*V + cn|u|^2)u); the kernel forms K = ai*(...) and
+// the factor i moves into the output coefficients (`fold`), with the trap
+// (`trap`, FORM_TRAP recipes) or without it.
 struct RhsForm {
   double ar0, ard, ai, cL, c0, cV, cn, U;
   int ud, uv, us, ug;
-  bool full;
+  bool full, trap;
 };
 
 RhsForm rhs_form(const gpe_ctx* c) {
   RhsForm f;
   fill_rhs_coeffs(c, f.ar0, f.ard, f.ai, f.cL, f.c0, f.cV, f.cn, f.U, f.ud, f.uv, f.us, f.ug);
-  f.full = f.ud || f.uv || f.us || f.ug;
+  f.full = f.ud || f.us || f.ug;
+  f.trap = f.uv && !f.full;
   return f;
+}
+
+int form_of(const RhsForm& f) {
+  return f.full ? FORM_FULL : f.trap ? FORM_TRAP : FORM_PLAIN;
 }
 
 // Recipe bit masks of a stage (see stage_kernel.cuh).
@@ -655,7 +672,7 @@ int fill_run(gpe_ctx* c, const StageSpec& sp, int R, const LaunchShape& sh,
   else { rd->gx1 = (TC)(8.0 / (12.0 * c->dx)); rd->gx2 = (TC)(-1.0 / (12.0 * c->dx)); }
   const double sc = f.full ? 1.0 : f.ai;
   rd->ar0 = (TC)f.ar0; rd->ard = (TC)f.ard; rd->ai = (TC)f.ai; rd->cL = (TC)(sc * f.cL);
-  rd->c0 = (TC)(sc * f.c0); rd->cV = (TC)f.cV; rd->cn = (TC)(sc * f.cn); rd->U = (TC)f.U;
+  rd->c0 = (TC)(sc * f.c0); rd->cV = (TC)(sc * f.cV); rd->cn = (TC)(sc * f.cn); rd->U = (TC)f.U;
   rd->use_diss = f.ud; rd->use_V = f.uv; rd->use_sphere = f.us; rd->use_grad = f.ug;
   for (int a = 0; a < 3; a++) {
     if (std::is_same<TC, float>::value) {
@@ -704,14 +721,26 @@ void fill_common(const StageSpec& sp, bool fold, const LaunchShape& sh,
   p->stall_plane = -1;
 }
 
-template <typename TS, typename TC, bool BATCH>
-KernelFn select_kernel(int R, bool kfull, const StageSpec& sp, int am, int bm) {
+template <typename TS, typename TC, int R, bool BATCH>
+KernelFn select_form(int form, const StageSpec& sp, int am, int bm) {
   const int ns = sp.stencil2 >= 0 ? 2 : 1;
-  if (R == 1)
-    return kfull ? pick_kernel<TS, TC, 1, true, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm)
-                 : pick_kernel<TS, TC, 1, false, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
-  return kfull ? pick_kernel<TS, TC, 2, true, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm)
-               : pick_kernel<TS, TC, 2, false, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
+  if (form == FORM_FULL)
+    return pick_kernel<TS, TC, R, FORM_FULL, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
+  if (form == FORM_TRAP)
+    return pick_kernel<TS, TC, R, FORM_TRAP, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
+  return pick_kernel<TS, TC, R, FORM_PLAIN, BATCH>(ns, sp.np, sp.nout, sp.epi, am, bm);
+}
+
+// The kernel of a stage in right-hand-side form *form; a trap recipe that
+// has no FORM_TRAP build steps with FORM_FULL (and *form says so).
+template <typename TS, typename TC, bool BATCH>
+KernelFn select_kernel(int R, int* form, const StageSpec& sp, int am, int bm) {
+  for (;;) {
+    KernelFn fn = R == 1 ? select_form<TS, TC, 1, BATCH>(*form, sp, am, bm)
+                         : select_form<TS, TC, 2, BATCH>(*form, sp, am, bm);
+    if (fn || *form != FORM_TRAP) return fn;
+    *form = FORM_FULL;
+  }
 }
 
 // part 0: the whole slab; part 1: its boundary planes z = 0, 1 and nz-2,
@@ -723,19 +752,19 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp, int part) {
   const int R = c->prm.order / 2;
   const RhsForm f = rhs_form(c);
   const bool special = (sp.epi & (EPI_LAP | EPI_ENERGY)) != 0;
-  const bool fold = !f.full && !special;
-  const bool kfull = f.full && !special;
+  int form = special ? FORM_PLAIN : form_of(f);
   int am, bm;
   recipe_masks(sp, &am, &bm);
-  KernelFn fn = select_kernel<TS, TC, false>(R, kfull, sp, am, bm);
+  KernelFn fn = select_kernel<TS, TC, false>(R, &form, sp, am, bm);
   if (!fn) return fail(c, GPE_ERR_INVALID, "no kernel for this stage shape");
+  const bool fold = form != FORM_FULL && !special;
   LaunchShape sh;
   int rc = choose_shape(c, fn, R, sp.np, sp.stencil2 >= 0 ? 2 : 1,
-                        occ3_recipe<TS, TC>(sp.np, kfull, false), &sh);
+                        occ3_recipe<TS, TC>(sp.np, form == FORM_FULL, false), &sh);
   if (rc) return rc;
   StageParams<TS, TC> p;
   memset(&p, 0, sizeof(p));
-  rc = fill_run<TS, TC>(c, sp, R, sh, f, &p.run);
+  rc = fill_run<TS, TC>(c, sp, R, sh, f, &p.run, special ? -1 : (form == FORM_FULL ? 1 : 0));
   if (rc) return rc;
   fill_common<TS, TC>(sp, fold, sh, &p);
   p.wait_limit_ns = c->wait_limit_ns;
@@ -1750,7 +1779,7 @@ struct gpe_batch {
   std::vector<gpe_ctx*> runs;
   gpe_batch_opts opts;
   int es = 8, R = 1;
-  bool full = false;
+  int form = FORM_PLAIN;  // the highest right-hand-side form among the members
   int TY = 8;
   WorkItem* d_items = nullptr;
   int* d_item_run = nullptr;
@@ -1810,7 +1839,8 @@ int batch_prepare_par(gpe_batch* b, cd dt, int par) {
     const StageSpec& sp = sp0[s];
     int am, bm;
     recipe_masks(sp, &am, &bm);
-    KernelFn fn = select_kernel<TS, TC, true>(b->R, b->full, sp, am, bm);
+    int form = b->form;
+    KernelFn fn = select_kernel<TS, TC, true>(b->R, &form, sp, am, bm);
     if (!fn) return bfail(b, GPE_ERR_INVALID, "no batched kernel for this stage");
     LaunchShape sh = ring_shape(b->es, b->R, sp.np, b->TY, sp.stencil2 >= 0 ? 2 : 1);
     BCU(b, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
@@ -1828,14 +1858,15 @@ int batch_prepare_par(gpe_batch* b, cd dt, int par) {
       shr.nty = (c->ny + sh.TY - 1) / sh.TY;
       shr.zchunk = 0;
       shr.nchunks = 0;
-      const int rc = fill_run<TS, TC>(c, spr[s], b->R, shr, rhs_form(c), &rds[r], b->full ? 1 : 0);
+      const int rc = fill_run<TS, TC>(c, spr[s], b->R, shr, rhs_form(c), &rds[r],
+                                      form == FORM_FULL ? 1 : 0);
       if (rc) return bfail(b, rc, c->err);
     }
     BCU(b, cudaMemcpy(b->d_rundesc[par][s], rds.data(), sizeof(RunDesc<TS, TC>) * rds.size(),
                       cudaMemcpyHostToDevice));
     StageParams<TS, TC> p;
     memset(&p, 0, sizeof(p));
-    fill_common<TS, TC>(sp, !b->full, sh, &p);
+    fill_common<TS, TC>(sp, form != FORM_FULL, sh, &p);
     p.runs = static_cast<const RunDesc<TS, TC>*>(b->d_rundesc[par][s]);
     p.items = b->d_items;
     p.nitems = b->nitems;
@@ -2909,7 +2940,7 @@ int gpe_batch_create(const gpe_params* prms, int32_t nruns, const gpe_batch_opts
       return bail(rc);
     }
     b->runs.push_back(c);
-    b->full = b->full || rhs_form(c).full;
+    b->form = std::max(b->form, form_of(rhs_form(c)));
     b->sites += (int64_t)c->nint;
   }
   if (cudaSetDevice(b->dev) != cudaSuccess ||

@@ -35,10 +35,12 @@
 // s0 and s1 are those fields at the site, P_q the pointwise inputs, alpha
 // and beta real Runge-Kutta weights present only where AMASK/BMASK say so,
 // a[o] one complex coefficient per output (it carries dt), and K the
-// right-hand side.  Without trap, sponge, gradient or sphere terms (FULL =
-// false) the right-hand side of every equation is i*B with
-// B = cL*lap(u) + (c0 + cn|u|^2) u, so K = B and the host folds the factor i
-// into a[o]; with FULL = true K = f(u) is formed site by site.
+// right-hand side.  Without sponge, gradient or sphere terms the
+// right-hand side of every equation is i*B with
+// B = cL*lap(u) + (c0 + cV*V + cn|u|^2) u, so K = B and the host folds the
+// factor i into a[o]: FORM_PLAIN without a trap (V = 0), FORM_TRAP with
+// V = Vx[i] + Vy[j] + Vz[k]; with FORM_FULL K = f(u) is formed site by site
+// with every term the equation may have.
 #pragma once
 
 #include <type_traits>
@@ -59,6 +61,9 @@ enum : int {
   EPI_ENERGY = 8,  // no outputs; reduce E (slot 0) and H4 (slot 1)
   EPI_LAP = 16,    // K is the Laplacian itself
 };
+
+// Right-hand-side forms of a recipe (see the top of this file).
+enum : int { FORM_PLAIN = 0, FORM_TRAP = 1, FORM_FULL = 2 };
 
 struct TileMaps {
   CUtensorMap halo;      // stencil field, box (64+4) x (TY+2R) x 1
@@ -146,10 +151,11 @@ using IC = std::integral_constant<int, K>;
 // The kernel body; the __global__ entries below differ only in their
 // register budget.
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
-          int BMASK, bool FULL, bool BATCH>
+          int BMASK, int FORM, bool BATCH>
 __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   using V = typename VT<TC>::T;
   using RD = RunDesc<TS, TC>;
+  constexpr bool FULL = FORM == FORM_FULL, TRAP = FORM == FORM_TRAP;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_abort, s_issued, s_stop;
   __shared__ double s_red[2][32];
@@ -334,7 +340,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   // Per-thread constants of this item.
   TC Vxy[2] = {TC(0), TC(0)}, Dxy[2] = {TC(0), TC(0)};
   double Wxy[2] = {0.0, 0.0};
-  if ((FULL || (EPI & EPI_ENERGY)) && useV) {
+  if (TRAP || ((FULL || (EPI & EPI_ENERGY)) && useV)) {
     Vxy[0] = rd.tabV[0][i0] + rd.tabV[1][j];
     Vxy[1] = rd.tabV[0][i0 + 1] + rd.tabV[1][j];
   }
@@ -441,7 +447,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
       }
       TC Vz = TC(0), Dz = TC(0);
       double Wz = 0.0;
-      if ((FULL || (EPI & EPI_ENERGY)) && useV) Vz = tabVz[z];
+      if (TRAP || ((FULL || (EPI & EPI_ENERGY)) && useV)) Vz = tabVz[z];
       if (FULL && useD) Dz = tabDz[z];
       if (EPI & EPI_NORM) Wz = tabWz[z];
 
@@ -481,7 +487,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
         if (EPI & EPI_LAP) {
           Kv = L;
         } else if (!FULL) {
-          const TC s = fma(cns, a2, c0s);
+          const TC s = TRAP ? fma(cns, a2, fma(cVs, Vxy[e] + Vz, c0s)) : fma(cns, a2, c0s);
           Kv = vfma(vsplat(s), f0, vmul(cLv, L));
         } else {
           const TC Vs = useV ? Vxy[e] + Vz : TC(0);
@@ -674,10 +680,10 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
 
 // Budget left to the compiler (one to two CTAs per SM, by shared memory).
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
-          int BMASK, bool FULL, bool BATCH>
+          int BMASK, int FORM, bool BATCH>
 __global__ void __launch_bounds__(288)
     stage_kernel(const __grid_constant__ StageParams<TS, TC> p) {
-  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FULL, BATCH>(p);
+  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FORM, BATCH>(p);
 }
 
 // Registers capped for three resident CTAs per SM: the complex64 recipes
@@ -685,10 +691,10 @@ __global__ void __launch_bounds__(288)
 // and shared-memory dependencies, so more warps per scheduler hide more of
 // it (their three rings of slots fit in shared memory).
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
-          int BMASK, bool FULL, bool BATCH>
+          int BMASK, int FORM, bool BATCH>
 __global__ void __launch_bounds__(288, 3)
     stage_kernel_occ3(const __grid_constant__ StageParams<TS, TC> p) {
-  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FULL, BATCH>(p);
+  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FORM, BATCH>(p);
 }
 
 }  // namespace gpe

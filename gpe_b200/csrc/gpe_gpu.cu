@@ -113,6 +113,7 @@ bool load_nccl(std::string* why) {
 
 struct LaunchShape {
   int TY, S, zchunk, ntx, nty, nchunks;
+  int rows = 1;  // tile rows per compute warp (rows_per_warp of the recipe)
   size_t smem;
   unsigned halo_box, pt_box, halo_smem, pt_smem;
 };
@@ -444,12 +445,13 @@ int choose_shape(gpe_ctx* c, KernelFn fn, int R, int np, int ns, bool occ3, Laun
   // energy recipe computes in FP64 and is not one of them)
   const int max_ctas = occ3 ? 3 : 2;
   LaunchShape s = ring_shape(c->es, R, np, c->prm.tile_y, ns, max_ctas);
+  s.rows = (occ3 && ns == 2) ? 2 : 1;  // rows_per_warp of the occ3 recipes
   s.ntx = (c->nx + TX - 1) / TX;
   s.nty = (c->ny + s.TY - 1) / s.TY;
   CU_CHECK(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)s.smem));
   int occ = 0;
-  CU_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (s.TY + 1),
+  CU_CHECK(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (s.TY / s.rows + 1),
                                                             s.smem));
   if (occ < 1) return fail(c, GPE_ERR_INVALID, "stage kernel cannot be resident");
   const long slots = (long)occ * c->num_sms;
@@ -490,7 +492,10 @@ constexpr bool occ3_recipe(int np, bool full, bool batch) {
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AM, int BM,
           int FORM, bool BATCH>
 KernelFn kernel_for() {
-  if constexpr (occ3_recipe<TS, TC>(NP, FORM == FORM_FULL, BATCH))
+  if constexpr (rows_per_warp<TS, TC>(NS, NP, FORM, BATCH) == 2)
+    return reinterpret_cast<KernelFn>(
+        &stage_kernel_rows2<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FORM, BATCH>);
+  else if constexpr (occ3_recipe<TS, TC>(NP, FORM == FORM_FULL, BATCH))
     return reinterpret_cast<KernelFn>(
         &stage_kernel_occ3<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FORM, BATCH>);
   else
@@ -791,7 +796,7 @@ int launch_stage_t(gpe_ctx* c, const StageSpec& sp, int part) {
   p.partials = c->d_partials + 2 * first_blk;
   p.nitems = (int)nblk;
   dim3 grid((unsigned)nblk, 1, 1);
-  dim3 block(32, (unsigned)sh.TY + 1, 1);
+  dim3 block(32, (unsigned)(sh.TY / sh.rows) + 1, 1);
   void* args[] = {&p};
   Launch L{};
   if (c->timing) {

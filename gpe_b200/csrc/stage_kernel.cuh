@@ -15,14 +15,15 @@
 //     (src/solve.f90:176-190) or the energy sum (src/variables.f90:563-587).
 //
 // Tiling: a CTA owns a 64 x TY tile in (x, y) and marches a chunk of
-// z-planes.  TY compute warps each own one row (two consecutive x sites per
-// lane); one more warp is the producer: its lane 0 issues, plane by plane,
+// z-planes.  TY / ROWS compute warps each own ROWS adjacent rows (one, or two
+// for the recipes rows_per_warp names; two consecutive x sites per lane);
+// one more warp is the producer: its lane 0 issues, plane by plane,
 // TMA tile loads (no multicast) of the stencil plane with its halo and of the
 // pointwise input tiles into a ring of `stages` shared-memory slots.  A slot
 // is handed over on a "full" mbarrier (TMA transaction count) and handed back
 // on an "empty" mbarrier that every compute warp arrives on once it no longer
 // reads the slot, so no block-wide barrier is taken per plane.  The
-// z-neighbours come from a register queue of 2R+1 planes (R = order/2),
+// z-neighbours come from a register queue of 2R+1 planes per row (R = order/2),
 // rotated by unrolling the plane loop 2R+1 times; x and y neighbours are read
 // from the staged halo plane.  Outputs go straight from registers to global
 // memory as 16-byte stores.
@@ -64,6 +65,23 @@ enum : int {
 
 // Right-hand-side forms of a recipe (see the top of this file).
 enum : int { FORM_PLAIN = 0, FORM_TRAP = 1, FORM_FULL = 2 };
+
+// Rows of the tile each compute warp owns.  Two for the complex64 recipes
+// that stage two stencil fields and nothing else (rk4 stages 2 and 3):
+// their shared-memory loads (both fields at every x and y neighbour) bound
+// them, and a warp with two adjacent rows loads the y-neighbour rows the two
+// share once (rows -2, -1, +2, +3 of its first row for four, each row's own
+// centre serving as the other's nearest neighbour).  Measured at 512^3: the
+// stage 0.655 -> 0.602 ms; the one-field stage 1 lost (0.429 -> 0.443 ms:
+// instruction-bound, and its warps per SM fell from 27 to 15), so it keeps
+// one row per warp.
+template <typename TS, typename TC>
+__host__ __device__ constexpr int rows_per_warp(int ns, int np, int form, bool batch) {
+  return (std::is_same<TS, float>::value && std::is_same<TC, float>::value && ns == 2 &&
+          np == 0 && form != FORM_FULL && !batch)
+             ? 2
+             : 1;
+}
 
 struct TileMaps {
   CUtensorMap halo;      // stencil field, box (64+4) x (TY+2R) x 1
@@ -156,6 +174,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   using V = typename VT<TC>::T;
   using RD = RunDesc<TS, TC>;
   constexpr bool FULL = FORM == FORM_FULL, TRAP = FORM == FORM_TRAP;
+  constexpr int ROWS = rows_per_warp<TS, TC>(NS, NP, FORM, BATCH);
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_abort, s_issued, s_stop;
   __shared__ double s_red[2][32];
@@ -165,6 +184,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   constexpr int QN = 2 * R + 1;             // z-queue length
   constexpr unsigned ES = 2 * sizeof(TS);   // bytes per stored complex
   const int TY = p.TY, S = p.stages;
+  const int NW = TY / ROWS;  // compute warps; warp NW is the producer
   const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
 
   // item it -> run descriptor, tile and z range
@@ -192,7 +212,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   if (tid == 0) {
     for (int s = 0; s < S; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], (uint32_t)TY);
+      mbar_init(&empty[s], (uint32_t)NW);
     }
     fence_mbar_init();
     s_abort = 0;
@@ -201,7 +221,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   }
   __syncthreads();
 
-  if (ty == TY) {
+  if (ty == NW) {
     // ---------------- producer warp: lane 0 streams the planes -------------
     // Planes of successive items follow each other through the ring, so the
     // next item's first planes load while the current item drains.
@@ -268,8 +288,9 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   // ------------------------------ compute warps ------------------------------
   int slot = 0, cslot = 0;
   uint32_t phase = 0;
-  const unsigned row_off = ES * (unsigned)((ty + R) * HW + 2 * lane + 2);
-  const unsigned pt_off = ES * (unsigned)(ty * TX + 2 * lane);
+  // the warp's first row; row rr of the warp sits rr rows further on
+  const unsigned row_off = ES * (unsigned)((ty * ROWS + R) * HW + 2 * lane + 2);
+  const unsigned pt_off = ES * (unsigned)(ty * ROWS * TX + 2 * lane);
   V ar[2], aix[2], alv[2], alv2[2], bev[2][NP > 0 ? NP : 1];
   TC a_re[2] = {p.a_r[0], p.a_r[1]}, a_im[2] = {p.a_i[0], p.a_i[1]};
   double cek_r = p.cek_r, cek_i = p.cek_i, dt0_r = p.dt0_r, dt0_i = p.dt0_i,
@@ -320,9 +341,13 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   const int z0 = w.z0;
   const int niters = (w.z1 - w.z0) + R;
   const int i0 = tile_x * TX + 2 * lane;
-  const int j = tile_y * TY + ty;
-  const bool ok0 = (i0 < nx) && (j < ny);
-  const bool ok1 = (i0 + 1 < nx) && (j < ny);
+  const int j0 = tile_y * TY + ty * ROWS;  // the warp's first row
+  bool ok0[ROWS], ok1[ROWS];
+#pragma unroll
+  for (int rr = 0; rr < ROWS; rr++) {
+    ok0[rr] = (i0 < nx) && (j0 + rr < ny);
+    ok1[rr] = (i0 + 1 < nx) && (j0 + rr < ny);
+  }
   const size_t Nx = (size_t)rd.Nx, NxNy = (size_t)rd.Nx * (size_t)rd.Ny;
   TS* const outp[2] = {rd.out[0], rd.out[1]};
   const TC c0s = rd.c0, cns = rd.cn, cVs = rd.cV, ar0 = rd.ar0, ard = rd.ard, ais = rd.ai;
@@ -337,24 +362,13 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
           c0l = vsplat(rd.c0lap), cLv = vsplat(rd.cL);
   double red0 = 0.0, red1 = 0.0;
 
-  // Per-thread constants of this item.
-  TC Vxy[2] = {TC(0), TC(0)}, Dxy[2] = {TC(0), TC(0)};
-  double Wxy[2] = {0.0, 0.0};
-  if (TRAP || ((FULL || (EPI & EPI_ENERGY)) && useV)) {
-    Vxy[0] = rd.tabV[0][i0] + rd.tabV[1][j];
-    Vxy[1] = rd.tabV[0][i0 + 1] + rd.tabV[1][j];
-  }
-  if (FULL && useD) {
-    Dxy[0] = rd.tabD[0][i0] + rd.tabD[1][j];
-    Dxy[1] = rd.tabD[0][i0 + 1] + rd.tabD[1][j];
-  }
-  if (EPI & EPI_NORM) {
-    Wxy[0] = rd.tabW[0][i0] * rd.tabW[1][j];
-    Wxy[1] = rd.tabW[0][i0 + 1] * rd.tabW[1][j];
-  }
+  // Per-thread constants of this item, per row.
+  TC Vxy[ROWS][2], Dxy[ROWS][2];
+  double Wxy[ROWS][2];
   // Ghost copies this thread's sites feed, as element offsets from the site
-  // (x and y fixed per thread; z per plane, uniform across the CTA).
-  int gxo[2][2], gyo[2];
+  // (x and y fixed per thread and row; z per plane, uniform across the CTA).
+  int gxo[2][2], gyo[ROWS][2];
+  bool edge_xy[ROWS];
   {
     int a, b;
     for (int e = 0; e < 2; e++) {
@@ -362,32 +376,54 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
       gxo[e][0] = (a != NO_GHOST) ? a - (i0 + e) : 0;
       gxo[e][1] = (b != NO_GHOST) ? b - (i0 + e) : 0;
     }
-    ghost_targets(j, ny, bcs, a, b);
-    gyo[0] = (a != NO_GHOST) ? (a - j) * rd.Nx : 0;
-    gyo[1] = (b != NO_GHOST) ? (b - j) * rd.Nx : 0;
-  }
-  const bool edge_xy = (gxo[0][0] | gxo[0][1] | gxo[1][0] | gxo[1][1] | gyo[0] | gyo[1]) != 0;
-  // element offset of this thread's first site in plane z0
-  size_t base = (size_t)(z0 + GH) * NxNy + (size_t)(j + GH) * Nx + (size_t)(i0 + GH);
-
-  // z-queue: physical slot of push number c is c % QN; after push c the
-  // plane d above the one being computed sits in slot (c + 1 + R + d) % QN.
-  CPair<TC> q[QN];
 #pragma unroll
-  for (int w = 0; w < R; w++) {
-    CPair<TC> v = {vsplat(TC(0)), vsplat(TC(0))};
-    if (ok0) {
-      const size_t off = 2 * (base - (size_t)(R - w) * NxNy);
-      v = ld_cpair<TS, TC>(rd.stencil + off);
-      if (NS == 2) {
-        const CPair<TC> v2 = ld_cpair<TS, TC>(rd.stencil2 + off);
-        v = {vadd(v.a, v2.a), vadd(v.b, v2.b)};
+    for (int rr = 0; rr < ROWS; rr++) {
+      const int j = j0 + rr;
+      Vxy[rr][0] = Vxy[rr][1] = Dxy[rr][0] = Dxy[rr][1] = TC(0);
+      Wxy[rr][0] = Wxy[rr][1] = 0.0;
+      if (TRAP || ((FULL || (EPI & EPI_ENERGY)) && useV)) {
+        Vxy[rr][0] = rd.tabV[0][i0] + rd.tabV[1][j];
+        Vxy[rr][1] = rd.tabV[0][i0 + 1] + rd.tabV[1][j];
       }
+      if (FULL && useD) {
+        Dxy[rr][0] = rd.tabD[0][i0] + rd.tabD[1][j];
+        Dxy[rr][1] = rd.tabD[0][i0 + 1] + rd.tabD[1][j];
+      }
+      if (EPI & EPI_NORM) {
+        Wxy[rr][0] = rd.tabW[0][i0] * rd.tabW[1][j];
+        Wxy[rr][1] = rd.tabW[0][i0 + 1] * rd.tabW[1][j];
+      }
+      ghost_targets(j, ny, bcs, a, b);
+      gyo[rr][0] = (a != NO_GHOST) ? (a - j) * rd.Nx : 0;
+      gyo[rr][1] = (b != NO_GHOST) ? (b - j) * rd.Nx : 0;
+      edge_xy[rr] = (gxo[0][0] | gxo[0][1] | gxo[1][0] | gxo[1][1] | gyo[rr][0] | gyo[rr][1]) != 0;
     }
-    q[w] = v;
   }
+  // element offset of this thread's first site (first row) in plane z0
+  size_t base = (size_t)(z0 + GH) * NxNy + (size_t)(j0 + GH) * Nx + (size_t)(i0 + GH);
+
+  // z-queues, one per row: physical slot of push number c is c % QN; after
+  // push c the plane d above the one being computed sits in slot
+  // (c + 1 + R + d) % QN.
+  CPair<TC> q[ROWS][QN];
 #pragma unroll
-  for (int w = R; w < QN; w++) q[w] = {vsplat(TC(0)), vsplat(TC(0))};
+  for (int rr = 0; rr < ROWS; rr++) {
+#pragma unroll
+    for (int w = 0; w < R; w++) {
+      CPair<TC> v = {vsplat(TC(0)), vsplat(TC(0))};
+      if (ok0[rr]) {
+        const size_t off = 2 * (base + rr * Nx - (size_t)(R - w) * NxNy);
+        v = ld_cpair<TS, TC>(rd.stencil + off);
+        if (NS == 2) {
+          const CPair<TC> v2 = ld_cpair<TS, TC>(rd.stencil2 + off);
+          v = {vadd(v.a, v2.a), vadd(v.b, v2.b)};
+        }
+      }
+      q[rr][w] = v;
+    }
+#pragma unroll
+    for (int w = R; w < QN; w++) q[rr][w] = {vsplat(TC(0)), vsplat(TC(0))};
+  }
 
   int t = 0;
 
@@ -399,16 +435,17 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
       atomicExch(p.status, 6);
       return false;
     }
-    {
+#pragma unroll
+    for (int rr = 0; rr < ROWS; rr++) {
       // the stencil value is the sum of the NS stencil fields
-      const unsigned char* sp = sbase + (size_t)slot * stride + row_off;
+      const unsigned char* sp = sbase + (size_t)slot * stride + row_off + ES * rr * HW;
       CPair<TC> v = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(sp));
       if (NS == 2) {
         const CPair<TC> v2 =
             ld_cpair<TS, TC>(reinterpret_cast<const TS*>(sp + p.halo_smem_bytes));
         v = {vadd(v.a, v2.a), vadd(v.b, v2.b)};
       }
-      q[(R + KK) % QN] = v;
+      q[rr][(R + KK) % QN] = v;
     }
     if (t >= R) {
       const int z = z0 + t - R;
@@ -422,178 +459,197 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
         }
         return v;
       };
-      // NS = 2: the two stencil fields at the site, kept apart for the
-      // pointwise part of the recipe
-      CPair<TC> sc0, sc1;
-      if (NS == 2) {
-        sc0 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hc));
-        sc1 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hc + p.halo_smem_bytes));
-      }
-      auto zq = [&](int d) -> const CPair<TC>& { return q[(R + KK + 1 + R + d + 2 * QN) % QN]; };
-      const CPair<TC> xa = lds(0, -2);
-      const CPair<TC> xc = lds(0, 2);
-      const CPair<TC> yp1 = lds(1, 0), ym1 = lds(-1, 0);
-      CPair<TC> yp2 = yp1, ym2 = ym1;
-      if (R == 2) {
-        yp2 = lds(2, 0);
-        ym2 = lds(-2, 0);
-      }
-      CPair<TC> P[NP > 0 ? NP : 1];
-      if (NP > 0) {
-        const unsigned char* pb = sbase + (size_t)slot * stride + hstride + pt_off;
+      auto zq = [&](int rr, int d) -> const CPair<TC>& {
+        return q[rr][(R + KK + 1 + R + d + 2 * QN) % QN];
+      };
+      // y-neighbour rows of the warp's rows, each loaded once: the rows
+      // below (-R.. -1 relative to its first row) and above (ROWS..
+      // ROWS-1+R) from the halo box; its own rows are their z-queue centres
+      CPair<TC> ylo[R], yhi[R];
 #pragma unroll
-        for (int qq = 0; qq < NP; qq++)
-          P[qq] = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(pb + (size_t)qq * p.pt_smem_bytes));
+      for (int k = 0; k < R; k++) {
+        ylo[k] = lds(k - R, 0);
+        yhi[k] = lds(ROWS + k, 0);
       }
+      auto yrow = [&](int dr) -> const CPair<TC>& {
+        return dr < 0 ? ylo[R + dr] : dr >= ROWS ? yhi[dr - ROWS] : zq(dr, 0);
+      };
       TC Vz = TC(0), Dz = TC(0);
       double Wz = 0.0;
       if (TRAP || ((FULL || (EPI & EPI_ENERGY)) && useV)) Vz = tabVz[z];
       if (FULL && useD) Dz = tabDz[z];
       if (EPI & EPI_NORM) Wz = tabWz[z];
 
-      V res[2][2];  // [output][site]
 #pragma unroll
-      for (int e = 0; e < 2; e++) {
-        const CPair<TC>& ctr = zq(0);
-        const V f0 = e ? ctr.b : ctr.a;
-        const V xm1 = e ? ctr.a : xa.b, xp1 = e ? xc.a : ctr.b;
-        const V xm2 = e ? xa.b : xa.a, xp2 = e ? xc.b : xc.a;
-        V L = vmul(cx1, vadd(xp1, xm1));
-        L = vfma(cy1, vadd(e ? yp1.b : yp1.a, e ? ym1.b : ym1.a), L);
-        L = vfma(cz1, vadd(e ? zq(1).b : zq(1).a, e ? zq(-1).b : zq(-1).a), L);
-        if (R == 2) {
-          L = vfma(cx2, vadd(xp2, xm2), L);
-          L = vfma(cy2, vadd(e ? yp2.b : yp2.a, e ? ym2.b : ym2.a), L);
-          L = vfma(cz2, vadd(e ? zq(2).b : zq(2).a, e ? zq(-2).b : zq(-2).a), L);
+      for (int rr = 0; rr < ROWS; rr++) {
+        const unsigned char* hr = hc + ES * rr * HW;  // the row's centre
+        // NS = 2: the two stencil fields at the site, kept apart for the
+        // pointwise part of the recipe
+        CPair<TC> sc0, sc1;
+        if (NS == 2) {
+          sc0 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hr));
+          sc1 = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(hr + p.halo_smem_bytes));
         }
-        L = vfma(c0l, f0, L);
-        const bool ok = e ? ok1 : ok0;
-
-        if (EPI & EPI_ENERGY) {
-          if (ok) {
-            const double lr = (double)L.x, li = (double)L.y;
-            const double fr = (double)f0.x, fi = (double)f0.y;
-            const double d2 = fr * fr + fi * fi;
-            const double kin = -(lr * fr + li * fi);
-            red0 += kin + 0.5 * (d2 * d2);
-            red1 += 0.5 * kin + (double)(Vxy[e] + Vz) * d2 + 0.5 * eg * d2 * d2 -
-                    emu * d2;
-          }
-          continue;
-        }
-
-        const TC a2 = fma(f0.y, f0.y, f0.x * f0.x);
-        V Kv;
-        if (EPI & EPI_LAP) {
-          Kv = L;
-        } else if (!FULL) {
-          const TC s = TRAP ? fma(cns, a2, fma(cVs, Vxy[e] + Vz, c0s)) : fma(cns, a2, c0s);
-          Kv = vfma(vsplat(s), f0, vmul(cLv, L));
-        } else {
-          const TC Vs = useV ? Vxy[e] + Vz : TC(0);
-          const TC s = c0s + cVs * Vs + cns * a2;
-          const V B = vfma(vsplat(s), f0, vmul(cLv, L));
-          const TC arr = useD ? ar0 + ard * (Dxy[e] + Dz) : ar0;
-          Kv = vfma(vsplat(arr), B, vmul(vpair(-ais, ais), vswap(B)));
-          if (useG) {
-            V gx = vmul(vsplat(gx1), vfma(xm1, mone, xp1));
-            if (R == 2) gx = vfma(vsplat(gx2), vfma(xm2, mone, xp2), gx);
-            Kv = vfma(vsplat(Us), gx, Kv);
-          }
-          if (useS) {
-            const double X = rd.tabX[0][i0 + e], Y = rd.tabX[1][j], Z = rd.tabX[2][z];
-            const TC m = (TC)(0.5 * (1.0 + tanh(sqrt(X * X + Y * Y + Z * Z) - 10.0 - 2.0)));
-            Kv = vmul(vsplat(m), Kv);
-          }
-        }
-
-        const V Ks = vswap(Kv);
-#pragma unroll
-        for (int o = 0; o < NOUT; o++) {
-          // smallest terms first: a (x) K, field 1, pointwise, field 0
-          V v = vfma(ar[o], Kv, vmul(aix[o], Ks));
-          if (NS == 2 && (AMASK & (4 << o))) v = vfma(alv2[o], e ? sc1.b : sc1.a, v);
+        const CPair<TC> xa = lds(rr, -2);
+        const CPair<TC> xc = lds(rr, 2);
+        const CPair<TC>& yp1 = yrow(rr + 1);
+        const CPair<TC>& ym1 = yrow(rr - 1);
+        const CPair<TC>& yp2 = yrow(R == 2 ? rr + 2 : rr + 1);
+        const CPair<TC>& ym2 = yrow(R == 2 ? rr - 2 : rr - 1);
+        CPair<TC> P[NP > 0 ? NP : 1];
+        if (NP > 0) {
+          const unsigned char* pb =
+              sbase + (size_t)slot * stride + hstride + pt_off + ES * rr * TX;
 #pragma unroll
           for (int qq = 0; qq < NP; qq++)
-            if (BMASK & (1 << (o * 8 + qq))) v = vfma(bev[o][qq], e ? P[qq].b : P[qq].a, v);
-          if (AMASK & (1 << o)) v = vfma(alv[o], NS == 2 ? (e ? sc0.b : sc0.a) : f0, v);
-          res[o][e] = v;
+            P[qq] = ld_cpair<TS, TC>(reinterpret_cast<const TS*>(pb + (size_t)qq * p.pt_smem_bytes));
         }
 
-        if (EPI & EPI_KAHAN) {
-          // res[0] is the increment delta; compensated add to psi.  Slots:
-          // psi = P[0] when NP >= 2 (else the stencil field), c = P[NP-1].
-          // psi: stencil field 0 at the site when there are two, else
-          // P[0] when NP >= 2, else the stencil field
-          const V psi = (NS == 2) ? (e ? sc0.b : sc0.a)
-                                  : (NP >= 2) ? (e ? P[0].b : P[0].a) : f0;
-          const V cc = e ? P[NP > 0 ? NP - 1 : 0].b : P[NP > 0 ? NP - 1 : 0].a;
-          const V y = vfma(cc, mone, res[0][e]);
-          const V tt = vadd(psi, y);
-          res[1][e] = vfma(y, mone, vfma(psi, mone, tt));
-          res[0][e] = tt;
-        }
-
-        if (ok && (EPI & EPI_NORM)) {
-          const double vr = (double)res[0][e].x, vi = (double)res[0][e].y;
-          red0 = fma(Wxy[e] * Wz, fma(vr, vr, vi * vi), red0);
-        }
-        if (ok && (EPI & EPI_ERR)) {
-          // err = sum_q ce[q] P_q + cek (x) K; psi = P[0], k1 = P[1]
-          const double kr = (double)Kv.x, ki = (double)Kv.y;
-          double er = cek_r * kr - cek_i * ki;
-          double ei = cek_r * ki + cek_i * kr;
+        V res[2][2];  // [output][site]
 #pragma unroll
-          for (int qq = 1; qq < NP; qq++) {
-            const V pv = e ? P[qq].b : P[qq].a;
-            er = fma(p.ce[qq], (double)pv.x, er);
-            ei = fma(p.ce[qq], (double)pv.y, ei);
+        for (int e = 0; e < 2; e++) {
+          const CPair<TC>& ctr = zq(rr, 0);
+          const V f0 = e ? ctr.b : ctr.a;
+          const V xm1 = e ? ctr.a : xa.b, xp1 = e ? xc.a : ctr.b;
+          const V xm2 = e ? xa.b : xa.a, xp2 = e ? xc.b : xc.a;
+          V L = vmul(cx1, vadd(xp1, xm1));
+          L = vfma(cy1, vadd(e ? yp1.b : yp1.a, e ? ym1.b : ym1.a), L);
+          L = vfma(cz1, vadd(e ? zq(rr, 1).b : zq(rr, 1).a, e ? zq(rr, -1).b : zq(rr, -1).a), L);
+          if (R == 2) {
+            L = vfma(cx2, vadd(xp2, xm2), L);
+            L = vfma(cy2, vadd(e ? yp2.b : yp2.a, e ? ym2.b : ym2.a), L);
+            L = vfma(cz2, vadd(e ? zq(rr, 2).b : zq(rr, 2).a, e ? zq(rr, -2).b : zq(rr, -2).a), L);
           }
-          const V psi0 = e ? P[0].b : P[0].a;
-          const V k1 = e ? P[NP > 1 ? 1 : 0].b : P[NP > 1 ? 1 : 0].a;
-          const double apsi = hypot((double)psi0.x, (double)psi0.y);
-          const double m = hypot((double)k1.x, (double)k1.y) * inv_absdt;
-          const double sr = apsi + dt0_r * m + 1e-30, si = dt0_i * m;
-          red1 = fmax(red1, hypot(er, ei) / hypot(sr, si));
-        }
-      }
+          L = vfma(c0l, f0, L);
+          const bool ok = e ? ok1[rr] : ok0[rr];
 
-      if (!(EPI & EPI_ENERGY)) {
-        long gzo[2] = {0, 0};
-        if (near_edge(z, nz)) {
-          int a, b;
-          ghost_targets(z, nz, bcs, a, b);
-          if (a != NO_GHOST && !((a < 0) ? zg_lo : zg_hi)) a = NO_GHOST;
-          if (b != NO_GHOST && !((b < 0) ? zg_lo : zg_hi)) b = NO_GHOST;
-          gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
-          gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
-        }
-        const bool edge = edge_xy || ((gzo[0] | gzo[1]) != 0);
-#pragma unroll
-        for (int o = 0; o < NOUT; o++) {
-          TS* out = outp[o] + 2 * base;
-          if (ok1) {
-            st_cpair<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
-                                              cvt_v<TS>(res[o][1]));
-          } else if (ok0) {
-            st_c1<TS>(out, res[o][0]);
+          if (EPI & EPI_ENERGY) {
+            if (ok) {
+              const double lr = (double)L.x, li = (double)L.y;
+              const double fr = (double)f0.x, fi = (double)f0.y;
+              const double d2 = fr * fr + fi * fi;
+              const double kin = -(lr * fr + li * fi);
+              red0 += kin + 0.5 * (d2 * d2);
+              red1 += 0.5 * kin + (double)(Vxy[rr][e] + Vz) * d2 + 0.5 * eg * d2 * d2 -
+                      emu * d2;
+            }
+            continue;
           }
-          if (edge && (p.ghost_mask & (1 << o))) {
+
+          const TC a2 = fma(f0.y, f0.y, f0.x * f0.x);
+          V Kv;
+          if (EPI & EPI_LAP) {
+            Kv = L;
+          } else if (!FULL) {
+            const TC s = TRAP ? fma(cns, a2, fma(cVs, Vxy[rr][e] + Vz, c0s)) : fma(cns, a2, c0s);
+            Kv = vfma(vsplat(s), f0, vmul(cLv, L));
+          } else {
+            const TC Vs = useV ? Vxy[rr][e] + Vz : TC(0);
+            const TC s = c0s + cVs * Vs + cns * a2;
+            const V B = vfma(vsplat(s), f0, vmul(cLv, L));
+            const TC arr = useD ? ar0 + ard * (Dxy[rr][e] + Dz) : ar0;
+            Kv = vfma(vsplat(arr), B, vmul(vpair(-ais, ais), vswap(B)));
+            if (useG) {
+              V gx = vmul(vsplat(gx1), vfma(xm1, mone, xp1));
+              if (R == 2) gx = vfma(vsplat(gx2), vfma(xm2, mone, xp2), gx);
+              Kv = vfma(vsplat(Us), gx, Kv);
+            }
+            if (useS) {
+              const double X = rd.tabX[0][i0 + e], Y = rd.tabX[1][j0 + rr], Z = rd.tabX[2][z];
+              const TC m = (TC)(0.5 * (1.0 + tanh(sqrt(X * X + Y * Y + Z * Z) - 10.0 - 2.0)));
+              Kv = vmul(vsplat(m), Kv);
+            }
+          }
+
+          const V Ks = vswap(Kv);
 #pragma unroll
-            for (int e = 0; e < 2; e++) {
-              if (!(e ? ok1 : ok0)) continue;
-              TS* o1 = out + 2 * e;
-              const V v = res[o][e];
-              if (gxo[e][0]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gxo[e][0], v);
-              if (gxo[e][1]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gxo[e][1], v);
-              if (gyo[0]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gyo[0], v);
-              if (gyo[1]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gyo[1], v);
-              if (gzo[0]) st_c1<TS>(o1 + 2 * gzo[0], v);
-              if (gzo[1]) st_c1<TS>(o1 + 2 * gzo[1], v);
+          for (int o = 0; o < NOUT; o++) {
+            // smallest terms first: a (x) K, field 1, pointwise, field 0
+            V v = vfma(ar[o], Kv, vmul(aix[o], Ks));
+            if (NS == 2 && (AMASK & (4 << o))) v = vfma(alv2[o], e ? sc1.b : sc1.a, v);
+#pragma unroll
+            for (int qq = 0; qq < NP; qq++)
+              if (BMASK & (1 << (o * 8 + qq))) v = vfma(bev[o][qq], e ? P[qq].b : P[qq].a, v);
+            if (AMASK & (1 << o)) v = vfma(alv[o], NS == 2 ? (e ? sc0.b : sc0.a) : f0, v);
+            res[o][e] = v;
+          }
+
+          if (EPI & EPI_KAHAN) {
+            // res[0] is the increment delta; compensated add to psi.  Slots:
+            // psi = P[0] when NP >= 2 (else the stencil field), c = P[NP-1].
+            // psi: stencil field 0 at the site when there are two, else
+            // P[0] when NP >= 2, else the stencil field
+            const V psi = (NS == 2) ? (e ? sc0.b : sc0.a)
+                                    : (NP >= 2) ? (e ? P[0].b : P[0].a) : f0;
+            const V cc = e ? P[NP > 0 ? NP - 1 : 0].b : P[NP > 0 ? NP - 1 : 0].a;
+            const V y = vfma(cc, mone, res[0][e]);
+            const V tt = vadd(psi, y);
+            res[1][e] = vfma(y, mone, vfma(psi, mone, tt));
+            res[0][e] = tt;
+          }
+
+          if (ok && (EPI & EPI_NORM)) {
+            const double vr = (double)res[0][e].x, vi = (double)res[0][e].y;
+            red0 = fma(Wxy[rr][e] * Wz, fma(vr, vr, vi * vi), red0);
+          }
+          if (ok && (EPI & EPI_ERR)) {
+            // err = sum_q ce[q] P_q + cek (x) K; psi = P[0], k1 = P[1]
+            const double kr = (double)Kv.x, ki = (double)Kv.y;
+            double er = cek_r * kr - cek_i * ki;
+            double ei = cek_r * ki + cek_i * kr;
+#pragma unroll
+            for (int qq = 1; qq < NP; qq++) {
+              const V pv = e ? P[qq].b : P[qq].a;
+              er = fma(p.ce[qq], (double)pv.x, er);
+              ei = fma(p.ce[qq], (double)pv.y, ei);
+            }
+            const V psi0 = e ? P[0].b : P[0].a;
+            const V k1 = e ? P[NP > 1 ? 1 : 0].b : P[NP > 1 ? 1 : 0].a;
+            const double apsi = hypot((double)psi0.x, (double)psi0.y);
+            const double m = hypot((double)k1.x, (double)k1.y) * inv_absdt;
+            const double sr = apsi + dt0_r * m + 1e-30, si = dt0_i * m;
+            red1 = fmax(red1, hypot(er, ei) / hypot(sr, si));
+          }
+        }
+
+        if (!(EPI & EPI_ENERGY)) {
+          long gzo[2] = {0, 0};
+          if (near_edge(z, nz)) {
+            int a, b;
+            ghost_targets(z, nz, bcs, a, b);
+            if (a != NO_GHOST && !((a < 0) ? zg_lo : zg_hi)) a = NO_GHOST;
+            if (b != NO_GHOST && !((b < 0) ? zg_lo : zg_hi)) b = NO_GHOST;
+            gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
+            gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
+          }
+          const bool edge = edge_xy[rr] || ((gzo[0] | gzo[1]) != 0);
+#pragma unroll
+          for (int o = 0; o < NOUT; o++) {
+            TS* out = outp[o] + 2 * (base + rr * Nx);
+            if (ok1[rr]) {
+              st_cpair<TS, typename VT<TS>::T>(out, cvt_v<TS>(res[o][0]),
+                                                cvt_v<TS>(res[o][1]));
+            } else if (ok0[rr]) {
+              st_c1<TS>(out, res[o][0]);
+            }
+            if (edge && (p.ghost_mask & (1 << o))) {
+#pragma unroll
+              for (int e = 0; e < 2; e++) {
+                if (!(e ? ok1[rr] : ok0[rr])) continue;
+                TS* o1 = out + 2 * e;
+                const V v = res[o][e];
+                if (gxo[e][0]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gxo[e][0], v);
+                if (gxo[e][1]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gxo[e][1], v);
+                if (gyo[rr][0]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gyo[rr][0], v);
+                if (gyo[rr][1]) st_c1<TS>(o1 + 2 * (ptrdiff_t)gyo[rr][1], v);
+                if (gzo[0]) st_c1<TS>(o1 + 2 * gzo[0], v);
+                if (gzo[1]) st_c1<TS>(o1 + 2 * gzo[1], v);
+              }
             }
           }
         }
-      }
+      }  // rows
+
       base += NxNy;
     }
     if (t >= R) {
@@ -644,10 +700,10 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
       s_red[0][ty] = red0;
       s_red[1][ty] = red1;
     }
-    named_barrier_sync(1, 32 * TY);
+    named_barrier_sync(1, 32 * NW);
     if (tid == 0) {
       double a = 0.0, b = 0.0;
-      for (int w2 = 0; w2 < TY; w2++) {
+      for (int w2 = 0; w2 < NW; w2++) {
         a += s_red[0][w2];
         b = (EPI & EPI_ERR) ? fmax(b, s_red[1][w2]) : b + s_red[1][w2];
       }
@@ -655,7 +711,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
       p.partials[2 * (size_t)it + 1] = b;
       s_stop = *(volatile int*)&s_abort;
     }
-    named_barrier_sync(1, 32 * TY);
+    named_barrier_sync(1, 32 * NW);
     if (*(volatile int*)&s_stop) break;
   } else if (aborted) {
     break;  // no barrier among the compute warps in this recipe
@@ -689,11 +745,21 @@ __global__ void __launch_bounds__(288)
 // Registers capped for three resident CTAs per SM: the complex64 recipes
 // that stage only stencil planes, whose warps mostly wait on fixed-latency
 // and shared-memory dependencies, so more warps per scheduler hide more of
-// it (their three rings of slots fit in shared memory).
+// it (their three rings of slots fit in shared memory).  One row per warp:
+// 8 compute warps + the producer.
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
           int BMASK, int FORM, bool BATCH>
 __global__ void __launch_bounds__(288, 3)
     stage_kernel_occ3(const __grid_constant__ StageParams<TS, TC> p) {
+  stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FORM, BATCH>(p);
+}
+
+// The same for the two-row recipes (rows_per_warp == 2): 4 compute warps +
+// the producer on an 8-row tile, three CTAs per SM.
+template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AMASK,
+          int BMASK, int FORM, bool BATCH>
+__global__ void __launch_bounds__(160, 3)
+    stage_kernel_rows2(const __grid_constant__ StageParams<TS, TC> p) {
   stage_body<TS, TC, R, NS, NP, NOUT, EPI, AMASK, BMASK, FORM, BATCH>(p);
 }
 

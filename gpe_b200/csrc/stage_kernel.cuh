@@ -479,6 +479,22 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
       if (TRAP || ((FULL || (EPI & EPI_ENERGY)) && useV)) Vz = tabVz[z];
       if (FULL && useD) Dz = tabDz[z];
       if (EPI & EPI_NORM) Wz = tabWz[z];
+      // z ghosts this plane feeds (element offsets): once per plane for
+      // several rows, at the store for one (fewer registers held through
+      // the stencil)
+      auto z_ghosts = [&](long* gzo) {
+        gzo[0] = gzo[1] = 0;
+        if (near_edge(z, nz)) {
+          int a, b;
+          ghost_targets(z, nz, bcs, a, b);
+          if (a != NO_GHOST && !((a < 0) ? zg_lo : zg_hi)) a = NO_GHOST;
+          if (b != NO_GHOST && !((b < 0) ? zg_lo : zg_hi)) b = NO_GHOST;
+          gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
+          gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
+        }
+      };
+      long gzo_plane[2] = {0, 0};
+      if (ROWS > 1 && !(EPI & EPI_ENERGY)) z_ghosts(gzo_plane);
 
 #pragma unroll
       for (int rr = 0; rr < ROWS; rr++) {
@@ -613,15 +629,8 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
         }
 
         if (!(EPI & EPI_ENERGY)) {
-          long gzo[2] = {0, 0};
-          if (near_edge(z, nz)) {
-            int a, b;
-            ghost_targets(z, nz, bcs, a, b);
-            if (a != NO_GHOST && !((a < 0) ? zg_lo : zg_hi)) a = NO_GHOST;
-            if (b != NO_GHOST && !((b < 0) ? zg_lo : zg_hi)) b = NO_GHOST;
-            gzo[0] = (a != NO_GHOST) ? (long)(a - z) * (long)NxNy : 0;
-            gzo[1] = (b != NO_GHOST) ? (long)(b - z) * (long)NxNy : 0;
-          }
+          long gzo[2] = {gzo_plane[0], gzo_plane[1]};
+          if (ROWS == 1) z_ghosts(gzo);
           const bool edge = edge_xy[rr] || ((gzo[0] | gzo[1]) != 0);
 #pragma unroll
           for (int o = 0; o < NOUT; o++) {

@@ -72,7 +72,7 @@ enum : int { FORM_PLAIN = 0, FORM_TRAP = 1, FORM_FULL = 2 };
 // them, and a warp with two adjacent rows loads the y-neighbour rows the two
 // share once (rows -2, -1, +2, +3 of its first row for four, each row's own
 // centre serving as the other's nearest neighbour).  Measured at 512^3: the
-// stage 0.655 -> 0.602 ms; the one-field stage 1 lost (0.429 -> 0.443 ms:
+// stage 0.655 -> 0.605 ms; the one-field stage 1 lost (0.429 -> 0.443 ms:
 // instruction-bound, and its warps per SM fell from 27 to 15), so it keeps
 // one row per warp.
 template <typename TS, typename TC>

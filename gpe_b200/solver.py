@@ -301,19 +301,34 @@ class GpeSolver:
                                                  ctypes.byref(v)), self._ctx)
         return v.value
 
-    def zeros(self):
+    def zeros(self, out: np.ndarray | None = None):
         """get_zeros / get_extra_zeros / get_re_im_zeros (src/io.f90:895-1402)
-        -> (counts[12], points (n, 3)), sections in the reference's order."""
-        from ._lib import pinned_empty
+        -> (counts[12], points (n, 3)), sections in the reference's order.
+
+        The point list can run to gigabytes.  By default it goes to a new
+        array; `out` (float64, C-contiguous, shape (cap, 3), cap >= the point
+        count) is filled instead and a view of its first n rows returned, so
+        a caller that asks repeatedly can keep one page-locked buffer
+        (`gpe_b200._lib.pinned_empty`) and copy at the link's full rate
+        without locking gigabytes of pages on every call."""
         counts = np.zeros(12, dtype=np.int64)
         P64 = ctypes.POINTER(ctypes.c_int64)
         check(lib().gpe_gpu_zeros(self._ctx, counts.ctypes.data_as(P64), None, 0), self._ctx)
-        # page-locked: the point list can run to gigabytes
-        pts = pinned_empty((max(int(counts.sum()), 1), 3), np.float64)
+        n = int(counts.sum())
+        if out is None:
+            pts = np.empty((max(n, 1), 3), np.float64)
+        else:
+            if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.ndim != 2
+                    or out.shape[1] != 3 or not out.flags.c_contiguous or not out.flags.writeable):
+                raise GpeError(1, "out must be a writeable C-contiguous float64 array of "
+                                  "shape (cap, 3)")
+            if out.shape[0] < n:
+                raise GpeError(1, f"out holds {out.shape[0]} points, {n} found")
+            pts = out
         check(lib().gpe_gpu_zeros(self._ctx, counts.ctypes.data_as(P64),
                                   pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                   pts.shape[0]), self._ctx)
-        return counts, pts[:int(counts.sum())]
+        return counts, pts[:n]
 
     def renormalise(self, norm: float) -> None:
         """renormalise (src/variables.f90:698-709)."""

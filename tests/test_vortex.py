@@ -172,6 +172,29 @@ def test_gpu_zeros_of_lines_and_a_random_phase_state():
 
 
 @pytest.mark.gpu
+def test_gpu_zeros_into_a_kept_buffer():
+    from gpe_b200 import GpeError
+    from gpe_b200._lib import pinned_empty
+    rng = np.random.default_rng(5)
+    psi = rng.standard_normal((14, 13, 12)) + 1j * rng.standard_normal((14, 13, 12))
+    with _solver(14, 13, 12) as s:
+        s.set_state(psi)
+        want_c, want_p = s.zeros()
+        n = int(want_c.sum())
+        buf = pinned_empty((n + 7, 3), np.float64)
+        buf[:] = -1.0
+        counts, pts = s.zeros(out=buf)
+        assert counts.tolist() == want_c.tolist()
+        np.testing.assert_array_equal(pts, want_p)
+        assert pts.base is not None and np.shares_memory(pts, buf)
+        assert np.all(buf[n:] == -1.0)
+        for bad in (np.zeros((n - 1, 3)), np.zeros((n, 3), np.float32), np.zeros((n, 4)),
+                    np.zeros((3, n)).T):
+            with pytest.raises(GpeError):
+                s.zeros(out=bad)
+
+
+@pytest.mark.gpu
 def test_gpu_zeros_rejects_a_small_buffer_and_fills_the_counts():
     import ctypes
 

@@ -492,7 +492,7 @@ constexpr bool occ3_recipe(int np, bool full, bool batch) {
 template <typename TS, typename TC, int R, int NS, int NP, int NOUT, int EPI, int AM, int BM,
           int FORM, bool BATCH>
 KernelFn kernel_for() {
-  if constexpr (rows_per_warp<TS, TC>(NS, NP, FORM, BATCH) == 2)
+  if constexpr (rows_per_warp<TS, TC>(R, NS, NP, FORM, BATCH) == 2)
     return reinterpret_cast<KernelFn>(
         &stage_kernel_rows2<TS, TC, R, NS, NP, NOUT, EPI, AM, BM, FORM, BATCH>);
   else if constexpr (occ3_recipe<TS, TC>(NP, FORM == FORM_FULL, BATCH))
@@ -1847,10 +1847,15 @@ int batch_prepare_par(gpe_batch* b, cd dt, int par) {
     int form = b->form;
     KernelFn fn = select_kernel<TS, TC, true>(b->R, &form, sp, am, bm);
     if (!fn) return bfail(b, GPE_ERR_INVALID, "no batched kernel for this stage");
-    LaunchShape sh = ring_shape(b->es, b->R, sp.np, b->TY, sp.stencil2 >= 0 ? 2 : 1);
+    const int ns = sp.stencil2 >= 0 ? 2 : 1;
+    const int rows = rows_per_warp<TS, TC>(b->R, ns, sp.np, form, true);
+    // two-row recipes: rings for three CTAs per SM, as their registers allow
+    LaunchShape sh = ring_shape(b->es, b->R, sp.np, b->TY, ns, rows == 2 ? 3 : 2);
+    sh.rows = rows;
     BCU(b, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     int occ = 0;
-    BCU(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (sh.TY + 1), sh.smem));
+    BCU(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * (sh.TY / sh.rows + 1),
+                                                         sh.smem));
     if (occ < 1) return bfail(b, GPE_ERR_INVALID, "batched stage kernel cannot be resident");
     const int per_sm = b->opts.ctas_per_sm > 0 ? std::min(b->opts.ctas_per_sm, occ) : occ;
     const int grid = std::min(b->nitems, per_sm * b->runs[0]->num_sms);
@@ -1916,7 +1921,7 @@ int batch_enqueue_step(gpe_batch* b, int par) {
   for (int s = 0; s < 4; s++) {
     auto& S = b->st[par][s];
     void* args[] = {S.params.data()};
-    BCU(b, cudaLaunchKernel(S.fn, dim3((unsigned)S.grid), dim3(32, (unsigned)S.sh.TY + 1),
+    BCU(b, cudaLaunchKernel(S.fn, dim3((unsigned)S.grid), dim3(32, (unsigned)(S.sh.TY / S.sh.rows) + 1),
                             args, S.sh.smem, b->stream));
   }
   batch_finalize_kernel<<<(unsigned)b->runs.size(), 256, 0, b->stream>>>(

@@ -67,7 +67,8 @@ enum : int {
 enum : int { FORM_PLAIN = 0, FORM_TRAP = 1, FORM_FULL = 2 };
 
 // Rows of the tile each compute warp owns.  Two for the complex64 recipes
-// that stage two stencil fields and nothing else (rk4 stages 2 and 3):
+// that stage two stencil fields and nothing else (rk4 stages 2 and 3, in
+// single-run and batched launches):
 // their shared-memory loads (both fields at every x and y neighbour) bound
 // them, and a warp with two adjacent rows loads the y-neighbour rows the two
 // share once (rows -2, -1, +2, +3 of its first row for four, each row's own
@@ -75,10 +76,12 @@ enum : int { FORM_PLAIN = 0, FORM_TRAP = 1, FORM_FULL = 2 };
 // stage 0.655 -> 0.605 ms; the one-field stage 1 lost (0.429 -> 0.443 ms:
 // instruction-bound, and its warps per SM fell from 27 to 15), so it keeps
 // one row per warp.
+// A batched launch holds its run descriptor in registers too; with two rows
+// its order-4 recipes spill, so batched launches take two rows at order 2.
 template <typename TS, typename TC>
-__host__ __device__ constexpr int rows_per_warp(int ns, int np, int form, bool batch) {
+__host__ __device__ constexpr int rows_per_warp(int r, int ns, int np, int form, bool batch) {
   return (std::is_same<TS, float>::value && std::is_same<TC, float>::value && ns == 2 &&
-          np == 0 && form != FORM_FULL && !batch)
+          np == 0 && form != FORM_FULL && !(batch && r > 1))
              ? 2
              : 1;
 }
@@ -174,7 +177,7 @@ __device__ __forceinline__ void stage_body(const StageParams<TS, TC>& p) {
   using V = typename VT<TC>::T;
   using RD = RunDesc<TS, TC>;
   constexpr bool FULL = FORM == FORM_FULL, TRAP = FORM == FORM_TRAP;
-  constexpr int ROWS = rows_per_warp<TS, TC>(NS, NP, FORM, BATCH);
+  constexpr int ROWS = rows_per_warp<TS, TC>(R, NS, NP, FORM, BATCH);
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_abort, s_issued, s_stop;
   __shared__ double s_red[2][32];

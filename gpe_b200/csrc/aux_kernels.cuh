@@ -121,12 +121,10 @@ __global__ void norm_kernel(const TS* __restrict__ f, Geom g,
 // Fixed-order reduction of partials[2*b + slot], b < nblk, by one CTA of
 // 1024 threads.  op 0 = sum, 1 = max.  out[0] = result * scale; when
 // `series` is non-null also series[*counter] = out[0] and ++*counter.
-__global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
-                                int slot, int op, double scale,
-                                double* __restrict__ out,
-                                double* __restrict__ series,
-                                int* __restrict__ counter) {
-  __shared__ double s[1024];
+// Fixed-order reduction of slot `slot` of the per-CTA partials by one block
+// (sum, or max for op 1); the result is s[0] for every thread on return.
+__device__ __forceinline__ void reduce_partials(const double* __restrict__ partials, int nblk,
+                                                int slot, int op, double* s) {
   double a = 0.0;
   for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
     const double v = partials[2 * (size_t)b + slot];
@@ -141,6 +139,15 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
     }
     __syncthreads();
   }
+}
+
+__global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
+                                int slot, int op, double scale,
+                                double* __restrict__ out,
+                                double* __restrict__ series,
+                                int* __restrict__ counter) {
+  __shared__ double s[1024];
+  reduce_partials(partials, nblk, slot, op, s);
   if (threadIdx.x == 0) {
     const double r = s[0] * scale;
     out[0] = r;
@@ -183,11 +190,10 @@ __global__ void rk45_begin_kernel(DevTime* T, cudaGraphConditionalHandle h, int 
 // direction; an accepted one grows to safety dt errmax^dt_increase, or 5 dt
 // when errmax <= errcon; t advances by the accepted dt and im_t by the new
 // |Im dt|.
-__global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
-                                    double* __restrict__ s_norm, double* __restrict__ s_dt,
-                                    int* __restrict__ s_att, int cap,
-                                    cudaGraphConditionalHandle h, int use_cond) {
-  if (threadIdx.x != 0) return;
+__device__ void rk45_control(DevTime* T, const double* __restrict__ scal,
+                             double* __restrict__ s_norm, double* __restrict__ s_dt,
+                             int* __restrict__ s_att, int cap, cudaGraphConditionalHandle h,
+                             int use_cond) {
   const double safety = 0.9, dt_decrease = -0.25, dt_increase = -0.20;
   if (T->halt) {
     if (use_cond) cudaGraphSetConditional(h, 0u);
@@ -246,6 +252,34 @@ __global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
     }
   }
   if (use_cond) cudaGraphSetConditional(h, done ? 0u : 1u);
+}
+
+__global__ void rk45_control_kernel(DevTime* T, const double* __restrict__ scal,
+                                    double* __restrict__ s_norm, double* __restrict__ s_dt,
+                                    int* __restrict__ s_att, int cap,
+                                    cudaGraphConditionalHandle h, int use_cond) {
+  if (threadIdx.x == 0) rk45_control(T, scal, s_norm, s_dt, s_att, cap, h, use_cond);
+}
+
+// A context with no neighbours: the attempt's two reductions (error maximum
+// into scal[3], trial-state norm into scal[0], each as finalize_kernel forms
+// it) and the step control in one launch of 1024 threads.
+__global__ void rk45_reduce_control_kernel(const double* __restrict__ partials, int nblk,
+                                           double err_scale, double norm_scale,
+                                           double* __restrict__ scal, DevTime* T,
+                                           double* __restrict__ s_norm,
+                                           double* __restrict__ s_dt, int* __restrict__ s_att,
+                                           int cap, cudaGraphConditionalHandle h,
+                                           int use_cond) {
+  __shared__ double s[1024];
+  reduce_partials(partials, nblk, 1, 1, s);
+  if (threadIdx.x == 0) scal[3] = s[0] * err_scale;
+  __syncthreads();
+  reduce_partials(partials, nblk, 0, 0, s);
+  if (threadIdx.x == 0) {
+    scal[0] = s[0] * norm_scale;
+    rk45_control(T, scal, s_norm, s_dt, s_att, cap, h, use_cond);
+  }
 }
 
 // Slab group: combine d_scal[idx] of n members in member order (sum, or max

@@ -1170,7 +1170,9 @@ int step_rk4(gpe_ctx* c, cd dt) {
 
 // rkck (src/solve.f90:248-378) with the psi_scal / errmax reduction of rkqs
 // (:176-190) fused into the last stage.  Writes the trial state to alt.
-int attempt_rkck(gpe_ctx* c, cd dt, cd dt0, const double* dyn = nullptr) {
+// reduce = false leaves the error maximum and the norm in the per-CTA
+// partials for rk45_reduce_control_kernel.
+int attempt_rkck(gpe_ctx* c, cd dt, cd dt0, const double* dyn = nullptr, bool reduce = true) {
   const bool K = c->prm.kahan != 0;
   const int psi = c->psi_id;
   const int stencils[6] = {psi, F_UA, F_UB, F_UA, F_UB, F_UA};
@@ -1243,6 +1245,7 @@ int attempt_rkck(gpe_ctx* c, cd dt, cd dt0, const double* dyn = nullptr) {
   }
   rc = launch_stage(c, s);
   if (rc) return rc;
+  if (!reduce) return GPE_OK;
   rc = finalize(c, c->last_nblk, 1, 1, 1.0 / RK_EPS, 3, false);
   if (rc) return rc;
   return finalize(c, c->last_nblk, 0, 0, cell_volume(c), 0, false);
@@ -1279,13 +1282,28 @@ bool rk45_capturable(const gpe_ctx* c) { return !c->comm && !c->timing; }
 
 // Enqueues one attempt and its control kernel (use_cond: inside the WHILE
 // node whose handle is h).
+// A context with no z-neighbours reduces the attempt's error maximum and norm
+// in the step-control launch itself; slabs combine them across slabs first.
+bool rk45_fused_control(const gpe_ctx* c) { return !c->group && !c->comm; }
+
+// Launches of one attempt: the six stages, then either the fused reduction
+// and control or two reductions and the control.
+int rk45_launches_per_attempt(const gpe_ctx* c) { return rk45_fused_control(c) ? 7 : 9; }
+
 int rk45_attempt(gpe_ctx* c, cudaGraphConditionalHandle h, int use_cond) {
   DevTime* T = rk45_time(c);
   const double* dyn = reinterpret_cast<const double*>(T);  // dt_r, dt_i, dt0_r, dt0_i
-  int rc = attempt_rkck(c, cd(1.0, 0.0), cd(1.0, 0.0), dyn);
+  const bool fused = rk45_fused_control(c);
+  int rc = attempt_rkck(c, cd(1.0, 0.0), cd(1.0, 0.0), dyn, !fused);
   if (rc) return rc;
-  rk45_control_kernel<<<1, 32, 0, c->stream>>>(T, c->d_scal, c->d_series, c->d_ser_dt,
-                                                c->d_ser_att, (int)c->series_cap, h, use_cond);
+  if (fused) {
+    rk45_reduce_control_kernel<<<1, 1024, 0, c->stream>>>(
+        c->d_partials, c->last_nblk, 1.0 / RK_EPS, cell_volume(c), c->d_scal, T, c->d_series,
+        c->d_ser_dt, c->d_ser_att, (int)c->series_cap, h, use_cond);
+  } else {
+    rk45_control_kernel<<<1, 32, 0, c->stream>>>(T, c->d_scal, c->d_series, c->d_ser_dt,
+                                                  c->d_ser_att, (int)c->series_cap, h, use_cond);
+  }
   CU_CHECK(c, cudaGetLastError());
   c->launches++;
   return GPE_OK;
@@ -1457,7 +1475,7 @@ int step_rk45(gpe_ctx* c, gpe_time* tm, gpe_step_info* info) {
   rc = check_status(c);
   if (rc) return rc;
   if (done != 1) return rk45_halted(c, h);
-  c->launches += rk45_capturable(c) ? 1 + 9 * (int64_t)h.attempts : 0;
+  c->launches += rk45_capturable(c) ? 1 + rk45_launches_per_attempt(c) * (int64_t)h.attempts : 0;
   tm->t = h.t;
   tm->im_t = h.im_t;
   tm->dt_re = h.dt_r;
@@ -2393,7 +2411,7 @@ int gpe_gpu_advance(gpe_ctx* c, int64_t nsteps, gpe_time* tm, double* norms) {
         std::vector<int> att((size_t)done);
         CU_CHECK(c, cudaMemcpy(att.data(), c->d_ser_att, sizeof(int) * done,
                                cudaMemcpyDeviceToHost));
-        for (int a : att) c->launches += 9 * (int64_t)a;
+        for (int a : att) c->launches += rk45_launches_per_attempt(c) * (int64_t)a;
         c->launches += done;
       }
     }

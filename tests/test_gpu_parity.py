@@ -499,3 +499,33 @@ def test_dispersion_matched_laplacian(r):
     assert rel_l2(got, exp) < 1e-12
     with pytest.raises(GpeError):
         GpeSolver(GpeParams(nx=8, ny=8, nz=8, order=2, fd_match=0.5))
+
+
+@pytest.mark.parametrize("precision,kahan,order,bcs,trap", [(8, True, 4, 1, False),
+                                                            (8, False, 2, 2, True),
+                                                            (16, False, 4, 2, False)])
+def test_launch_shape_does_not_change_the_state(precision, kahan, order, bcs, trap):
+    """Every site is computed by the same arithmetic whatever the tile height
+    (4 or 8 rows; the complex64 two-field stages then run 2 or 4 warps of two
+    rows each), the planes per CTA (a ragged last chunk of 3) or the
+    library's own choice, so five rk4 steps leave the same state bit for bit."""
+    n = (70, 13, 11)  # two x tiles (second ragged), ragged y tiles
+    kw = dict(g=1.3, mu=0.9)
+    if trap:
+        kw.update(omx=0.3, omy=0.2, omz=0.4)
+    psi = random_field((n[2], n[1], n[0]), seed=31 + order)
+    if precision == 8:
+        psi = psi.astype(np.complex64)
+    states = []
+    for ty, zc in ((0, 0), (4, 0), (8, 0), (4, 3), (8, 5)):
+        prm = GpeParams(nx=n[0], ny=n[1], nz=n[2], xr=8.0, yr=4.0, zr=3.5, scheme="rk4",
+                        eqn_to_solve=4, bcs=bcs, order=order, precision=precision, kahan=kahan,
+                        tile_y=ty, zchunk=zc, **kw)
+        with GpeSolver(prm, dt=0.01) as s:
+            s.set_state(psi)
+            for _ in range(5):
+                s.solver()
+            states.append((s.get_state(), s.get_norm()))
+    for st, nm in states[1:]:
+        assert np.array_equal(st, states[0][0])
+        assert nm == pytest.approx(states[0][1], rel=1e-12)

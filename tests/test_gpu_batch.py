@@ -80,11 +80,15 @@ def test_fp64_batch_matches_oracle():
             assert norms[r, -1] == pytest.approx(o.get_norm(psi), rel=1e-12)
 
 
-@pytest.mark.parametrize("kahan", [False, True])
-def test_complex64_batch_is_bitwise_single_runs(kahan):
+# order 2: the batched two-field stages run two rows per warp, as the single
+# contexts do; order 4: one row in the batch against two in the single
+# contexts -- the same per-site arithmetic either way
+@pytest.mark.parametrize("kahan,order", [(False, 2), (True, 2), (False, 4), (True, 4)])
+def test_complex64_batch_is_bitwise_single_runs(kahan, order):
     rng = np.random.default_rng(3)
     sizes = rng.choice([32, 48, 64, 96], size=5)
-    prms = [member((int(n),) * 3, om=float(rng.uniform(0.05, 0.15)), precision=8, kahan=kahan)
+    prms = [member((int(n),) * 3, om=float(rng.uniform(0.05, 0.15)), precision=8, kahan=kahan,
+                   order=order)
             for n in sizes]
     psis = states(prms, 11, np.complex64)
     exp, enorm = singles(prms, psis, 12)

@@ -107,6 +107,25 @@ def test_group_stage_launches_boundary_planes_apart_when_slabs_are_deep(nslabs):
         assert np.array_equal(g.get_global_state(), s.get_state())
 
 
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_group_rk45_complex64_kahan_is_bitwise_single_domain(nslabs):
+    """rk45 in complex64 + Kahan: the group combines the slabs' error maxima
+    (a max, independent of order) before its step control, the single context
+    reduces its own in the step-control launch; the same attempts, steps and
+    states, bit for bit."""
+    prm = _prm("rk45", 2, 4, precision=8, kahan=True)
+    psi = random_field((N[2], N[1], N[0]), seed=11).astype(np.complex64)
+    with SlabGroup(prm, nslabs, dt=0.02) as g, GpeSolver(prm, dt=0.02) as s:
+        g.set_global_state(psi)
+        s.set_state(psi)
+        for _ in range(6):
+            gi = g.solver()
+            si = s.solver()
+            assert gi.attempts == si.attempts
+            assert g.dt == s.dt and g.t == s.t
+        assert np.array_equal(g.get_global_state(np.complex64), s.get_state(np.complex64))
+
+
 def test_group_members_refuse_stepping_alone():
     prm = _prm("rk4", 1, 2)
     with SlabGroup(prm, 2, dt=0.01) as g:
